@@ -1,0 +1,204 @@
+/*
+ * laph_gpu.h -- C ABI of liblaph_gpu.so, the B200 (sm_100a) implementation of
+ * the per-timeslice LapH eigensystem path of HISKP-LQCD/LapH_EigSys:
+ *   smearing (HYP / APE / stout)  ->  Chebyshev-accelerated covariant
+ *   Laplacian matvec  ->  lowest-nev eigensolve  ->  phase fixing.
+ *
+ * Every entry point returns an int status (LAPH_OK = 0) and never exits the
+ * process; laph_last_error() gives a one-line message for the calling thread.
+ * Plain pointers and sizes only.  "Host" pointers are ordinary CPU memory and
+ * are staged through the context's stream; "device" pointers are CUDA global
+ * memory of the context's device and are used in place.
+ *
+ * Conventions (identical to the reference):
+ *   site      = x*L*L + y*L + z                     (modules/navigation.cpp:27-88)
+ *   vector    = complex128[3*V3], index 3*site+colour (modules/shell_matop.cpp:33-38)
+ *   eigvecs   = column-major complex128 [3*V3][nev]   (src/ev_ts.cpp:298)
+ *   eigvals   = eigenvalues of Delta = hop - 6, i.e. -lambda(-Delta) <= 0, in
+ *               ascending order of lambda (recover_spectrum, modules/recover_spec.cpp:45-54)
+ */
+#ifndef LAPH_GPU_H_
+#define LAPH_GPU_H_
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+  LAPH_OK = 0,
+  LAPH_EINVAL = 1,     /* bad argument */
+  LAPH_ECUDA = 2,      /* CUDA runtime error */
+  LAPH_ENOMEM = 3,     /* device or host allocation failed */
+  LAPH_EIO = 4,        /* cannot open/read/write (reference: exit(500)) */
+  LAPH_ENORECORD = 5,  /* no ildg-binary-data record (reference: exit(-2)) */
+  LAPH_ESIZE = 6,      /* record size does not match lattice (reference: exit(501)) */
+  LAPH_ESINGLE = 7,    /* single-precision ILDG payload (reference: "Not implemented") */
+  LAPH_ENOTCONV = 8,   /* eigensolver stopped at max_it before nev pairs converged */
+  LAPH_ETIMEOUT = 9,   /* a bounded device wait gave up */
+  LAPH_ETRACE = 10,    /* tr(V^dag V) / sum(V^dag V) check failed (reference check_trace) */
+  LAPH_EPARSE = 11,    /* parameters.txt line the reference parser cannot read */
+  LAPH_ENODEV = 12     /* no CUDA device */
+};
+const char* laph_strerror(int status);
+const char* laph_last_error(void);
+int laph_version(void);
+
+/* ---- link layouts accepted at the boundary -------------------------------- */
+enum {
+  LAPH_LAYOUT_ROWMAJOR = 0, /* double[V3][3][3][3][2]: [site][dir][a][b][re,im]                */
+  LAPH_LAYOUT_EIGEN = 1,    /* double[V3][3][9][2]: Matrix3cd memory (column-major 3x3),
+                               the order write_link_matrices_ts dumps (read_write.cpp:263-274) */
+  LAPH_LAYOUT_CONF = 2      /* one timeslice of the read_lime_gauge_field_doubleprec_timeslices
+                               buffer: double[V3][4][3][3][2], slot 0 = U_t, 1..3 = U_x..U_z
+                               (io.cpp:112-131, mapped as timeslice.cpp:34-79)              */
+};
+enum { LAPH_SMEAR_NONE = 0, LAPH_SMEAR_HYP = 1, LAPH_SMEAR_STOUT = 2, LAPH_SMEAR_APE = 3 };
+
+/* ---- single-timeslice context: the MatShell drop-in ------------------------
+ * Replaces the process-global IO/Nav/Tslice singletons the reference's
+ * MatMult_Laplacian2D reads (modules/shell_matop.cpp:9-11): one context holds
+ * one timeslice's links on one device, plus LAM_L, LAM_C and DEG.           */
+typedef struct laph_ctx laph_ctx;
+typedef struct {
+  int L;          /* spatial extent LX = LY = LZ (par_io.cpp:110-112)               */
+  double lam_l;   /* LAM_L, upper end of the Chebyshev window (shell_matop.cpp:18) */
+  double lam_c;   /* LAM_C, cut (shell_matop.cpp:19)                               */
+  int deg;        /* DEG, Chebyshev degree (shell_matop.cpp:143)                   */
+  int device;     /* CUDA device ordinal                                           */
+} laph_params;
+
+int laph_ctx_create(laph_ctx** ctx, const laph_params* p);
+int laph_ctx_destroy(laph_ctx* ctx);
+int laph_ctx_set_window(laph_ctx* ctx, double lam_l, double lam_c, int deg);
+
+/* Load one timeslice of links (host pointer, FP64).  Replaces
+ * Tslice::map_timeslice_to_eigen (modules/timeslice.cpp:34-79) for
+ * layout = LAPH_LAYOUT_CONF, and Tslice::set_gauge for the others. */
+int laph_set_links(laph_ctx* ctx, const double* links, int layout);
+/* Read the (smeared) links back, Tslice::get_gauge (timeslice.cpp:81-83). */
+int laph_get_links(laph_ctx* ctx, double* links, int layout);
+
+/* FP64 smearing on the device.  kind = LAPH_SMEAR_HYP: p1 = alpha_1, p2 = alpha_2
+ * (Tslice::smearing_hyp, timeslice.cpp:243-369); LAPH_SMEAR_STOUT: p1 = rho
+ * (smearing_stout, :145-193); LAPH_SMEAR_APE: p1 = alpha (smearing_ape, :196-239).
+ * compat = 1 keeps the reference's backward-staple factor U[nu][dir] of
+ * stout/APE (timeslice.cpp:171-172, :221-222); compat = 0 uses the
+ * gauge-covariant U[nu][not_dir].  HYP ignores compat (its staples are correct). */
+int laph_smear(laph_ctx* ctx, int kind, double p1, double p2, int iters, int compat);
+
+/* y = T_deg(B) x in FP64, B = c(hop - 6) + a, c = 2/(LAM_L - LAM_C),
+ * a = 1 + c LAM_C: the body of MatMult_Laplacian2D (shell_matop.cpp:136-168,
+ * :226-244).  deg >= 1 (deg = 1 gives B x).  x, y: complex128[3*V3];
+ * on_device = 0 for host pointers (staged), 1 for device pointers. */
+int laph_matmult(laph_ctx* ctx, const double* x, double* y, int deg, int on_device);
+/* y = (-Delta) x = 6x - hop(x) in FP64 (for residuals). */
+int laph_apply_neglap(laph_ctx* ctx, const double* x, double* y, int on_device);
+/* MatGetDiagonal_Laplacian2D (shell_matop.cpp:248-255): fills diag with -6. */
+int laph_get_diagonal(laph_ctx* ctx, double* diag, int on_device);
+/* Average spatial plaquette of the context's links (config_utils.cpp:388-426). */
+int laph_plaquette(laph_ctx* ctx, double* plaq);
+
+/* ---- batched block eigensolver (the "chosen" form) ------------------------
+ * Solves many timeslices (possibly of different L and nev) in one batched,
+ * device-resident Chebyshev-filtered subspace iteration: FP32 filter matvecs
+ * (links FP32 or BF16 + per-site scale), FP64 Gram/Cholesky/Rayleigh-Ritz and
+ * residuals.  Replaces, per timeslice, the body of the ev_ts loop
+ * (src/ev_ts.cpp:176-336): smearing, MatShell + EPSSolve, fix_phase,
+ * recover_spectrum. */
+enum { LAPH_WINDOW_FIXED = 0, LAPH_WINDOW_LANCZOS = 1, LAPH_WINDOW_MLP = 2 };
+enum { LAPH_LINKS_FP32 = 0, LAPH_LINKS_BF16 = 1 };
+
+typedef struct {
+  int L;             /* spatial extent of this timeslice                       */
+  int nev;           /* wanted eigenpairs                                      */
+} laph_problem;
+
+typedef struct {
+  int smear_kind;       /* LAPH_SMEAR_*                                          */
+  double smear_p1, smear_p2;
+  int smear_iters;
+  int smear_compat;
+  int guard;            /* block vectors beyond nev (>= 0; rounded up to a multiple of 8) */
+  int link_prec;        /* LAPH_LINKS_FP32 / LAPH_LINKS_BF16                      */
+  double tol;           /* target ||(-Delta)v - lambda v|| / (||v|| lambda_max)   */
+  int max_it;           /* outer iterations                                       */
+  int window;           /* LAPH_WINDOW_*                                          */
+  double lam_cut;       /* fixed window: cut (<= 0: from the first Rayleigh-Ritz) */
+  double lam_max;       /* fixed window: upper end (<= 0: Lanczos bound)          */
+  int deg;              /* filter degree (<= 0: default)                          */
+  int phase_fix;        /* apply fix_phase to the output eigenvectors             */
+  uint64_t seed;        /* start block                                            */
+} laph_solve_opts;
+void laph_solve_opts_default(laph_solve_opts* o);
+
+typedef struct {
+  int status;           /* LAPH_OK or LAPH_ENOTCONV                               */
+  int iters;            /* outer iterations used                                  */
+  int nconv;            /* converged wanted pairs                                 */
+  int deg;              /* filter degree used                                     */
+  double lam_cut0, lam_max;  /* initial window                                    */
+  double max_resid;     /* max over the nev wanted pairs                          */
+  double trace_vdv;     /* tr(V^dag V) of the returned eigenvectors               */
+} laph_result;
+
+typedef struct laph_solver laph_solver;
+/* Allocate a solver for n problems (device memory sized for all of them). */
+int laph_solver_create(laph_solver** s, const laph_problem* probs, int n, const laph_solve_opts* opts, int device);
+int laph_solver_destroy(laph_solver* s);
+/* Links of problem i: FP64, layout as above; host (on_device = 0) or device pointer. */
+int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout, int on_device);
+/* Run: smear + solve all problems.  Results stay on the device. */
+int laph_solver_run(laph_solver* s, laph_result* results);
+/* Fetch problem i: evals[nev] (reference convention, see top), evecs column-major
+ * complex128 [3*V3][nev] (may be NULL), phases[nev] (may be NULL). */
+int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double* phases, int on_device);
+/* Device-side timing of the last run (ms): smearing, filter, dense, total. */
+int laph_solver_timings(laph_solver* s, double* ms4);
+/* Counters of the last run for roofline accounting: filter site-vector-steps,
+ * number of filter kernel launches, total device kernel launches. */
+int laph_solver_counters(laph_solver* s, long long* c3);
+
+/* ---- host-side utilities (no device needed) ------------------------------ */
+/* Seeded synthetic gauge field U = exp(i eps H), H = sum_a c_a lambda_a with
+ * c_a ~ N(0,1) i.i.d. (Gell-Mann basis), for all 4 directions; output in the
+ * LAPH_LAYOUT_CONF order for nt timeslices: double[nt][V3][4][3][3][2]. */
+int laph_gauge_random(double* conf, int L, int nt, double eps, uint64_t seed);
+/* LIME/ILDG I/O.  The reader replaces read_lime_gauge_field_doubleprec_timeslices
+ * (modules/io.cpp:22-146): conf gets timeslices [t_i, t_f] in the order above.
+ * The writer emits ildg-format + ildg-binary-data records (big-endian FP64). */
+int laph_lime_write_gauge(const char* path, const double* conf, int L, int T);
+int laph_lime_read_gauge(const char* path, int T, int L, int t_i, int t_f, double* conf);
+/* write_eig_sys_bin / write_eigenvalues_bin (modules/read_write.cpp:176-250):
+ * "<dir>/<prefix>.%04d.%03d".  The eigenvector writer runs check_trace first
+ * and returns LAPH_ETRACE (nothing written) where the reference exits. */
+int laph_write_eigsys_bin(const char* dir, const char* prefix, int config, int t, int dim, int nev, const double* V);
+int laph_write_eigenvalues_bin(const char* dir, const char* prefix, int config, int t, int nev, const double* ev);
+int laph_read_eigsys_bin(const char* dir, const char* prefix, int config, int t, int dim, int nev, double* V);
+int laph_read_eigenvalues_bin(const char* dir, const char* prefix, int config, int t, int nev, double* ev);
+/* check_trace (read_write.cpp:20-35): 1 if |tr|-nev, |Im tr|, |sum|-nev, |Im sum| <= 1e-9. */
+int laph_check_trace(int dim, int nev, const double* V, double* trace, double* sum);
+/* fix_phase (modules/eigensystem.cpp:4-30) on host data. */
+int laph_fix_phase_host(int dim, int nev, const double* V, double* Vfix, double* phase);
+/* recover_spectrum (modules/recover_spec.cpp:45-54). */
+int laph_recover_spectrum(int nev, const double* theta, int deg, double lam_l, double lam_c, double* out);
+
+/* parameters.txt (modules/par_io.cpp:8-136), same key/value rules. */
+typedef struct {
+  char config_path[512], result_path[512], in_path[512], phase_path[512];
+  int LT, LX, NEV, iter, DEG, OMP_THRDS;
+  double alpha_1, alpha_2, LAM_L, LAM_C;
+  /* keys added by this library */
+  int smear;            /* LAPH_SMEAR_* (key "smear" = hyp|stout|ape|none; default hyp) */
+  double rho, alpha;    /* stout rho, APE alpha                                        */
+  double tol;           /* residual target                                             */
+  int guard, block, window, solver; /* solver: 0 = block (default), 1 = plain MatShell */
+  int V3, MAT_ENTRIES, V_TS;
+} laph_config;
+int laph_parse_parameters(const char* path, laph_config* cfg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,254 @@
+"""laph_eigsys_b200 -- B200 (sm_100a) implementation of the per-timeslice LapH
+eigensystem path of HISKP-LQCD/LapH_EigSys.
+
+The compute path is the CUDA library liblaph_gpu.so (C ABI: include/laph_gpu.h).
+This module is a thin Python mirror of that ABI for tests and benchmarks; the
+reference's own host interface (MatShell MatMult, parameters.txt, ev_ts) is the
+C++ layer in laph_eigsys_b200/host.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (LAYOUT_CONF, LAYOUT_EIGEN, LAYOUT_ROWMAJOR, LINKS_BF16, LINKS_FP32, SMEAR_APE, SMEAR_HYP,
+                   SMEAR_NONE, SMEAR_STOUT, WINDOW_FIXED, WINDOW_LANCZOS, WINDOW_MLP, LaphError, check, lib)
+
+__all__ = ["Context", "Solver", "gauge_random", "lime_write_gauge", "lime_read_gauge", "parse_parameters",
+           "check_trace", "fix_phase", "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin",
+           "read_eigsys_bin", "read_eigenvalues_bin", "LaphError", "lib"]
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _c128(a):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    return a
+
+
+def gauge_random(L, nt, eps, seed):
+    """Seeded U = exp(i eps H) links; array (nt, L^3, 4, 3, 3) complex128, slot 0 = U_t."""
+    conf = np.empty((nt, L ** 3, 4, 3, 3), dtype=np.complex128)
+    check(lib.laph_gauge_random(_ptr(conf), L, nt, eps, seed), "laph_gauge_random")
+    return conf
+
+
+def lime_write_gauge(path, conf, L, T):
+    conf = _c128(conf)
+    check(lib.laph_lime_write_gauge(str(path).encode(), _ptr(conf), L, T), "laph_lime_write_gauge")
+
+
+def lime_read_gauge(path, T, L, t_i, t_f):
+    conf = np.empty((t_f - t_i + 1, L ** 3, 4, 3, 3), dtype=np.complex128)
+    check(lib.laph_lime_read_gauge(str(path).encode(), T, L, t_i, t_f, _ptr(conf)), "laph_lime_read_gauge")
+    return conf
+
+
+def spatial_links(conf_ts):
+    """(V3, 4, 3, 3) conf timeslice -> (V3, 3, 3, 3) spatial links (map_timeslice_to_eigen)."""
+    return np.ascontiguousarray(np.asarray(conf_ts)[:, 1:4])
+
+
+def parse_parameters(path):
+    cfg = _lib.laph_config()
+    check(lib.laph_parse_parameters(str(path).encode(), ctypes.byref(cfg)), "laph_parse_parameters")
+    out = {}
+    for name, _ in cfg._fields_:
+        v = getattr(cfg, name)
+        out[name] = v.decode() if isinstance(v, bytes) else v
+    return out
+
+
+def check_trace(V):
+    V = np.asfortranarray(V, dtype=np.complex128)
+    dim, nev = V.shape
+    tr, sm = ctypes.c_double(), ctypes.c_double()
+    ok = lib.laph_check_trace(dim, nev, ctypes.c_void_p(V.ctypes.data), ctypes.byref(tr), ctypes.byref(sm))
+    return bool(ok), tr.value, sm.value
+
+
+def fix_phase(V):
+    V = np.asfortranarray(V, dtype=np.complex128)
+    dim, nev = V.shape
+    Vf = np.empty_like(V, order="F")
+    ph = np.empty(nev)
+    check(lib.laph_fix_phase_host(dim, nev, ctypes.c_void_p(V.ctypes.data), ctypes.c_void_p(Vf.ctypes.data),
+                                  _ptr(ph)), "laph_fix_phase_host")
+    return Vf, ph
+
+
+def recover_spectrum(theta, deg, lam_l, lam_c):
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    out = np.empty_like(theta)
+    check(lib.laph_recover_spectrum(len(theta), _ptr(theta), deg, lam_l, lam_c, _ptr(out)), "laph_recover_spectrum")
+    return out
+
+
+def write_eigsys_bin(dirname, prefix, config, t, V):
+    V = np.asfortranarray(V, dtype=np.complex128)
+    check(lib.laph_write_eigsys_bin(str(dirname).encode(), prefix.encode(), config, t, V.shape[0], V.shape[1],
+                                    ctypes.c_void_p(V.ctypes.data)), "laph_write_eigsys_bin")
+
+
+def write_eigenvalues_bin(dirname, prefix, config, t, ev):
+    ev = np.ascontiguousarray(ev, dtype=np.float64)
+    check(lib.laph_write_eigenvalues_bin(str(dirname).encode(), prefix.encode(), config, t, len(ev), _ptr(ev)),
+          "laph_write_eigenvalues_bin")
+
+
+def read_eigsys_bin(dirname, prefix, config, t, dim, nev):
+    V = np.empty((dim, nev), dtype=np.complex128, order="F")
+    check(lib.laph_read_eigsys_bin(str(dirname).encode(), prefix.encode(), config, t, dim, nev,
+                                   ctypes.c_void_p(V.ctypes.data)), "laph_read_eigsys_bin")
+    return V
+
+
+def read_eigenvalues_bin(dirname, prefix, config, t, nev):
+    ev = np.empty(nev)
+    check(lib.laph_read_eigenvalues_bin(str(dirname).encode(), prefix.encode(), config, t, nev, _ptr(ev)),
+          "laph_read_eigenvalues_bin")
+    return ev
+
+
+class Context:
+    """One timeslice on one device: the MatShell drop-in (laph_ctx)."""
+
+    def __init__(self, L, lam_l=11.8, lam_c=0.6, deg=8, device=0):
+        self.L, self.V3, self.dim = L, L ** 3, 3 * L ** 3
+        p = _lib.laph_params(L, lam_l, lam_c, deg, device)
+        h = ctypes.c_void_p()
+        check(lib.laph_ctx_create(ctypes.byref(h), ctypes.byref(p)), "laph_ctx_create")
+        self._h = h
+        self.deg = deg
+
+    def close(self):
+        if self._h:
+            lib.laph_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_window(self, lam_l, lam_c, deg):
+        check(lib.laph_ctx_set_window(self._h, lam_l, lam_c, deg), "laph_ctx_set_window")
+        self.deg = deg
+
+    def set_links(self, links, layout=LAYOUT_ROWMAJOR):
+        links = _c128(links)
+        check(lib.laph_set_links(self._h, _ptr(links), layout), "laph_set_links")
+
+    def get_links(self, layout=LAYOUT_ROWMAJOR):
+        shape = (self.V3, 4, 3, 3) if layout == LAYOUT_CONF else (self.V3, 3, 3, 3)
+        out = np.empty(shape, dtype=np.complex128)
+        check(lib.laph_get_links(self._h, _ptr(out), layout), "laph_get_links")
+        return out
+
+    def smear(self, kind, p1, p2, iters, compat=1):
+        check(lib.laph_smear(self._h, kind, p1, p2, iters, compat), "laph_smear")
+
+    def smearing_hyp(self, alpha_1, alpha_2, iters):
+        self.smear(SMEAR_HYP, alpha_1, alpha_2, iters, 0)
+
+    def smearing_stout(self, rho, iters, compat=1):
+        self.smear(SMEAR_STOUT, rho, 0.0, iters, compat)
+
+    def smearing_ape(self, alpha, iters, compat=1):
+        self.smear(SMEAR_APE, alpha, 0.0, iters, compat)
+
+    def matmult(self, x, deg=None):
+        x = _c128(x)
+        y = np.empty_like(x)
+        check(lib.laph_matmult(self._h, _ptr(x), _ptr(y), self.deg if deg is None else deg, 0), "laph_matmult")
+        return y
+
+    def matmult_device(self, x_ptr, y_ptr, deg=None):
+        check(lib.laph_matmult(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                               self.deg if deg is None else deg, 1), "laph_matmult")
+
+    def apply_neglap(self, x):
+        x = _c128(x)
+        y = np.empty_like(x)
+        check(lib.laph_apply_neglap(self._h, _ptr(x), _ptr(y), 0), "laph_apply_neglap")
+        return y
+
+    def get_diagonal(self):
+        d = np.empty(self.dim, dtype=np.complex128)
+        check(lib.laph_get_diagonal(self._h, _ptr(d), 0), "laph_get_diagonal")
+        return d
+
+    def plaquette(self):
+        p = ctypes.c_double()
+        check(lib.laph_plaquette(self._h, ctypes.byref(p)), "laph_plaquette")
+        return p.value
+
+
+def solve_opts(**kw):
+    o = _lib.laph_solve_opts()
+    lib.laph_solve_opts_default(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class Solver:
+    """Batched block eigensolver over many timeslices (laph_solver)."""
+
+    def __init__(self, problems, opts=None, device=0, **kw):
+        self.problems = [(int(L), int(nev)) for L, nev in problems]
+        arr = (_lib.laph_problem * len(self.problems))(*[_lib.laph_problem(L, n) for L, n in self.problems])
+        self.opts = opts if opts is not None else solve_opts(**kw)
+        h = ctypes.c_void_p()
+        check(lib.laph_solver_create(ctypes.byref(h), arr, len(self.problems), ctypes.byref(self.opts), device),
+              "laph_solver_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib.laph_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_links(self, i, links, layout=LAYOUT_ROWMAJOR):
+        links = _c128(links)
+        check(lib.laph_solver_set_links(self._h, i, _ptr(links), layout, 0), "laph_solver_set_links")
+
+    def set_links_device(self, i, ptr, layout=LAYOUT_ROWMAJOR):
+        check(lib.laph_solver_set_links(self._h, i, ctypes.c_void_p(ptr), layout, 1), "laph_solver_set_links")
+
+    def run(self):
+        res = (_lib.laph_result * len(self.problems))()
+        st = lib.laph_solver_run(self._h, res)
+        if st not in (_lib.LAPH_OK, _lib.LAPH_ENOTCONV):
+            check(st, "laph_solver_run")
+        return st, [dict((f, getattr(r, f)) for f, _ in r._fields_) for r in res]
+
+    def get(self, i, vectors=True):
+        L, nev = self.problems[i]
+        ev = np.empty(nev)
+        V = np.empty((3 * L ** 3, nev), dtype=np.complex128, order="F") if vectors else None
+        ph = np.empty(nev)
+        check(lib.laph_solver_get(self._h, i, _ptr(ev), ctypes.c_void_p(V.ctypes.data) if vectors else None,
+                                  _ptr(ph), 0), "laph_solver_get")
+        return ev, V, ph
+
+    def timings(self):
+        t = (ctypes.c_double * 4)()
+        check(lib.laph_solver_timings(self._h, t), "laph_solver_timings")
+        return list(t)
+
+    def counters(self):
+        c = (ctypes.c_longlong * 3)()
+        check(lib.laph_solver_counters(self._h, c), "laph_solver_counters")
+        return list(c)

@@ -1,0 +1,181 @@
+"""ctypes wrapper of the CPU FP64 oracle (oracle/liblaph_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py as the checker / timed CPU baseline, never by the
+product path.  Parity status: unpinned against reference outputs (the
+reference cannot be built here and ships no golden vectors); pinned by
+analytic known answers (see laph_oracle.h).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblaph_oracle.so")
+
+
+def build():
+    subprocess.run(["make", "-C", _HERE], check=True, stdout=subprocess.DEVNULL)
+
+
+if not os.path.exists(LIB_PATH):
+    build()
+
+_lib = ctypes.CDLL(LIB_PATH)
+_d, _i, _vp = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+
+
+_sig("orc_set_threads", None, _i)
+_sig("orc_lime_read_gauge", _i, ctypes.c_char_p, _i, _i, _i, _i, _vp)
+_sig("orc_map_timeslice", None, _vp, _i, _vp)
+_sig("orc_proj_su3", None, _vp)
+_sig("orc_expiH", None, _vp, _vp)
+_sig("orc_smear_stout", None, _vp, _i, _d, _i, _i)
+_sig("orc_smear_ape", None, _vp, _i, _d, _i, _i)
+_sig("orc_smear_hyp", None, _vp, _i, _d, _d, _i)
+_sig("orc_tv2", None, _vp, _i, _d, _d, _vp, _vp)
+_sig("orc_tv_iter", None, _vp, _i, _d, _d, _i, _vp, _vp)
+_sig("orc_neglap", None, _vp, _i, _vp, _vp)
+_sig("orc_plaquette", _d, _vp, _i)
+_sig("orc_eps_solve", _i, _vp, _i, _d, _d, _i, _i, _i, _d, _i, ctypes.c_uint64, _vp, _vp,
+     ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_longlong))
+_sig("orc_recover_spectrum", None, _i, _vp, _i, _d, _d, _vp)
+_sig("orc_fix_phase", None, _i, _i, _vp, _vp, _vp)
+_sig("orc_build_neglap_dense", None, _vp, _i, _vp)
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _links(U):
+    return np.ascontiguousarray(U, dtype=np.complex128).copy()
+
+
+def set_threads(n):
+    _lib.orc_set_threads(int(n))
+
+
+def lime_read_gauge(path, T, L, t_i, t_f):
+    conf = np.zeros((t_f - t_i + 1, L ** 3, 4, 3, 3), dtype=np.complex128)
+    st = _lib.orc_lime_read_gauge(str(path).encode(), T, L, t_i, t_f, _p(conf))
+    return st, conf
+
+
+def map_timeslice(conf_ts, L):
+    conf_ts = np.ascontiguousarray(conf_ts, dtype=np.complex128)
+    out = np.empty((L ** 3, 3, 3, 3), dtype=np.complex128)
+    _lib.orc_map_timeslice(_p(conf_ts), L, _p(out))
+    return out
+
+
+def proj_su3(m):
+    m = np.ascontiguousarray(m, dtype=np.complex128).copy()
+    _lib.orc_proj_su3(_p(m))
+    return m
+
+
+def expiH(h):
+    h = np.ascontiguousarray(h, dtype=np.complex128)
+    out = np.empty((3, 3), dtype=np.complex128)
+    _lib.orc_expiH(_p(h), _p(out))
+    return out
+
+
+def smear_stout(U, L, rho, iters, compat=1):
+    U = _links(U)
+    _lib.orc_smear_stout(_p(U), L, rho, iters, compat)
+    return U
+
+
+def smear_ape(U, L, alpha, iters, compat=1):
+    U = _links(U)
+    _lib.orc_smear_ape(_p(U), L, alpha, iters, compat)
+    return U
+
+
+def smear_hyp(U, L, a1, a2, iters):
+    U = _links(U)
+    _lib.orc_smear_hyp(_p(U), L, a1, a2, iters)
+    return U
+
+
+def tv2(U, L, lam_l, lam_c, x):
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    y = np.zeros_like(x)
+    _lib.orc_tv2(_p(U), L, lam_l, lam_c, _p(x), _p(y))
+    return y
+
+
+def tv_iter(U, L, lam_l, lam_c, deg, x, y=None):
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    y = np.zeros_like(x) if y is None else np.ascontiguousarray(y, dtype=np.complex128).copy()
+    _lib.orc_tv_iter(_p(U), L, lam_l, lam_c, deg, _p(x), _p(y))
+    return y
+
+
+def neglap(U, L, x):
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    y = np.zeros_like(x)
+    _lib.orc_neglap(_p(U), L, _p(x), _p(y))
+    return y
+
+
+def plaquette(U, L):
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    return _lib.orc_plaquette(_p(U), L)
+
+
+def eps_solve(U, L, lam_l, lam_c, deg, nev, ncv=0, tol=1e-12, max_it=200, seed=1227):
+    """SLEPc-style Krylov-Schur on T_deg(B), largest magnitude.  Returns
+    (status, theta[nev], V (dim x nev, column-major), nconv, its, nmatvec)."""
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    dim = 3 * L ** 3
+    theta = np.zeros(nev)
+    V = np.zeros((dim, nev), dtype=np.complex128, order="F")
+    nconv, its, nmv = _i(), _i(), ctypes.c_longlong()
+    st = _lib.orc_eps_solve(_p(U), L, lam_l, lam_c, deg, nev, ncv, tol, max_it, seed, _p(theta),
+                            ctypes.c_void_p(V.ctypes.data), ctypes.byref(nconv), ctypes.byref(its), ctypes.byref(nmv))
+    return st, theta, V, nconv.value, its.value, nmv.value
+
+
+def recover_spectrum(theta, deg, lam_l, lam_c):
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    out = np.empty_like(theta)
+    _lib.orc_recover_spectrum(len(theta), _p(theta), deg, lam_l, lam_c, _p(out))
+    return out
+
+
+def fix_phase(V):
+    V = np.asfortranarray(V, dtype=np.complex128)
+    dim, nev = V.shape
+    Vf = np.empty_like(V, order="F")
+    ph = np.empty(nev)
+    _lib.orc_fix_phase(dim, nev, ctypes.c_void_p(V.ctypes.data), ctypes.c_void_p(Vf.ctypes.data), _p(ph))
+    return Vf, ph
+
+
+def neglap_dense(U, L):
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    dim = 3 * L ** 3
+    A = np.zeros((dim, dim), dtype=np.complex128)
+    _lib.orc_build_neglap_dense(_p(U), L, _p(A))
+    return A
+
+
+def free_spectrum(L):
+    """Analytic spectrum of -Delta for U = 1: sum_i 4 sin^2(pi n_i / L), x3 colours."""
+    k = 4.0 * np.sin(np.pi * np.arange(L) / L) ** 2
+    ev = (k[:, None, None] + k[None, :, None] + k[None, None, :]).ravel()
+    return np.sort(np.repeat(ev, 3))

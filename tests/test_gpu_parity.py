@@ -1,0 +1,87 @@
+"""CUDA path vs the FP64 oracle: smearing (<= 1e-12 relative per link) and the
+MatShell MatMult body T_deg(B) x (<= 1e-13 relative), through the C ABI."""
+import numpy as np
+import pytest
+
+from conftest import random_links, unit_links
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_link_err(A, B):
+    a = A.reshape(-1, 9)
+    b = B.reshape(-1, 9)
+    return (np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)).max()
+
+
+@pytest.mark.parametrize("L", [4, 6, 8])
+@pytest.mark.parametrize("kind,p1,p2,it,compat", [
+    ("stout", 0.1, 0.0, 3, 1), ("stout", 0.1, 0.0, 5, 0), ("ape", 0.5, 0.0, 3, 1), ("ape", 0.5, 0.0, 2, 0),
+    ("hyp", 0.62, 0.52, 3, 0), ("hyp", 0.62, 0.62, 1, 0)])
+def test_smearing_parity(gpu, orc, L, kind, p1, p2, it, compat):
+    U = random_links(L, 0.4, 1227 + L)
+    ctx = gpu.Context(L)
+    ctx.set_links(U)
+    if kind == "stout":
+        ctx.smearing_stout(p1, it, compat)
+        ref = orc.smear_stout(U, L, p1, it, compat)
+    elif kind == "ape":
+        ctx.smearing_ape(p1, it, compat)
+        ref = orc.smear_ape(U, L, p1, it, compat)
+    else:
+        ctx.smearing_hyp(p1, p2, it)
+        ref = orc.smear_hyp(U, L, p1, p2, it)
+    got = ctx.get_links()
+    assert rel_link_err(got, ref) <= 1e-12
+    ctx.close()
+
+
+def test_link_layouts_roundtrip(gpu):
+    L = 4
+    U = random_links(L, 0.4, 9)
+    ctx = gpu.Context(L)
+    ctx.set_links(U, gpu.LAYOUT_ROWMAJOR)
+    E = ctx.get_links(gpu.LAYOUT_EIGEN)
+    assert np.array_equal(E, np.transpose(U, (0, 1, 3, 2)))
+    ctx.set_links(E, gpu.LAYOUT_EIGEN)
+    assert np.array_equal(ctx.get_links(), U)
+    conf = gpu.gauge_random(L, 1, 0.4, 3)[0]
+    ctx.set_links(conf, gpu.LAYOUT_CONF)
+    assert np.array_equal(ctx.get_links(), conf[:, 1:4])
+
+
+@pytest.mark.parametrize("L", [4, 8, 12])
+@pytest.mark.parametrize("deg", [1, 2, 3, 8, 12])
+def test_matmult_parity(gpu, orc, L, deg):
+    U = orc.smear_hyp(random_links(L, 0.4, 1300 + L), L, 0.62, 0.52, 1)
+    lam_l, lam_c = 11.8, 0.6
+    ctx = gpu.Context(L, lam_l, lam_c, deg)
+    ctx.set_links(U)
+    rng = np.random.default_rng(L * 100 + deg)
+    x = rng.normal(size=3 * L ** 3) + 1j * rng.normal(size=3 * L ** 3)
+    y = ctx.matmult(x)
+    ref = orc.tv2(U, L, lam_l, lam_c, x) if deg == 1 else orc.tv_iter(U, L, lam_l, lam_c, deg, x)
+    assert np.linalg.norm(y - ref) / np.linalg.norm(ref) <= 1e-13
+    ctx.close()
+
+
+def test_neglap_diag_plaquette(gpu, orc):
+    L = 6
+    U = random_links(L, 0.4, 77)
+    ctx = gpu.Context(L)
+    ctx.set_links(U)
+    rng = np.random.default_rng(1)
+    x = rng.normal(size=3 * L ** 3) + 1j * rng.normal(size=3 * L ** 3)
+    y = ctx.apply_neglap(x)
+    ref = orc.neglap(U, L, x)
+    assert np.linalg.norm(y - ref) / np.linalg.norm(ref) <= 1e-14
+    assert np.all(ctx.get_diagonal() == -6.0)
+    assert abs(ctx.plaquette() - orc.plaquette(U, L)) < 1e-13
+    ctx.set_links(unit_links(L))
+    assert abs(ctx.plaquette() - 1.0) < 1e-15
+
+
+def test_matmult_rejects_bad_window(gpu):
+    ctx = gpu.Context(4, 1.0, 2.0, 8)
+    with pytest.raises(gpu.LaphError):
+        ctx.matmult(np.zeros(3 * 64, dtype=np.complex128))

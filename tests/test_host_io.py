@@ -1,0 +1,146 @@
+"""Host-side product logic on CPU: LIME/ILDG I/O against the oracle restatement
+of read_lime_gauge_field_doubleprec_timeslices, eigensystem files and
+check_trace, parameters.txt quirks, recover_spectrum / fix_phase."""
+import os
+import struct
+
+import numpy as np
+import pytest
+
+import laph_eigsys_b200 as lb
+from laph_eigsys_b200 import _lib
+
+
+def test_lime_roundtrip_matches_oracle_reader(tmp_path, orc):
+    L, T = 4, 6
+    conf = lb.gauge_random(L, T, 0.4, 1227)
+    p = tmp_path / "conf.1227"
+    lb.lime_write_gauge(p, conf, L, T)
+    assert os.path.getsize(p) > T * L ** 3 * 72 * 8
+    got = lb.lime_read_gauge(p, T, L, 0, T - 1)
+    assert np.array_equal(got, conf)
+    sub = lb.lime_read_gauge(p, T, L, 2, 4)
+    st, ref = orc.lime_read_gauge(p, T, L, 2, 4)
+    assert st == 0
+    assert np.array_equal(sub, ref) and np.array_equal(sub, conf[2:5])
+    # map_timeslice_to_eigen == spatial slots 1..3
+    assert np.array_equal(orc.map_timeslice(conf[3], L), lb.spatial_links(conf[3]))
+
+
+def test_lime_file_layout_is_big_endian_ildg(tmp_path):
+    L, T = 3, 2
+    conf = lb.gauge_random(L, T, 0.4, 5)
+    p = tmp_path / "c"
+    lb.lime_write_gauge(p, conf, L, T)
+    raw = open(p, "rb").read()
+    assert raw[:4] == bytes([0x45, 0x67, 0x89, 0xab])
+    # locate the binary record: header magic + type
+    i = raw.index(b"ildg-binary-data") - 16
+    n = struct.unpack(">Q", raw[i + 8:i + 16])[0]
+    assert n == L ** 3 * T * 72 * 8
+    data = raw[i + 144:i + 144 + n]
+    # first site (t=0,z=0,y=0,x=0), mu=x first -> conf slot 1, element (0,0)
+    re0, im0 = struct.unpack(">dd", data[:16])
+    assert re0 == conf[0, 0, 1, 0, 0].real and im0 == conf[0, 0, 1, 0, 0].imag
+    # second site in file order is x=1 -> site index 1*L*L
+    re1 = struct.unpack(">d", data[72 * 8:72 * 8 + 8])[0]
+    assert re1 == conf[0, L * L, 1, 0, 0].real
+
+
+def _lime_record(typ, payload, mb=True, me=True):
+    h = bytearray(144)
+    h[0:4] = bytes([0x45, 0x67, 0x89, 0xab])
+    h[4:6] = (1).to_bytes(2, "big")
+    h[6:8] = ((0x8000 if mb else 0) | (0x4000 if me else 0)).to_bytes(2, "big")
+    h[8:16] = len(payload).to_bytes(8, "big")
+    h[16:16 + len(typ)] = typ.encode()
+    pad = (-len(payload)) % 8
+    return bytes(h) + payload + b"\0" * pad
+
+
+@pytest.mark.parametrize("case,status,ref_status", [
+    ("missing", _lib.LAPH_EIO, 500),
+    ("norecord", _lib.LAPH_ENORECORD, -2),
+    ("badsize", _lib.LAPH_ESIZE, 501),
+    ("single", _lib.LAPH_ESINGLE, 502),
+    ("truncated", _lib.LAPH_EIO, 500),
+])
+def test_lime_error_paths(tmp_path, orc, case, status, ref_status):
+    L, T = 3, 2
+    p = tmp_path / "bad"
+    full = L ** 3 * T * 72 * 8
+    if case == "norecord":
+        p.write_bytes(_lime_record("ildg-format", b"<xml/>"))
+    elif case == "badsize":
+        p.write_bytes(_lime_record("ildg-binary-data", b"\0" * 800))
+    elif case == "single":
+        p.write_bytes(_lime_record("ildg-binary-data", b"\0" * (full // 2)))
+    elif case == "truncated":
+        rec = _lime_record("ildg-binary-data", b"\0" * full)
+        p.write_bytes(rec[:144 + full // 3])
+    with pytest.raises(lb.LaphError) as e:
+        lb.lime_read_gauge(p, T, L, 0, T - 1)
+    assert e.value.status == status
+    st, _ = orc.lime_read_gauge(p, T, L, 0, T - 1)
+    assert st == ref_status
+
+
+def test_eigsys_files_and_check_trace(tmp_path):
+    rng = np.random.default_rng(0)
+    dim, nev = 96, 7
+    A = rng.normal(size=(dim, nev)) + 1j * rng.normal(size=(dim, nev))
+    Q, _ = np.linalg.qr(A)
+    Q = np.asfortranarray(Q)
+    ok, tr, sm = lb.check_trace(Q)
+    VdV = Q.conj().T @ Q
+    assert abs(tr - np.trace(VdV).real) < 1e-12 and abs(sm - VdV.sum().real) < 1e-12
+    lb.write_eigsys_bin(tmp_path, "eigenvectors", 1227, 5, Q)
+    raw = open(tmp_path / "eigenvectors.1227.005", "rb").read()
+    assert raw == Q.tobytes(order="F")
+    assert np.array_equal(lb.read_eigsys_bin(tmp_path, "eigenvectors", 1227, 5, dim, nev), Q)
+    ev = np.linspace(-1, 0, nev)
+    lb.write_eigenvalues_bin(tmp_path, "eigenvalues", 1227, 5, ev)
+    assert open(tmp_path / "eigenvalues.1227.005", "rb").read() == ev.tobytes()
+    # damaged eigenvectors: nothing is written (the reference exits)
+    bad = Q * 1.01
+    with pytest.raises(lb.LaphError) as e:
+        lb.write_eigsys_bin(tmp_path, "eigenvectors", 1227, 6, bad)
+    assert e.value.status == _lib.LAPH_ETRACE
+    assert not (tmp_path / "eigenvectors.1227.006").exists()
+
+
+def test_parameters_parser_quirks(tmp_path):
+    p = tmp_path / "parameters.txt"
+    p.write_text("# comment\nconfig_path = /gauges\nLT = 48\nLX = 24\nNEV = 120\nalpha_1 = 0.62\n"
+                 "alpha_2 = 0.52\niter = 3\nLAM_L = 11.8\nLAM_C = 0.6\nDEG = 8\nOMP_THRDS = 2\n"
+                 "LT=99\nsmear = stout\nDEG = 12")  # unterminated last line is dropped
+    c = lb.parse_parameters(p)
+    assert c["config_path"] == "/gauges" and c["LT"] == 48 and c["LX"] == 24 and c["NEV"] == 120
+    assert c["DEG"] == 8 and c["iter"] == 3 and abs(c["LAM_L"] - 11.8) < 1e-15
+    assert c["V3"] == 24 ** 3 and c["MAT_ENTRIES"] == 3 * 24 ** 3 and c["V_TS"] == 72 * 24 ** 3
+    assert c["smear"] == lb.SMEAR_STOUT
+    p.write_text("LT = 4\n\nLX = 4\n")
+    with pytest.raises(lb.LaphError) as e:
+        lb.parse_parameters(p)
+    assert e.value.status == _lib.LAPH_EPARSE
+
+
+def test_recover_spectrum_and_fix_phase(orc):
+    theta = np.array([50.0, 3.0, 1.2, 1.0])
+    assert np.allclose(lb.recover_spectrum(theta, 8, 11.8, 0.6), orc.recover_spectrum(theta, 8, 11.8, 0.6),
+                       rtol=0, atol=1e-15)
+    rng = np.random.default_rng(1)
+    V = rng.normal(size=(30, 4)) + 1j * rng.normal(size=(30, 4))
+    a, pa = lb.fix_phase(V)
+    b, pb = orc.fix_phase(V)
+    assert np.abs(a - b).max() < 1e-15 and np.array_equal(pa, pb)
+
+
+def test_gauge_random_deterministic_and_seeded():
+    a = lb.gauge_random(3, 2, 0.3, 11)
+    b = lb.gauge_random(3, 2, 0.3, 11)
+    c = lb.gauge_random(3, 2, 0.3, 12)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    # eps = 0 gives the unit field
+    u = lb.gauge_random(3, 1, 0.0, 1)
+    assert np.abs(u - np.eye(3)).max() < 1e-14
