@@ -1,0 +1,639 @@
+// dense.cu -- FP64 dense block operations of the batched solver:
+//   k_gram        [G | H] = W^H [W | Y]  (partials over row chunks)
+//   k_gram_reduce fixed-order sum of the partials, Hermitian completion
+//   k_small       per problem: column scaling, Cholesky, triangular inverse,
+//                 projected Hermitian matrix, Jacobi eigensolve, sort, C,
+//                 next Chebyshev window and coefficient table
+//   k_rotate      V = W C,  R = Y C - V diag(theta),  S = s_j R (FP32),
+//                 residual partial sums
+//   k_resid       residual norms, convergence mask
+// These replace SLEPc's BV orthogonalisation and DS dense eigensolve inside
+// EPSSolve (src/ev_ts.cpp:263).  Complex FP64 on CUDA cores: B200 has no FP64
+// kind for tcgen05, and its FP64 DMMA rate equals its FP64 FMA rate.
+#include "batch.cuh"
+#include "dense.cuh"
+
+namespace laph {
+
+// ------------------------------------------------------------------ Gram ---
+// CTA: 64 threads, output tile 32x32 (thread: 4x4 complex), rows of one chunk.
+constexpr int GT = 32, GK = 16;
+
+__global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
+                                             const int* __restrict__ start, int np, int chunk_rows,
+                                             const double2* __restrict__ W, const double2* __restrict__ Y,
+                                             double2* __restrict__ gpart) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int T = d.k / GT;
+  const int npair = T * (T + 1) / 2;
+  int t = blockIdx.x - start[p];
+  const int chunk = t / (2 * npair);
+  t -= chunk * 2 * npair;
+  const int which = t / npair;  // 0: G = W^H W, 1: H = W^H Y
+  int pr = t - which * npair;
+  int ti = 0;
+  while (pr >= T - ti) {
+    pr -= T - ti;
+    ++ti;
+  }
+  const int tj = ti + pr;
+  const double2* A = W + d.blk + (size_t)(ti * GT) * d.dim;
+  const double2* B = (which ? Y : W) + d.blk + (size_t)(tj * GT) * d.dim;
+  const int r0 = chunk * chunk_rows, r1 = min(d.dim, r0 + chunk_rows);
+  __shared__ double2 sA[GK][GT + 1], sB[GK][GT + 1];
+  const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
+  double2 acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = make_double2(0.0, 0.0);
+  for (int r = r0; r < r1; r += GK) {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int idx = threadIdx.x + 64 * e;
+      const int c = idx >> 4, q = idx & 15;
+      const int row = r + q;
+      const bool ok = row < r1;
+      sA[q][c] = ok ? __ldg(A + (size_t)c * d.dim + row) : make_double2(0.0, 0.0);
+      sB[q][c] = ok ? __ldg(B + (size_t)c * d.dim + row) : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < GK; ++q) {
+      double2 a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = sA[q][ty + 8 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = sB[q][tx + 8 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cfmac(acc[i][j], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+  double2* out = gpart + d.gp + ((size_t)(chunk * 2 + which) * npair + (t - which * npair)) * (GT * GT);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[(ty + 8 * i) * GT + tx + 8 * j] = acc[i][j];
+}
+
+// Sum partials (fixed order) and complete the Hermitian matrices G, H
+// (column-major k x k at kk and kk + k*k).
+__global__ void k_gram_reduce(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
+                              const int* __restrict__ start, int np, const double2* __restrict__ gpart,
+                              double2* __restrict__ GH) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int T = d.k / GT, npair = T * (T + 1) / 2;
+  const int e = (blockIdx.x - start[p]) * blockDim.x + threadIdx.x;
+  if (e >= 2 * npair * GT * GT) return;
+  const int tile = e / (GT * GT), w = e - tile * GT * GT;
+  const int which = tile / npair;
+  int pr = tile - which * npair, ti = 0;
+  while (pr >= T - ti) {
+    pr -= T - ti;
+    ++ti;
+  }
+  const int tj = ti + pr;
+  double2 s = make_double2(0.0, 0.0);
+  for (int c = 0; c < d.nchunk; ++c) s = cadd(s, gpart[d.gp + ((size_t)(c * 2 + which) * npair + tile - which * npair) * (GT * GT) + w]);
+  const int i = ti * GT + w / GT, j = tj * GT + w % GT;
+  double2* M = GH + d.kk + (size_t)which * d.k * d.k;
+  if (ti == tj) {
+    // diagonal tile holds both triangles; keep the upper one and mirror it
+    if (i <= j) {
+      if (i == j) s.y = 0.0;
+      M[i + (size_t)j * d.k] = s;
+      M[j + (size_t)i * d.k] = cconj(s);
+    }
+  } else {
+    M[i + (size_t)j * d.k] = s;
+    M[j + (size_t)i * d.k] = cconj(s);
+  }
+}
+
+// ------------------------------------------------------------ small dense --
+// One CTA (1024 threads) per active problem.  Work arrays (column-major k x k)
+// at kk: [0] G -> C, [1] H, [2] Minv, [3] T1 / Q, [4] Ht.
+__device__ __forceinline__ double2& at(double2* M, int k, int i, int j) { return M[i + (size_t)j * k]; }
+
+__global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd, ProbState* __restrict__ ps,
+                                                double2* __restrict__ KK, double* __restrict__ theta,
+                                                double* __restrict__ tcoef, double* __restrict__ scol,
+                                                double* __restrict__ dwork, int first_iter, int fixed_cut,
+                                                int max_sweeps) {
+  const int p = blockIdx.x;
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int k = d.k, tid = threadIdx.x, nt = blockDim.x;
+  const size_t kk2 = (size_t)k * k;
+  double2* G = KK + d.kk;
+  double2* H = G + kk2;
+  double2* Mi = G + 2 * kk2;
+  double2* Q = G + 3 * kk2;
+  double2* Ht = G + 4 * kk2;
+  double* dinv = dwork + d.kv * 4;  // 4 k-length scratch vectors per problem
+  double* lam = dinv + k;
+  int* perm = reinterpret_cast<int*>(lam + k);
+  __shared__ int s_flag;
+  __shared__ double s_red[32];
+
+  // (a) column scaling D = sqrt(diag G)
+  for (int i = tid; i < k; i += nt) {
+    const double g = G[i + (size_t)i * k].x;
+    dinv[i] = g > 0.0 ? 1.0 / sqrt(g) : 1.0;
+  }
+  if (tid == 0) s_flag = 0;
+  __syncthreads();
+  for (size_t e = tid; e < kk2; e += nt) {
+    const int i = (int)(e % k), j = (int)(e / k);
+    G[e] = cscal(G[e], dinv[i] * dinv[j]);
+  }
+  __syncthreads();
+  // (b) Cholesky G = R^H R, R upper, in place (right-looking)
+  for (int q = 0; q < k; ++q) {
+    if (tid == 0) {
+      double piv = at(G, k, q, q).x;
+      if (!(piv > 1e-28)) {
+        piv = 1e-28;
+        s_flag = 1;
+      }
+      at(G, k, q, q) = make_double2(sqrt(piv), 0.0);
+    }
+    __syncthreads();
+    const double rinv = 1.0 / at(G, k, q, q).x;
+    for (int j = q + 1 + tid; j < k; j += nt) at(G, k, q, j) = cscal(at(G, k, q, j), rinv);
+    __syncthreads();
+    const int m = k - q - 1;
+    for (int e = tid; e < m * m; e += nt) {
+      const int i = q + 1 + e / m, j = q + 1 + e % m;
+      if (i <= j) {
+        double2 v = at(G, k, i, j);
+        const double2 a = at(G, k, q, i), b = at(G, k, q, j);
+        // v -= conj(a) b
+        v.x -= a.x * b.x + a.y * b.y;
+        v.y -= a.x * b.y - a.y * b.x;
+        at(G, k, i, j) = v;
+      }
+    }
+    __syncthreads();
+  }
+  // (c) Minv = D^{-1} R^{-1} (upper triangular), column by column
+  for (size_t e = tid; e < kk2; e += nt) Mi[e] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    const double rjj = at(G, k, j, j).x;
+    for (int i = tid; i <= j; i += nt) {
+      double2 s = make_double2(i == j ? 1.0 : 0.0, 0.0);
+      for (int q = i; q < j; ++q) {
+        // s -= Rinv(i,q) R(q,j)
+        const double2 a = at(Mi, k, i, q), b = at(G, k, q, j);
+        s.x -= a.x * b.x - a.y * b.y;
+        s.y -= a.x * b.y + a.y * b.x;
+      }
+      at(Mi, k, i, j) = cscal(s, 1.0 / rjj);
+    }
+    __syncthreads();
+  }
+  for (size_t e = tid; e < kk2; e += nt) {
+    const int i = (int)(e % k);
+    Mi[e] = cscal(Mi[e], dinv[i]);
+  }
+  __syncthreads();
+  // (d) T1 = H Minv ; Ht = Minv^H T1 (Hermitian part)
+  for (size_t e = tid; e < kk2; e += nt) {
+    const int i = (int)(e % k), j = (int)(e / k);
+    double2 s = make_double2(0.0, 0.0);
+    for (int q = 0; q <= j; ++q) cfma(s, at(H, k, i, q), at(Mi, k, q, j));
+    Q[e] = s;
+  }
+  __syncthreads();
+  for (size_t e = tid; e < kk2; e += nt) {
+    const int i = (int)(e % k), j = (int)(e / k);
+    double2 s = make_double2(0.0, 0.0);
+    for (int q = 0; q <= i; ++q) cfmac(s, at(Mi, k, q, i), at(Q, k, q, j));
+    Ht[e] = s;
+  }
+  __syncthreads();
+  for (size_t e = tid; e < kk2; e += nt) {
+    const int i = (int)(e % k), j = (int)(e / k);
+    if (i < j) {
+      const double2 a = at(Ht, k, i, j), b = at(Ht, k, j, i);
+      const double2 h = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+      at(Ht, k, i, j) = h;
+      at(Ht, k, j, i) = cconj(h);
+    } else if (i == j) {
+      at(Ht, k, i, i).y = 0.0;
+    }
+    Q[e] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  // (e) cyclic Jacobi, round-robin ordering of k/2 disjoint pairs per step
+  __shared__ double s_c[512], s_s[512];
+  __shared__ double2 s_e[512];
+  __shared__ int s_p[512], s_q[512];
+  const int half = k / 2;
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (size_t e = tid; e < kk2; e += nt) {
+      const int i = (int)(e % k), j = (int)(e / k);
+      const double2 v = Ht[e];
+      if (i != j) off += v.x * v.x + v.y * v.y;
+      else dia += v.x * v.x;
+    }
+    // block reduce off and dia
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      dia += __shfl_xor_sync(0xffffffffu, dia, o);
+    }
+    __shared__ double s_off[32], s_dia[32];
+    if ((tid & 31) == 0) {
+      s_off[tid >> 5] = off;
+      s_dia[tid >> 5] = dia;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < (nt >> 5); ++w) {
+        a += s_off[w];
+        b += s_dia[w];
+      }
+      s_red[0] = a;
+      s_red[1] = b;
+    }
+    __syncthreads();
+    if (s_red[0] <= 1e-30 * s_red[1]) break;
+    for (int step = 0; step < k - 1; ++step) {
+      for (int r = tid; r < half; r += nt) {
+        auto rot = [&](int pos) { return ((pos - 1 + step) % (k - 1)) + 1; };
+        const int pp = (r == 0) ? 0 : rot(r);
+        const int qq = rot(k - 1 - r);
+        const int pa = min(pp, qq), qb = max(pp, qq);
+        const double2 g = at(Ht, k, pa, qb);
+        const double rr = hypot(g.x, g.y);
+        const double app = at(Ht, k, pa, pa).x, aqq = at(Ht, k, qb, qb).x;
+        double c = 1.0, s = 0.0;
+        double2 em = make_double2(1.0, 0.0);
+        if (rr > 1e-300 && rr > 1e-18 * sqrt(fabs(app * aqq))) {
+          em = make_double2(g.x / rr, -g.y / rr);  // e^{-i phi}
+          const double tau = (aqq - app) / (2.0 * rr);
+          const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          c = 1.0 / sqrt(1.0 + tt * tt);
+          s = tt * c;
+        }
+        s_p[r] = pa;
+        s_q[r] = qb;
+        s_c[r] = c;
+        s_s[r] = s;
+        s_e[r] = em;
+      }
+      __syncthreads();
+      // columns: H <- H J ; Q <- Q J.  J: (p,p)=c (p,q)=s (q,p)=-s e (q,q)=c e, e = e^{-i phi}
+      for (int e = tid; e < half * k; e += nt) {
+        const int r = e / k, i = e - r * k;
+        const int pa = s_p[r], qb = s_q[r];
+        const double c = s_c[r], s = s_s[r];
+        if (s == 0.0) continue;
+        const double2 em = s_e[r];
+        const double2 hp = at(Ht, k, i, pa), hq = at(Ht, k, i, qb);
+        const double2 hqe = cmul(hq, em);
+        at(Ht, k, i, pa) = make_double2(c * hp.x - s * hqe.x, c * hp.y - s * hqe.y);
+        at(Ht, k, i, qb) = make_double2(s * hp.x + c * hqe.x, s * hp.y + c * hqe.y);
+        const double2 qp = at(Q, k, i, pa), qq = at(Q, k, i, qb);
+        const double2 qqe = cmul(qq, em);
+        at(Q, k, i, pa) = make_double2(c * qp.x - s * qqe.x, c * qp.y - s * qqe.y);
+        at(Q, k, i, qb) = make_double2(s * qp.x + c * qqe.x, s * qp.y + c * qqe.y);
+      }
+      __syncthreads();
+      // rows: H <- J^H H.  J^H: (p,p)=c (p,q)=-s conj(e) (q,p)=s (q,q)=c conj(e)
+      for (int e = tid; e < half * k; e += nt) {
+        const int r = e / k, j = e - r * k;
+        const int pa = s_p[r], qb = s_q[r];
+        const double c = s_c[r], s = s_s[r];
+        if (s == 0.0) continue;
+        const double2 ep = cconj(s_e[r]);
+        const double2 hp = at(Ht, k, pa, j), hq = at(Ht, k, qb, j);
+        const double2 hqe = cmul(hq, ep);
+        at(Ht, k, pa, j) = make_double2(c * hp.x - s * hqe.x, c * hp.y - s * hqe.y);
+        at(Ht, k, qb, j) = make_double2(s * hp.x + c * hqe.x, s * hp.y + c * hqe.y);
+      }
+      __syncthreads();
+      for (int r = tid; r < half; r += nt) {
+        if (s_s[r] == 0.0) continue;
+        const int pa = s_p[r], qb = s_q[r];
+        at(Ht, k, pa, qb) = make_double2(0.0, 0.0);
+        at(Ht, k, qb, pa) = make_double2(0.0, 0.0);
+        at(Ht, k, pa, pa).y = 0.0;
+        at(Ht, k, qb, qb).y = 0.0;
+      }
+      __syncthreads();
+    }
+  }
+  // (f) sort ascending (rank sort, ties by index)
+  for (int i = tid; i < k; i += nt) lam[i] = at(Ht, k, i, i).x;
+  __syncthreads();
+  for (int i = tid; i < k; i += nt) {
+    const double li = lam[i];
+    int r = 0;
+    for (int j = 0; j < k; ++j) {
+      const double lj = lam[j];
+      r += (lj < li) || (lj == li && j < i);
+    }
+    perm[r] = i;
+  }
+  __syncthreads();
+  double* th = theta + d.kv;
+  for (int r = tid; r < k; r += nt) th[r] = lam[perm[r]];
+  // (g) C = Minv Q[:, perm] -> G storage
+  for (size_t e = tid; e < kk2; e += nt) {
+    const int i = (int)(e % k), j = (int)(e / k);
+    const int pj = perm[j];
+    double2 s = make_double2(0.0, 0.0);
+    for (int q = i; q < k; ++q) cfma(s, at(Mi, k, i, q), at(Q, k, q, pj));
+    G[e] = s;
+  }
+  __syncthreads();
+  // (h) next window [lam_cut, lam_max] and Chebyshev coefficients
+  if (tid == 0) {
+    ProbState& S = ps[p];
+    double cut = th[k - 1];
+    if (fixed_cut || (first_iter && S.lam_cut > 0.0)) cut = S.lam_cut;
+    if (cut >= S.lam_max - 1e-3) cut = S.lam_max - 1e-3;
+    if (cut < 1e-6) cut = 1e-6;
+    S.lam_cut = cut;
+    const double al = 2.0 / (S.lam_max - cut);
+    S.c_hop = al;
+    S.c_diag = (S.lam_max + cut - 12.0) / (S.lam_max - cut);
+    S.chol_fail = s_flag;
+  }
+  __syncthreads();
+  {
+    // Scaled recurrence.  With E_1 = S/2, E_0 = 0 and
+    //   E_{n+1} = 2B E_n - E_{n-1} + T_n(theta_B) S,
+    // T_m(B) V = V T_m(Theta_B) + E_m exactly (S = 2(BV - V Theta_B)).  Each
+    // column is carried as E'_n = E_n / nu_n, nu_n = max(1, |T_n|), so that
+    // every FP32 value stays O(|S|):
+    //   step 1: E'_2 = (B S + T_1 S) / nu_2
+    //   step 2: E'_3 = (2 nu_2 B E'_2 + (T_2 - 1/2) S) / nu_3
+    //   step n: E'_{n+1} = (2 nu_n B E'_n - nu_{n-1} E'_{n-1} + T_n S) / nu_{n+1}
+    //   final : W' = (T_m / nu_m) V + E'_m   (= W / nu_m)
+    const ProbState S = ps[p];
+    const int m = d.mdeg;
+    double* tc = tcoef + d.tc;
+    for (int j = tid; j < k; j += nt) {
+      const double tb = 1.0 + 2.0 * (S.lam_cut - th[j]) / (S.lam_max - S.lam_cut);
+      double tn[66], nu[66];
+      tn[0] = 1.0;
+      tn[1] = tb;
+      for (int n = 2; n <= m; ++n) tn[n] = 2.0 * tb * tn[n - 1] - tn[n - 2];
+      for (int n = 0; n <= m; ++n) nu[n] = fmax(1.0, fabs(tn[n]));
+      for (int n = 1; n < m; ++n) {
+        double a, z, g;
+        if (n == 1) {
+          a = 1.0 / nu[2];
+          z = 0.0;
+          g = tn[1] / nu[2];
+        } else if (n == 2) {
+          a = 2.0 * nu[2] / nu[3];
+          z = 0.0;
+          g = (tn[2] - 0.5) / nu[3];
+        } else {
+          a = 2.0 * nu[n] / nu[n + 1];
+          z = -nu[n - 1] / nu[n + 1];
+          g = tn[n] / nu[n + 1];
+        }
+        tc[((size_t)n * 3 + 0) * k + j] = a;
+        tc[((size_t)n * 3 + 1) * k + j] = z;
+        tc[((size_t)n * 3 + 2) * k + j] = g;
+      }
+      tc[((size_t)m * 3 + 0) * k + j] = tn[m] / nu[m];
+      scol[d.kv + j] = -2.0 * S.c_hop;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- rotate ---
+// CTA: 128 threads, tile 64 rows x 32 columns; thread: rows ty+16i, cols tx+8j.
+constexpr int RR = 64, RC = 32, RK = 16;
+
+__global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
+                                                const int* __restrict__ start, int np, const double2* __restrict__ Wp,
+                                                const double2* __restrict__ Yp, const double2* __restrict__ KK,
+                                                const double* __restrict__ theta, const double* __restrict__ scol,
+                                                double2* __restrict__ Vp, float2* __restrict__ Sp,
+                                                double* __restrict__ rpart) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int nct = d.k / RC;
+  const int t = blockIdx.x - start[p];
+  const int rt = t / nct, ct = t - rt * nct;
+  const int row0 = rt * RR, col0 = ct * RC;
+  const int k = d.k;
+  const double2* C = KK + d.kk;  // C in G storage, column-major k x k
+  const double2* Wb = Wp + d.blk;
+  const double2* Yb = Yp + d.blk;
+  __shared__ double2 sW[RK][RR], sY[RK][RR], sC[RK][RC + 1];
+  const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
+  double2 av[4][4], ay[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) av[i][j] = ay[i][j] = make_double2(0.0, 0.0);
+  for (int q0 = 0; q0 < k; q0 += RK) {
+    // W, Y tiles: 16 columns x 64 rows each (coalesced along rows)
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int idx = threadIdx.x + 128 * e;
+      const int c = idx >> 6, r = idx & 63;
+      const int row = row0 + r;
+      const bool ok = row < d.dim;
+      sW[c][r] = ok ? __ldg(Wb + (size_t)(q0 + c) * d.dim + row) : make_double2(0.0, 0.0);
+      sY[c][r] = ok ? __ldg(Yb + (size_t)(q0 + c) * d.dim + row) : make_double2(0.0, 0.0);
+    }
+    // C tile: rows q0..q0+15, columns col0..col0+31
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int idx = threadIdx.x + 128 * e;
+      const int c = idx >> 4, r = idx & 15;
+      sC[r][c] = __ldg(C + (size_t)(col0 + c) * k + q0 + r);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < RK; ++q) {
+      double2 w[4], y[4], c[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        w[i] = sW[q][ty + 16 * i];
+        y[i] = sY[q][ty + 16 * i];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) c[j] = sC[q][tx + 8 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          cfma(av[i][j], w[i], c[j]);
+          cfma(ay[i][j], y[i], c[j]);
+        }
+    }
+    __syncthreads();
+  }
+  // epilogue
+  __shared__ double sres[16][RC + 1];
+  double rs[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int col = col0 + tx + 8 * j;
+    const double th = __ldg(theta + d.kv + col);
+    const double sc = __ldg(scol + d.kv + col);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = row0 + ty + 16 * i;
+      if (row < d.dim) {
+        const size_t o = (size_t)d.blk + (size_t)col * d.dim + row;
+        const double2 v = av[i][j];
+        const double2 r = make_double2(ay[i][j].x - th * v.x, ay[i][j].y - th * v.y);
+        Vp[o] = v;
+        Sp[o] = make_float2((float)(sc * r.x), (float)(sc * r.y));
+        rs[j] += r.x * r.x + r.y * r.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) sres[ty][tx + 8 * j] = rs[j];
+  __syncthreads();
+  if (threadIdx.x < RC) {
+    double s = 0.0;
+    for (int r = 0; r < 16; ++r) s += sres[r][threadIdx.x];
+    rpart[d.rp + (size_t)rt * k + col0 + threadIdx.x] = s;
+  }
+}
+
+// ------------------------------------------------------- residuals/conv ----
+__global__ void k_resid(const ProbDesc* __restrict__ pd, ProbState* __restrict__ ps, const double* __restrict__ rpart,
+                        double* __restrict__ resid, double tol, int* __restrict__ n_active) {
+  const int p = blockIdx.x;
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  __shared__ double s_max[32];
+  __shared__ int s_cnt[32];
+  double mx = 0.0;
+  int cnt = 0;
+  const double lmax = ps[p].lam_max;
+  for (int j = threadIdx.x; j < d.k; j += blockDim.x) {
+    double s = 0.0;
+    for (int r = 0; r < d.nrt; ++r) s += rpart[d.rp + (size_t)r * d.k + j];
+    const double rr = sqrt(s) / lmax;
+    resid[d.kv + j] = rr;
+    if (j < d.nev) {
+      mx = fmax(mx, rr);
+      cnt += rr <= tol;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s_max[threadIdx.x >> 5] = mx;
+    s_cnt[threadIdx.x >> 5] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    int c = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      m = fmax(m, s_max[w]);
+      c += s_cnt[w];
+    }
+    ProbState& S = ps[p];
+    S.max_resid = m;
+    S.nconv = c;
+    S.iters += 1;
+    if (c >= d.nev) S.active = 0;
+    else atomicAdd(n_active, 1);
+  }
+}
+
+// ---------------------------------------------------------------- output ---
+// fix_phase (modules/eigensystem.cpp:4-30) on V[:, :nev]: phase_j = arg V(0,j),
+// V_j <- e^{-i phase_j} V_j; also |V_j|^2 for tr(V^dag V).  One CTA per column.
+__global__ void k_phase_fix(const ProbDesc* __restrict__ pd, const int* __restrict__ start, int np,
+                            double2* __restrict__ Vp, double* __restrict__ phases, double* __restrict__ norms,
+                            int apply) {
+  const int p = find_prob(start, np, blockIdx.x);
+  const ProbDesc d = pd[p];
+  const int j = blockIdx.x - start[p];
+  if (j >= d.nev) return;
+  double2* v = Vp + d.blk + (size_t)j * d.dim;
+  const double2 v0 = v[0];
+  const double ph = atan2(v0.y, v0.x);
+  double sn, cs;
+  sincos(ph, &sn, &cs);
+  const double2 f = apply ? make_double2(cs, -sn) : make_double2(1.0, 0.0);
+  double nrm = 0.0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < d.dim; i += blockDim.x) {
+    const double2 x = v[i];
+    nrm += x.x * x.x + x.y * x.y;
+    if (apply) v[i] = cmul(f, x);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = nrm;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    phases[d.kv + j] = ph;
+    norms[d.kv + j] = red[0];
+  }
+}
+
+// ------------------------------------------------------------- launchers ---
+int gram(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int chunk_rows,
+         const double2* W, const double2* Y, double2* gpart, cudaStream_t st) {
+  k_gram<<<nblk, 64, 0, st>>>(pd, ps, start, np, chunk_rows, W, Y, gpart);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+int gram_reduce(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* gpart,
+                double2* KK, cudaStream_t st) {
+  k_gram_reduce<<<nblk, 256, 0, st>>>(pd, ps, start, np, gpart, KK);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* theta, double* tcoef, double* scol,
+                double* dwork, int first_iter, int fixed_cut, int max_sweeps, cudaStream_t st) {
+  k_small<<<np, 1024, 0, st>>>(pd, ps, KK, theta, tcoef, scol, dwork, first_iter, fixed_cut, max_sweeps);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* W,
+           const double2* Y, const double2* KK, const double* theta, const double* scol, double2* V, float2* S,
+           double* rpart, cudaStream_t st) {
+  k_rotate<<<nblk, 128, 0, st>>>(pd, ps, start, np, W, Y, KK, theta, scol, V, S, rpart);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+int resid_check(const ProbDesc* pd, ProbState* ps, int np, const double* rpart, double* resid, double tol,
+                int* n_active, cudaStream_t st) {
+  k_resid<<<np, 256, 0, st>>>(pd, ps, rpart, resid, tol, n_active);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+int phase_fix(const ProbDesc* pd, const int* start, int np, int nblk, double2* V, double* phases, double* norms,
+              int apply, cudaStream_t st) {
+  k_phase_fix<<<nblk, 256, 0, st>>>(pd, start, np, V, phases, norms, apply);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+
+}  // namespace laph

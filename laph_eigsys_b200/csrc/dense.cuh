@@ -1,0 +1,21 @@
+// dense.cuh -- launchers of the FP64 dense block operations (dense.cu).
+#pragma once
+#include "batch.cuh"
+
+namespace laph {
+constexpr int kGramTile = 32;   // block widths k are multiples of this
+constexpr int kRotRows = 64;    // rows per rotation tile
+int gram(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int chunk_rows,
+         const double2* W, const double2* Y, double2* gpart, cudaStream_t st);
+int gram_reduce(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* gpart,
+                double2* KK, cudaStream_t st);
+int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* theta, double* tcoef, double* scol,
+                double* dwork, int first_iter, int fixed_cut, int max_sweeps, cudaStream_t st);
+int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* W,
+           const double2* Y, const double2* KK, const double* theta, const double* scol, double2* V, float2* S,
+           double* rpart, cudaStream_t st);
+int resid_check(const ProbDesc* pd, ProbState* ps, int np, const double* rpart, double* resid, double tol,
+                int* n_active, cudaStream_t st);
+int phase_fix(const ProbDesc* pd, const int* start, int np, int nblk, double2* V, double* phases, double* norms,
+              int apply, cudaStream_t st);
+}  // namespace laph

@@ -1,0 +1,267 @@
+// filter.cu -- the multi-right-hand-side Chebyshev filter (lap_cheb_mrhs) and
+// the other block stencils of the batched solver.
+//
+// lap_cheb_mrhs: one Chebyshev step on a block of k vectors of every active
+// problem in one launch,
+//     Y_j = a_j (c_hop hop(X_j) + c_diag X_j) + z_j Z_j + g_j S_j ,
+// FP32 arithmetic on complex64 vectors, links FP32 or BF16 (+ FP32 per-site
+// scale) reconstructed to FP32 in registers.  One thread owns one site and
+// walks kb columns, so the 6 links a site needs (its 3 forward links and the
+// 3 backward links U_mu(x-mu)) are read from HBM once per kb vectors and held
+// in 108 registers; the vector reads of consecutive threads are consecutive
+// 24-byte site vectors (fully coalesced), neighbour reuse comes from L1/L2.
+// Per-column coefficients (a_j, z_j, g_j) come from a device table written by
+// the Rayleigh-Ritz step, so every launch of an iteration is identical.
+// Algorithmic bytes per site and vector: 24 (X) + 24 (S) + 24 (Z) + 24 (Y)
+// plus (108 + 4) / kb for BF16 links; see the solver for the recurrence.
+#include "batch.cuh"
+#include "filter.cuh"
+
+#include <cuda_bf16.h>
+
+namespace laph {
+
+// ---------------------------------------------------------------- links ----
+__device__ __forceinline__ float2 ld_lk(const float2* __restrict__ p, const float*, size_t i, int) { return __ldg(p + i); }
+__device__ __forceinline__ float2 ld_lk(const __nv_bfloat162* __restrict__ p, const float* __restrict__ sc, size_t i,
+                                        int site) {
+  const float2 v = __bfloat1622float2(__ldg(p + i));
+  const float s = __ldg(sc + site);
+  return make_float2(v.x * s, v.y * s);
+}
+
+// FP64 site-minor links -> filter links (FP32, or BF16 with a per-site scale
+// = max |element| over the site's 27 complex entries).
+__global__ void k_pack_links(const ProbDesc* __restrict__ pd, const int* __restrict__ start, int np,
+                             const double2* __restrict__ U64, float2* __restrict__ Uf32,
+                             __nv_bfloat162* __restrict__ Ubf, float* __restrict__ scale, int bf16) {
+  const int p = find_prob(start, np, blockIdx.x);
+  const ProbDesc d = pd[p];
+  const int s = (blockIdx.x - start[p]) * blockDim.x + threadIdx.x;
+  if (s >= d.V3) return;
+  const double2* U = U64 + d.u64;
+  if (!bf16) {
+    for (int e = 0; e < 27; ++e) {
+      const double2 v = U[(size_t)e * d.V3 + s];
+      Uf32[d.uf + (size_t)e * d.V3 + s] = make_float2((float)v.x, (float)v.y);
+    }
+    return;
+  }
+  double m = 0.0;
+  for (int e = 0; e < 27; ++e) {
+    const double2 v = U[(size_t)e * d.V3 + s];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  const float scl = m > 0.0 ? (float)m : 1.0f;
+  scale[d.sc + s] = scl;
+  const double inv = 1.0 / (double)scl;
+  for (int e = 0; e < 27; ++e) {
+    const double2 v = U[(size_t)e * d.V3 + s];
+    Ubf[d.uf + (size_t)e * d.V3 + s] = __floats2bfloat162_rn((float)(v.x * inv), (float)(v.y * inv));
+  }
+}
+
+// ---------------------------------------------------------- the filter -----
+template <typename LT, bool HAS_Z, bool FINAL>
+__global__ void __launch_bounds__(128, 3)
+    k_cheb_mrhs(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, const int* __restrict__ start, int np,
+                int kb, const LT* __restrict__ links, const float* __restrict__ scale, const float2* __restrict__ Xp,
+                const float2* __restrict__ Zp, const float2* __restrict__ Sp, float2* __restrict__ Yp,
+                const double2* __restrict__ Vp, double2* __restrict__ Wp, const double* __restrict__ tcoef, int step) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int nst = (d.V3 + 127) >> 7;
+  const int t = blockIdx.x - start[p];
+  const int st = t % nst, cb = t / nst;
+  const int s = st * 128 + threadIdx.x;
+  if (s >= d.V3) return;
+  const int j0 = cb * kb;
+  const int j1 = min(j0 + kb, d.k);
+  const Lat g{d.L, d.L * d.L, d.V3};
+  int sx, sy, sz;
+  site_xyz(g, s, sx, sy, sz);
+  int up[3], dn[3];
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu) {
+    up[mu] = nb_up(g, sx, sy, sz, mu);
+    dn[mu] = nb_dn(g, sx, sy, sz, mu);
+  }
+  // 6 links in registers: forward U_mu(s), backward U_mu(s-mu)
+  const LT* U = links + d.uf;
+  const float* scl = scale + d.sc;
+  float2 uf[3][9], ub[3][9];
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu)
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      uf[mu][e] = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + s, s);
+      ub[mu][e] = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + dn[mu], dn[mu]);
+    }
+  const double c_hop = ps[p].c_hop, c_diag = ps[p].c_diag;
+  // coefficient table of this step: [step][0..2][k] = (a_j, z_j, g_j); the
+  // final step also reads [step+1][0][k] = T_m / nu_m (see k_small)
+  const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
+  const size_t base = (size_t)d.blk;
+#pragma unroll 1
+  for (int j = j0; j < j1; ++j) {
+    const size_t col = base + (size_t)j * d.dim;
+    const float2* x = Xp + col;
+    float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      float2 xu[3], xd[3];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        xu[b] = __ldg(x + 3 * (size_t)up[mu] + b);
+        xd[b] = __ldg(x + 3 * (size_t)dn[mu] + b);
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          cfmaf(acc[a], uf[mu][3 * a + b], xu[b]);
+          cfmacf(acc[a], ub[mu][3 * b + a], xd[b]);
+        }
+    }
+    const double aj = __ldg(tc + j);
+    const float a_h = (float)(aj * c_hop), a_d = (float)(aj * c_diag);
+    const float zc = (float)__ldg(tc + d.k + j);
+    const float gj = (float)__ldg(tc + 2 * d.k + j);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const size_t i = col + 3 * (size_t)s + a;
+      const float2 xs = __ldg(x + 3 * (size_t)s + a);
+      const float2 ss = __ldg(Sp + i);
+      float2 r;
+      r.x = fmaf(a_h, acc[a].x, fmaf(a_d, xs.x, gj * ss.x));
+      r.y = fmaf(a_h, acc[a].y, fmaf(a_d, xs.y, gj * ss.y));
+      if (HAS_Z) {
+        const float2 zz = __ldg(Zp + i);
+        r.x = fmaf(zc, zz.x, r.x);
+        r.y = fmaf(zc, zz.y, r.y);
+      }
+      if (FINAL) {
+        // W = T_m(theta_B) V + E_m in FP64
+        const double tm = __ldg(tc + (size_t)3 * d.k + j);
+        const double2 v = __ldg(Vp + i);
+        Wp[i] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
+      } else {
+        Yp[i] = r;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------ FP64 block stencil: A W --
+// Y_j = (-Delta) W_j = 6 W_j - hop(W_j), FP64, one thread per (site, column).
+__global__ void __launch_bounds__(128) k_neglap64_batch(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
+                                                        const int* __restrict__ start, int np,
+                                                        const double2* __restrict__ U64, const double2* __restrict__ Wp,
+                                                        double2* __restrict__ Yp) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int nst = (d.V3 + 127) >> 7;
+  const int t = blockIdx.x - start[p];
+  const int st = t % nst, j = t / nst;
+  const int s = st * 128 + threadIdx.x;
+  if (s >= d.V3 || j >= d.k) return;
+  const Lat g{d.L, d.L * d.L, d.V3};
+  const double2* U = U64 + d.u64;
+  const size_t col = (size_t)d.blk + (size_t)j * d.dim;
+  const double2* x = Wp + col;
+  int sx, sy, sz;
+  site_xyz(g, s, sx, sy, sz);
+  double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu) {
+    const int u = nb_up(g, sx, sy, sz, mu), dn = nb_dn(g, sx, sy, sz, mu);
+    double2 xu[3], xd[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      xu[b] = __ldg(x + 3 * (size_t)u + b);
+      xd[b] = __ldg(x + 3 * (size_t)dn + b);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        cfma(acc[a], __ldg(U + (size_t)(mu * 9 + 3 * a + b) * d.V3 + s), xu[b]);
+        cfmac(acc[a], __ldg(U + (size_t)(mu * 9 + 3 * b + a) * d.V3 + dn), xd[b]);
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double2 xs = __ldg(x + 3 * (size_t)s + a);
+    Yp[col + 3 * (size_t)s + a] = make_double2(6.0 * xs.x - acc[a].x, 6.0 * xs.y - acc[a].y);
+  }
+}
+
+// ------------------------------------------------------ random start block -
+__device__ __forceinline__ uint64_t mix64d(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+__global__ void k_random_block(const ProbDesc* __restrict__ pd, const int* __restrict__ start, int np,
+                               double2* __restrict__ W, uint64_t seed) {
+  const int p = find_prob(start, np, blockIdx.x);
+  const ProbDesc d = pd[p];
+  const long long i = (long long)(blockIdx.x - start[p]) * blockDim.x + threadIdx.x;
+  const long long n = (long long)d.dim * d.k;
+  if (i >= n) return;
+  uint64_t st = seed * 0x9E3779B97F4A7C15ULL + ((uint64_t)p << 40) + (uint64_t)i * 0xD1B54A32D192ED03ULL;
+  const double u1 = ((mix64d(st + 0x9E3779B97F4A7C15ULL) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  const double u2 = ((mix64d(st + 0x3C6EF372FE94F82AULL) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  const double r = sqrt(-2.0 * log(u1));
+  double sn, cs;
+  sincospi(2.0 * u2, &sn, &cs);
+  W[d.blk + i] = make_double2(r * cs, r * sn);
+}
+
+// ------------------------------------------------------------- launchers ---
+int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const double2* U64, float2* Uf32, void* Ubf,
+               float* scale, int bf16, cudaStream_t st) {
+  k_pack_links<<<nblk, 128, 0, st>>>(pd, start, np, U64, Uf32, reinterpret_cast<__nv_bfloat162*>(Ubf), scale, bf16);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+
+int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
+              const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
+              const double2* V, double2* W, const double* tcoef, int step, bool final_step, cudaStream_t st) {
+#define LAPH_CHEB(LT, HZ, FIN)                                                                                  \
+  k_cheb_mrhs<LT, HZ, FIN><<<nblk, 128, 0, st>>>(pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), scale, \
+                                                 X, Z, S, Y, V, W, tcoef, step)
+  const bool hz = Z != nullptr;
+  if (bf16) {
+    if (hz && final_step) LAPH_CHEB(__nv_bfloat162, true, true);
+    else if (hz) LAPH_CHEB(__nv_bfloat162, true, false);
+    else if (final_step) LAPH_CHEB(__nv_bfloat162, false, true);
+    else LAPH_CHEB(__nv_bfloat162, false, false);
+  } else {
+    if (hz && final_step) LAPH_CHEB(float2, true, true);
+    else if (hz) LAPH_CHEB(float2, true, false);
+    else if (final_step) LAPH_CHEB(float2, false, true);
+    else LAPH_CHEB(float2, false, false);
+  }
+#undef LAPH_CHEB
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+
+int neglap64_batch(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
+                   const double2* W, double2* Y, cudaStream_t st) {
+  k_neglap64_batch<<<nblk, 128, 0, st>>>(pd, ps, start, np, U64, W, Y);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+
+int random_block(const ProbDesc* pd, const int* start, int np, int nblk, double2* W, uint64_t seed, cudaStream_t st) {
+  k_random_block<<<nblk, 256, 0, st>>>(pd, start, np, W, seed);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+
+}  // namespace laph

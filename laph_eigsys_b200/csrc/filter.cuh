@@ -1,0 +1,20 @@
+// filter.cuh -- launchers of the block stencils (filter.cu).
+#pragma once
+#include "batch.cuh"
+
+namespace laph {
+// FP64 links -> FP32 or BF16 (+ per-site scale) filter links; nblk blocks of 128 sites.
+int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const double2* U64, float2* Uf32, void* Ubf,
+               float* scale, int bf16, cudaStream_t st);
+// One Chebyshev step Y_j = a_j (c_hop hop(X_j) + c_diag X_j) + z_j Z_j + g_j S_j (FP32)
+// with (a, z, g) = tcoef[step][0..2][j]; final_step writes W_j = tcoef[step+1][0][j] V_j + Y_j
+// in FP64 instead of Y.
+int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
+              const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
+              const double2* V, double2* W, const double* tcoef, int step, bool final_step, cudaStream_t st);
+// Y = (-Delta) W for every column, FP64.
+int neglap64_batch(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
+                   const double2* W, double2* Y, cudaStream_t st);
+// Gaussian random start block.
+int random_block(const ProbDesc* pd, const int* start, int np, int nblk, double2* W, uint64_t seed, cudaStream_t st);
+}  // namespace laph

@@ -47,6 +47,26 @@ int soa_to_links(const double2* soa, int V3, int layout, double* out) {
   return LAPH_OK;
 }
 
+__global__ void k_links_to_soa(const double2* __restrict__ in, int layout, int V3, double2* __restrict__ soa) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 27LL * V3) return;
+  const int e = (int)(t / V3), s = (int)(t - (long long)e * V3);  // e = dir*9 + 3a + b
+  const int d = e / 9, ab = e - d * 9;
+  const size_t src = layout == LAPH_LAYOUT_CONF ? (size_t)s * 36 + (d + 1) * 9 + ab : ((size_t)s * 3 + d) * 9 + ab;
+  soa[t] = in[src];
+}
+
+int links_to_soa_device(const double* links, int layout, int V3, double2* soa, cudaStream_t st) {
+  if (layout != LAPH_LAYOUT_ROWMAJOR && layout != LAPH_LAYOUT_CONF) {
+    set_error("links_to_soa_device: layout %d not supported for device links", layout);
+    return LAPH_EINVAL;
+  }
+  k_links_to_soa<<<ceil_div(27LL * V3, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(links), layout, V3, soa);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  LAPH_CUDA_TRY(cudaStreamSynchronize(st));
+  return LAPH_OK;
+}
+
 // One CTA per timeslice, fixed reduction order (deterministic).
 __global__ void __launch_bounds__(512) k_plaq_moments(const double2* __restrict__ Ub, Lat g, size_t ts_stride,
                                                       double* __restrict__ out) {

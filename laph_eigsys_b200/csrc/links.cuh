@@ -8,6 +8,8 @@ namespace laph {
 // soa[(dir*9 + 3a + b)*V3 + site] (complex128).
 int links_to_soa(const double* links, int layout, int V3, double2* soa);
 int soa_to_links(const double2* soa, int V3, int layout, double* links);
+// Device: same reorder for links already in device memory (ROWMAJOR or CONF).
+int links_to_soa_device(const double* links, int layout, int V3, double2* soa, cudaStream_t st);
 // Device: average spatial plaquette of nts timeslices -> out[nts]
 // (plaque_timeslice, modules/config_utils.cpp:388-426).
 int plaquette_batch(const double2* U, int L, int nts, double* out, cudaStream_t st);

@@ -1,0 +1,445 @@
+// solver.cu -- the batched block eigensolver (laph_solver_*): a device-resident
+// Chebyshev-filtered subspace iteration over many timeslices at once.
+//
+// Per problem (timeslice), with A = -Delta, block width k = nev + guard
+// (rounded up to a multiple of 32), FP64 Ritz block V, Ritz values Theta and
+// FP64 residuals R = A V - V Theta:
+//   1. filter   W = T_m(B) V with B = c_hop hop + c_diag mapping the damped
+//               interval [lam_cut, lam_max] to [-1, 1].  The exact part
+//               V T_m(Theta_B) is formed in FP64; only the correction E_m,
+//               driven by S = 2(B V - V Theta_B) = -2 c_hop R, runs through
+//               the FP32 multi-RHS stencil (lap_cheb_mrhs), so FP32 rounding
+//               scales with |R| and the iteration converges to FP64 accuracy.
+//   2. Y = A W  (FP64 stencil)
+//   3. [G | H] = W^H [W | Y]  (FP64)
+//   4. per problem: scaled Cholesky G = D R^H R D, Minv = D^-1 R^-1,
+//      Jacobi eigensolve of Minv^H H Minv = Q Theta Q^H, C = Minv Q,
+//      next window lam_cut = max Ritz value, Chebyshev coefficient table
+//   5. V = W C, R = Y C - V Theta, S = -2 c_hop R (FP32), residual norms
+//   6. convergence mask: all nev wanted ||r_j|| / lam_max <= tol
+// Every step is one launch over all active problems (CTA -> problem through a
+// prefix table), so the host loop issues the same launches each iteration.
+// This replaces, per timeslice, MatCreateShell + EPSSolve + EPSGetEigenpair +
+// fix_phase + recover_spectrum of the reference (src/ev_ts.cpp:197-319).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "batch.cuh"
+#include "common.cuh"
+#include "dense.cuh"
+#include "filter.cuh"
+#include "links.cuh"
+#include "smear.cuh"
+
+using namespace laph;
+
+struct laph_solver {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  laph_solve_opts o{};
+  int np = 0, mdeg = 16, kb = 32;
+  std::vector<ProbDesc> hd;
+  ProbDesc* d_pd = nullptr;
+  ProbState* d_ps = nullptr;
+  std::vector<ProbState> hps;
+  // CTA -> problem prefix tables
+  int *st_site = nullptr, *st_filt = nullptr, *st_nl = nullptr, *st_gram = nullptr, *st_gred = nullptr,
+      *st_rot = nullptr, *st_rand = nullptr, *st_col = nullptr;
+  int nb_site = 0, nb_filt = 0, nb_nl = 0, nb_gram = 0, nb_gred = 0, nb_rot = 0, nb_rand = 0, nb_col = 0;
+  // pools
+  double2 *U64 = nullptr, *Utmp = nullptr, *dec = nullptr;
+  float2* Uf32 = nullptr;
+  void* Ubf = nullptr;
+  float* scale = nullptr;
+  double2 *V = nullptr, *W = nullptr, *Y = nullptr;
+  float2 *S = nullptr, *E[3] = {nullptr, nullptr, nullptr};
+  double2 *KK = nullptr, *gpart = nullptr;
+  double *rpart = nullptr, *theta = nullptr, *tcoef = nullptr, *scol = nullptr, *dwork = nullptr, *resid = nullptr,
+         *phases = nullptr, *norms = nullptr;
+  int* d_nactive = nullptr;
+  int* h_nactive = nullptr;
+  size_t blk_total = 0;
+  std::vector<int> links_set;
+  double ms[4] = {0, 0, 0, 0};
+  long long cnt[3] = {0, 0, 0};
+  std::vector<cudaEvent_t> evf;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  int ran = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  if (cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("device allocation of %zu bytes failed", n * sizeof(T));
+    return LAPH_ENOMEM;
+  }
+  return LAPH_OK;
+}
+
+int upload_prefix(const std::vector<int>& per, int** d, int* total) {
+  std::vector<int> pre(per.size() + 1, 0);
+  for (size_t i = 0; i < per.size(); ++i) pre[i + 1] = pre[i] + per[i];
+  *total = pre.back();
+  LAPH_TRY(dalloc(d, pre.size()));
+  LAPH_CUDA_TRY(cudaMemcpy(*d, pre.data(), pre.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return LAPH_OK;
+}
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+}  // namespace
+
+extern "C" {
+
+void laph_solve_opts_default(laph_solve_opts* o) {
+  std::memset(o, 0, sizeof *o);
+  o->smear_kind = LAPH_SMEAR_NONE;
+  o->guard = 16;
+  o->link_prec = LAPH_LINKS_BF16;
+  o->tol = 1e-9;
+  o->max_it = 200;
+  o->window = LAPH_WINDOW_LANCZOS;
+  o->deg = 16;
+  o->phase_fix = 1;
+  o->seed = 1227;
+}
+
+int laph_solver_destroy(laph_solver* s) {
+  if (!s) return LAPH_OK;
+  cudaSetDevice(s->dev);
+  if (s->st) cudaStreamSynchronize(s->st);
+  void* ptrs[] = {s->d_pd, s->d_ps, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
+                  s->st_col, s->U64, s->Utmp, s->dec, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
+                  s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
+                  s->phases, s->norms, s->d_nactive};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (s->h_nactive) cudaFreeHost(s->h_nactive);
+  for (auto e : s->evf) cudaEventDestroy(e);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->ev2) cudaEventDestroy(s->ev2);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+  return LAPH_OK;
+}
+
+int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, const laph_solve_opts* opts, int device) {
+  if (!out || !probs || n < 1 || !opts) {
+    set_error("laph_solver_create: bad argument");
+    return LAPH_EINVAL;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("laph_solver_create: no CUDA device");
+    return LAPH_ENODEV;
+  }
+  if (opts->deg < 2 || opts->deg > 64 || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1) {
+    set_error("laph_solver_create: need 2 <= deg <= 64, guard >= 0, tol > 0, max_it >= 1");
+    return LAPH_EINVAL;
+  }
+  for (int i = 0; i < n; ++i) {
+    const int L = probs[i].L, nev = probs[i].nev;
+    const int k = round_up(nev + opts->guard, kGramTile);
+    if (L < 3 || L > 128 || nev < 1 || k > 512 || k > 3 * L * L * L / 2) {
+      set_error("laph_solver_create: problem %d: need 3 <= L <= 128, 1 <= nev, block width %d <= min(512, dim/2)", i, k);
+      return LAPH_EINVAL;
+    }
+  }
+  laph_solver* s = new laph_solver();
+  auto fail = [&](int stt) {
+    laph_solver_destroy(s);
+    return stt;
+  };
+  s->dev = device;
+  s->o = *opts;
+  s->np = n;
+  s->mdeg = opts->deg;
+  s->kb = 32;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("laph_solver_create: cannot use device %d", device);
+    return fail(LAPH_ECUDA);
+  }
+  // descriptors and pool offsets
+  long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
+  size_t max_run = 0;
+  std::vector<int> per_site, per_filt, per_nl, per_gram, per_gred, per_rot, per_rand, per_col;
+  for (int i = 0; i < n; ++i) {
+    ProbDesc d{};
+    d.L = probs[i].L;
+    d.V3 = d.L * d.L * d.L;
+    d.dim = 3 * d.V3;
+    d.nev = probs[i].nev;
+    d.k = round_up(d.nev + opts->guard, kGramTile);
+    d.mdeg = s->mdeg;
+    d.u64 = o_u64;
+    d.uf = o_uf;
+    d.sc = o_sc;
+    d.blk = o_blk;
+    d.kk = o_kk;
+    d.kv = o_kv;
+    d.gp = o_gp;
+    d.rp = o_rp;
+    d.tc = o_tc;
+    const int chunk_rows = 8192;
+    d.nchunk = (d.dim + chunk_rows - 1) / chunk_rows;
+    d.nrt = (d.dim + kRotRows - 1) / kRotRows;
+    const int T = d.k / kGramTile, npair = T * (T + 1) / 2;
+    o_u64 += 27LL * d.V3;
+    o_uf += 27LL * d.V3;
+    o_sc += d.V3;
+    o_blk += (long long)d.dim * d.k;
+    o_kk += 5LL * d.k * d.k;
+    o_kv += d.k;
+    o_gp += (long long)d.nchunk * 2 * npair * kGramTile * kGramTile;
+    o_rp += (long long)d.nrt * d.k;
+    o_tc += (long long)(s->mdeg + 1) * 3 * d.k;
+    s->hd.push_back(d);
+    const int nst = (d.V3 + 127) / 128;
+    per_site.push_back(nst);
+    per_filt.push_back(nst * ((d.k + s->kb - 1) / s->kb));
+    per_nl.push_back(nst * d.k);
+    per_gram.push_back(d.nchunk * 2 * npair);
+    per_gred.push_back((2 * npair * kGramTile * kGramTile + 255) / 256);
+    per_rot.push_back(d.nrt * (d.k / 32));
+    per_rand.push_back((int)(((long long)d.dim * d.k + 255) / 256));
+    per_col.push_back(d.nev);
+  }
+  // longest run of equal L (smearing is batched per run)
+  for (int i = 0; i < n;) {
+    int j = i;
+    while (j < n && s->hd[j].L == s->hd[i].L) ++j;
+    max_run = std::max(max_run, (size_t)(j - i) * 27 * s->hd[i].V3);
+    i = j;
+  }
+  s->blk_total = (size_t)o_blk;
+  int rc = LAPH_OK;
+  if ((rc = dalloc(&s->d_pd, n)) || (rc = dalloc(&s->d_ps, n)) || (rc = dalloc(&s->U64, o_u64)) ||
+      (rc = dalloc(&s->Utmp, max_run)) || (rc = dalloc(&s->dec, max_run * 2)) ||
+      (rc = dalloc(&s->scale, o_sc)) || (rc = dalloc(&s->V, o_blk)) || (rc = dalloc(&s->W, o_blk)) ||
+      (rc = dalloc(&s->Y, o_blk)) || (rc = dalloc(&s->S, o_blk)) || (rc = dalloc(&s->E[0], o_blk)) ||
+      (rc = dalloc(&s->E[1], o_blk)) || (rc = dalloc(&s->E[2], o_blk)) || (rc = dalloc(&s->KK, o_kk)) ||
+      (rc = dalloc(&s->gpart, o_gp)) || (rc = dalloc(&s->rpart, o_rp)) || (rc = dalloc(&s->theta, o_kv)) ||
+      (rc = dalloc(&s->tcoef, o_tc)) || (rc = dalloc(&s->scol, o_kv)) || (rc = dalloc(&s->dwork, 4 * o_kv)) ||
+      (rc = dalloc(&s->resid, o_kv)) || (rc = dalloc(&s->phases, o_kv)) || (rc = dalloc(&s->norms, o_kv)) ||
+      (rc = dalloc(&s->d_nactive, 1)))
+    return fail(rc);
+  if (opts->link_prec == LAPH_LINKS_BF16) {
+    if ((rc = dalloc(reinterpret_cast<float2**>(&s->Ubf), (size_t)o_uf))) return fail(rc);  // 4 B per element
+  } else {
+    if ((rc = dalloc(&s->Uf32, o_uf))) return fail(rc);
+  }
+  if (cudaMallocHost(&s->h_nactive, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(LAPH_ENOMEM);
+  }
+  if ((rc = upload_prefix(per_site, &s->st_site, &s->nb_site)) || (rc = upload_prefix(per_filt, &s->st_filt, &s->nb_filt)) ||
+      (rc = upload_prefix(per_nl, &s->st_nl, &s->nb_nl)) || (rc = upload_prefix(per_gram, &s->st_gram, &s->nb_gram)) ||
+      (rc = upload_prefix(per_gred, &s->st_gred, &s->nb_gred)) || (rc = upload_prefix(per_rot, &s->st_rot, &s->nb_rot)) ||
+      (rc = upload_prefix(per_rand, &s->st_rand, &s->nb_rand)) || (rc = upload_prefix(per_col, &s->st_col, &s->nb_col)))
+    return fail(rc);
+  if (cudaMemcpy(s->d_pd, s->hd.data(), n * sizeof(ProbDesc), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(LAPH_ECUDA);
+  }
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  cudaEventCreate(&s->ev2);
+  s->links_set.assign(n, 0);
+  s->hps.assign(n, ProbState{});
+  *out = s;
+  return LAPH_OK;
+}
+
+int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout, int on_device) {
+  if (!s || i < 0 || i >= s->np || !links) {
+    set_error("laph_solver_set_links: bad argument");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  const ProbDesc& d = s->hd[i];
+  double2* dst = s->U64 + d.u64;
+  if (on_device) {
+    if (layout != LAPH_LAYOUT_ROWMAJOR && layout != LAPH_LAYOUT_CONF) {
+      set_error("laph_solver_set_links: device links must be ROWMAJOR or CONF");
+      return LAPH_EINVAL;
+    }
+    // device-side reorder to site-minor order through a host-free path:
+    // copy to the scratch and transpose with a small kernel
+    LAPH_TRY(links_to_soa_device(links, layout, d.V3, dst, s->st));
+  } else {
+    std::vector<double2> soa(27 * (size_t)d.V3);
+    LAPH_TRY(links_to_soa(links, layout, d.V3, soa.data()));
+    LAPH_CUDA_TRY(cudaMemcpyAsync(dst, soa.data(), soa.size() * sizeof(double2), cudaMemcpyHostToDevice, s->st));
+    LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  }
+  s->links_set[i] = 1;
+  return LAPH_OK;
+}
+
+static int iteration_rr(laph_solver* s, int first_iter) {
+  const bool fixed = s->o.window == LAPH_WINDOW_FIXED && s->o.lam_cut > 0.0;
+  LAPH_TRY(neglap64_batch(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->W, s->Y, s->st));
+  LAPH_TRY(gram(s->d_pd, s->d_ps, s->st_gram, s->np, s->nb_gram, 8192, s->W, s->Y, s->gpart, s->st));
+  LAPH_TRY(gram_reduce(s->d_pd, s->d_ps, s->st_gred, s->np, s->nb_gred, s->gpart, s->KK, s->st));
+  LAPH_TRY(small_dense(s->d_pd, s->d_ps, s->np, s->KK, s->theta, s->tcoef, s->scol, s->dwork, first_iter, fixed ? 1 : 0,
+                       30, s->st));
+  LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->Y, s->KK, s->theta, s->scol, s->V, s->S,
+                  s->rpart, s->st));
+  LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
+  LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
+  return LAPH_OK;
+}
+
+static int filter(laph_solver* s) {
+  const int m = s->mdeg;
+  const int bf = s->o.link_prec == LAPH_LINKS_BF16;
+  const void* links = bf ? s->Ubf : static_cast<const void*>(s->Uf32);
+  for (int n = 1; n < m; ++n) {
+    const bool fin = (n == m - 1);
+    const float2* X = (n == 1) ? s->S : s->E[(n - 2) % 3];
+    const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
+    float2* Yo = s->E[(n - 1) % 3];
+    LAPH_TRY(cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo,
+                       s->V, s->W, s->tcoef, n, fin, s->st));
+  }
+  return LAPH_OK;
+}
+
+int laph_solver_run(laph_solver* s, laph_result* res) {
+  if (!s) {
+    set_error("null solver");
+    return LAPH_EINVAL;
+  }
+  for (int i = 0; i < s->np; ++i)
+    if (!s->links_set[i]) {
+      set_error("laph_solver_run: links of problem %d not set", i);
+      return LAPH_EINVAL;
+    }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  const laph_solve_opts& o = s->o;
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev0, s->st));
+  // smearing, per run of equal L
+  for (int i = 0; i < s->np;) {
+    int j = i;
+    while (j < s->np && s->hd[j].L == s->hd[i].L) ++j;
+    LAPH_TRY(smear_batch(s->U64 + s->hd[i].u64, s->Utmp, s->dec, s->hd[i].L, j - i, o.smear_kind, o.smear_p1,
+                         o.smear_p2, o.smear_iters, o.smear_compat, s->st));
+    i = j;
+  }
+  LAPH_TRY(pack_links(s->d_pd, s->st_site, s->np, s->nb_site, s->U64, s->Uf32, s->Ubf, s->scale,
+                      o.link_prec == LAPH_LINKS_BF16, s->st));
+  // initial state
+  for (int i = 0; i < s->np; ++i) {
+    ProbState& p = s->hps[i];
+    p = ProbState{};
+    p.lam_max = o.lam_max > 0.0 ? o.lam_max : 12.0;  // spectrum of -Delta lies in [0, 12]
+    p.lam_cut = o.lam_cut > 0.0 ? o.lam_cut : 0.0;
+    p.active = 1;
+  }
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->d_ps, s->hps.data(), s->np * sizeof(ProbState), cudaMemcpyHostToDevice, s->st));
+  LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->W, o.seed, s->st));
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
+  LAPH_TRY(iteration_rr(s, 1));
+  s->cnt[0] = s->cnt[1] = s->cnt[2] = 0;
+  double filt_ms = 0.0;
+  if (s->evf.empty()) {
+    s->evf.resize(2);
+    cudaEventCreate(&s->evf[0]);
+    cudaEventCreate(&s->evf[1]);
+  }
+  int it = 1;
+  for (; it < o.max_it; ++it) {
+    LAPH_CUDA_TRY(cudaMemcpyAsync(s->h_nactive, s->d_nactive, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    LAPH_CUDA_TRY(cudaMemcpyAsync(s->hps.data(), s->d_ps, s->np * sizeof(ProbState), cudaMemcpyDeviceToHost, s->st));
+    LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+    if (*s->h_nactive == 0) break;
+    for (int i = 0; i < s->np; ++i)
+      if (s->hps[i].active) s->cnt[0] += (long long)s->hd[i].V3 * s->hd[i].k * (s->mdeg - 1);
+    s->cnt[1] += s->mdeg - 1;
+    LAPH_CUDA_TRY(cudaEventRecord(s->evf[0], s->st));
+    LAPH_TRY(filter(s));
+    LAPH_CUDA_TRY(cudaEventRecord(s->evf[1], s->st));
+    LAPH_TRY(iteration_rr(s, 0));
+    s->cnt[2] += (s->mdeg - 1) + 6;
+    float f = 0.f;
+    LAPH_CUDA_TRY(cudaEventSynchronize(s->evf[1]));
+    LAPH_CUDA_TRY(cudaEventElapsedTime(&f, s->evf[0], s->evf[1]));
+    filt_ms += f;
+  }
+  LAPH_TRY(phase_fix(s->d_pd, s->st_col, s->np, s->nb_col, s->V, s->phases, s->norms, o.phase_fix, s->st));
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev2, s->st));
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->hps.data(), s->d_ps, s->np * sizeof(ProbState), cudaMemcpyDeviceToHost, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  float a = 0.f, b = 0.f;
+  cudaEventElapsedTime(&a, s->ev0, s->ev1);
+  cudaEventElapsedTime(&b, s->ev0, s->ev2);
+  s->ms[0] = a;
+  s->ms[1] = filt_ms;
+  s->ms[3] = b;
+  s->ms[2] = b - a - filt_ms;
+  s->ran = 1;
+  int status = LAPH_OK;
+  std::vector<double> nrm(s->blk_total ? 0 : 0);
+  for (int i = 0; i < s->np; ++i) {
+    const ProbState& p = s->hps[i];
+    if (p.active) status = LAPH_ENOTCONV;
+    if (res) {
+      laph_result& r = res[i];
+      r.status = p.active ? LAPH_ENOTCONV : LAPH_OK;
+      r.iters = p.iters;
+      r.nconv = p.nconv;
+      r.deg = s->mdeg;
+      r.lam_cut0 = o.lam_cut;
+      r.lam_max = p.lam_max;
+      r.max_resid = p.max_resid;
+      std::vector<double> nv(s->hd[i].nev);
+      cudaMemcpy(nv.data(), s->norms + s->hd[i].kv, nv.size() * sizeof(double), cudaMemcpyDeviceToHost);
+      double tr = 0.0;
+      for (double v : nv) tr += v;
+      r.trace_vdv = tr;
+    }
+  }
+  if (status != LAPH_OK) set_error("laph_solver_run: max_it = %d reached before all problems converged", o.max_it);
+  return status;
+}
+
+int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double* phases, int on_device) {
+  if (!s || i < 0 || i >= s->np || !s->ran) {
+    set_error("laph_solver_get: bad argument or solver not run");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  const ProbDesc& d = s->hd[i];
+  const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (evals) {
+    std::vector<double> th(d.nev);
+    LAPH_CUDA_TRY(cudaMemcpy(th.data(), s->theta + d.kv, d.nev * sizeof(double), cudaMemcpyDeviceToHost));
+    for (auto& v : th) v = -v;  // eigenvalues of Delta (recover_spectrum convention)
+    LAPH_CUDA_TRY(cudaMemcpy(evals, th.data(), d.nev * sizeof(double), on_device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost));
+  }
+  if (evecs) LAPH_CUDA_TRY(cudaMemcpy(evecs, s->V + d.blk, (size_t)d.dim * d.nev * sizeof(double2), kd));
+  if (phases) LAPH_CUDA_TRY(cudaMemcpy(phases, s->phases + d.kv, d.nev * sizeof(double), kd));
+  return LAPH_OK;
+}
+
+int laph_solver_timings(laph_solver* s, double* ms4) {
+  if (!s || !ms4) return LAPH_EINVAL;
+  for (int i = 0; i < 4; ++i) ms4[i] = s->ms[i];
+  return LAPH_OK;
+}
+
+int laph_solver_counters(laph_solver* s, long long* c3) {
+  if (!s || !c3) return LAPH_EINVAL;
+  for (int i = 0; i < 3; ++i) c3[i] = s->cnt[i];
+  return LAPH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+"""Batched block solver (laph_solver) vs a dense FP64 eigendecomposition of the
+assembled -Delta built by the oracle: eigenvalues <= 1e-10 relative, residual
+||(-Delta)v - lambda v|| / lambda_max <= tol, tr(V^dag V) = nev, phase-fixed
+eigenvectors (subspace projectors for clusters), smearing inside the solver."""
+import numpy as np
+import pytest
+
+from conftest import random_links
+
+pytestmark = pytest.mark.gpu
+
+
+def dense_ref(orc, U, L):
+    A = orc.neglap_dense(U, L)
+    w, X = np.linalg.eigh(A)
+    return A, w, X
+
+
+def check_solution(A, w, X, ev, V, ph, nev, tol):
+    lam = -ev
+    assert np.all(np.diff(lam) >= -1e-12)  # ascending lambda
+    assert np.abs(lam - w[:nev]).max() / w[-1] <= 1e-10
+    R = A @ V - V * lam[None, :]
+    res = np.linalg.norm(R, axis=0) / 12.0
+    assert res.max() <= tol * 1.01, res.max()
+    VdV = V.conj().T @ V
+    assert abs(np.trace(VdV).real - nev) <= 1e-9
+    assert np.abs(VdV - np.eye(nev)).max() <= 1e-10
+    # phase fix: first entry real and >= 0
+    assert np.abs(V[0].imag).max() <= 1e-13 and (V[0].real >= -1e-15).all()
+    assert np.allclose(ph, np.angle(ph * 0 + np.exp(1j * ph)))
+    # eigenvectors: subspace projectors over clusters (gap < 1e-6 lambda_max)
+    i = 0
+    while i < nev:
+        j = i + 1
+        while j < len(w) and w[j] - w[j - 1] < 1e-6 * w[-1]:
+            j += 1
+        if j <= nev:
+            P = V[:, i:j] @ V[:, i:j].conj().T
+            Pr = X[:, i:j] @ X[:, i:j].conj().T
+            assert np.abs(P - Pr).max() <= 1e-8
+        i = j
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+@pytest.mark.parametrize("L,nev", [(6, 20), (8, 40)])
+def test_block_solver_matches_dense(gpu, orc, L, nev, prec):
+    U = random_links(L, 0.4, 2000 + L)
+    tol = 1e-10
+    s = gpu.Solver([(L, nev)], guard=16, tol=tol, deg=10, max_it=300,
+                   link_prec=gpu.LINKS_BF16 if prec == "bf16" else gpu.LINKS_FP32)
+    s.set_links(0, U)
+    st, res = s.run()
+    assert st == 0, res
+    ev, V, ph = s.get(0)
+    A, w, X = dense_ref(orc, U, L)
+    check_solution(A, w, X, ev, V, ph, nev, tol)
+    assert abs(res[0]["trace_vdv"] - nev) < 1e-9
+    s.close()
+
+
+def test_block_solver_uneven_batch_with_smearing(gpu, orc):
+    """One launch mixing volumes and nev; stout smearing inside the solver."""
+    probs = [(6, 20), (8, 36), (6, 12), (4, 10)]
+    links = [random_links(L, 0.4, 3000 + i) for i, (L, _) in enumerate(probs)]
+    tol = 1e-10
+    s = gpu.Solver(probs, guard=16, tol=tol, deg=8, max_it=400, smear_kind=gpu.SMEAR_STOUT,
+                   smear_p1=0.1, smear_iters=3, smear_compat=1, link_prec=gpu.LINKS_FP32)
+    for i, U in enumerate(links):
+        s.set_links(i, U)
+    st, res = s.run()
+    assert st == 0, res
+    for i, (L, nev) in enumerate(probs):
+        Us = orc.smear_stout(links[i], L, 0.1, 3, 1)
+        A, w, X = dense_ref(orc, Us, L)
+        ev, V, ph = s.get(i)
+        check_solution(A, w, X, ev, V, ph, nev, tol)
+    s.close()
+
+
+def test_block_solver_repeatable(gpu):
+    L, nev = 6, 16
+    U = random_links(L, 0.4, 5)
+    out = []
+    for _ in range(2):
+        s = gpu.Solver([(L, nev)], tol=1e-10, deg=8)
+        s.set_links(0, U)
+        s.run()
+        out.append(s.get(0))
+        s.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
