@@ -1,0 +1,367 @@
+#!/usr/bin/env python3
+"""bench.py -- timeslices/s of the per-timeslice LapH eigensystem path on B200.
+
+Workload (one "step"): every timeslice of a seeded synthetic 32^3 x 64 gauge
+field (U = exp(i*0.3*H), stout-smeared 5 x rho=0.1 on the device in FP64),
+solved for the lowest nev = 120 eigenpairs of -Delta to a residual
+||(-Delta)v - lambda v|| / (||v|| lambda_max) <= 1e-9 by the batched block
+solver (FP32 filter matvecs with BF16 links + per-site scale, FP64 Gram /
+Cholesky / Rayleigh-Ritz / residuals), phase-fixed.  All 64 timeslices run as
+one batch.
+
+value : timeslices/s with links resident in HBM (device-timed, CUDA events on
+        the solver's stream, K steps between barriers, max over ranks).
+e2e   : the same through the public C ABI with host buffers: each step copies
+        the links from pinned host memory and reads every eigenpair back.
+roofline: lap_cheb_mrhs (the FP32 multi-RHS Chebyshev stencil), algorithmic
+        bytes / its event-timed duration, against the measured HBM copy peak.
+cpu_baseline: the CPU FP64 oracle (restated reference ev_ts path: stout
+        smearing + Krylov-Schur on T_DEG(B)) on one timeslice of the same
+        workload, all host cores.
+
+--impl reference runs that CPU path as the reference arm.
+Multi-GPU (torchrun): timeslices are independent; each rank solves its own
+64-timeslice batch (weak scaling), no collective on the data path.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # 32^3 x 64, eps 0.3, stout 5 x 0.1, nev 120 (+16 guard), BF16 links
+    "c3": dict(L=32, T=64, eps=0.3, seed=1229, smear="stout", p1=0.1, p2=0.0, iters=5, compat=1, nev=120,
+               guard=16, link_prec="bf16", tol=1e-9, deg=32),
+    # 24^3 x 48, eps 0.3, HYP 0.62/0.62 x 1, nev 120
+    "c2": dict(L=24, T=48, eps=0.3, seed=1228, smear="hyp", p1=0.62, p2=0.62, iters=1, compat=0, nev=120,
+               guard=16, link_prec="fp32", tol=1e-9, deg=12),
+    # 8^3 x 16, eps 0.4, stout 3 x 0.1, nev 60
+    "c1": dict(L=8, T=16, eps=0.4, seed=1227, smear="stout", p1=0.1, p2=0.0, iters=3, compat=1, nev=60,
+               guard=16, link_prec="fp32", tol=1e-9, deg=8),
+}
+HBM_FALLBACK = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def filter_bytes(m, kb, link_bytes):
+    """Algorithmic bytes of one filter pass (m-1 launches) per site-vector, and
+    the link bytes per site per column block per launch.
+    step 1 : read S, write E2                     (FP32 complex, 24 B each)
+    step 2 : read E2, S, write E3
+    step n : read E_n, E_{n-1}, S, write E_{n+1}
+    final  : as its step, but reads V (FP64) and writes W (FP64) instead of E_m."""
+    per = 0
+    for n in range(1, m):
+        reads = 1 if n == 1 else (2 if n == 2 else 3)
+        if n == m - 1:
+            per += reads * 24 + 48 + 48
+        else:
+            per += reads * 24 + 24
+    return per, link_bytes
+
+
+def generate_links(cfg, seed_offset=0):
+    import laph_eigsys_b200 as lb
+    conf = lb.gauge_random(cfg["L"], cfg["T"], cfg["eps"], cfg["seed"] + seed_offset)
+    return np.ascontiguousarray(conf[:, :, 1:4])  # (T, V3, 3, 3, 3) spatial links
+
+
+def make_solver(cfg, device):
+    import laph_eigsys_b200 as lb
+    kinds = {"stout": lb.SMEAR_STOUT, "ape": lb.SMEAR_APE, "hyp": lb.SMEAR_HYP, "none": lb.SMEAR_NONE}
+    probs = [(cfg["L"], cfg["nev"])] * cfg["T"]
+    return lb.Solver(probs, device=device, smear_kind=kinds[cfg["smear"]], smear_p1=cfg["p1"], smear_p2=cfg["p2"],
+                     smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
+                     link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
+                     max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227)
+
+
+def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
+    """One timeslice of the reference ev_ts path on the CPU oracle: smear + Krylov-Schur on T_DEG(B)."""
+    import oracle as orc
+    orc.set_threads(threads)
+    L = cfg["L"]
+    t0 = time.perf_counter()
+    if cfg["smear"] == "stout":
+        Us = orc.smear_stout(links_ts, L, cfg["p1"], cfg["iters"], cfg["compat"])
+    elif cfg["smear"] == "ape":
+        Us = orc.smear_ape(links_ts, L, cfg["p1"], cfg["iters"], cfg["compat"])
+    elif cfg["smear"] == "hyp":
+        Us = orc.smear_hyp(links_ts, L, cfg["p1"], cfg["p2"], cfg["iters"])
+    else:
+        Us = links_ts
+    st, theta, V, nconv, its, nmv = orc.eps_solve(Us, L, 12.0, lam_c, deg_ref, cfg["nev"], tol=1e-10, max_it=100)
+    Vf, ph = orc.fix_phase(V)
+    dt = time.perf_counter() - t0
+    return dt, dict(status=st, nconv=nconv, restarts=its, matvecs=nmv)
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    links = generate_links(cfg)
+    lam_c = cfg.get("lam_c_ref", 0.65)
+    deg_ref = 12
+    for _ in range(args.warmup):
+        cpu_reference_step(cfg, links[0], lam_c, deg_ref, threads)
+    tot = 0.0
+    info = None
+    for k in range(args.steps):
+        dt, info = cpu_reference_step(cfg, links[k % cfg["T"]], lam_c, deg_ref, threads)
+        tot += dt
+    value = args.steps / tot
+    sample = (f"1 timeslice per step ({cfg['L']}^3, nev {cfg['nev']}, smear + Krylov-Schur on T_{deg_ref}(B), "
+              f"LAM_L 12, LAM_C {lam_c}, tol 1e-10)")
+    line = {"impl": "reference", "metric": "timeslices/s to nev pairs @resid<=1e-9", "value": value,
+            "unit": "timeslices/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": workload_config(cfg),
+            "cpu_baseline": {"value": value, "unit": "timeslices/s", "cores": threads, "kind": "port",
+                             "sample": sample, "last": info},
+            "e2e": {"value": value, "unit": "timeslices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(cfg):
+    return {"workload": f"{cfg['L']}^3x{cfg['T']} eps {cfg['eps']} {cfg['smear']} {cfg['iters']}x{cfg['p1']}, "
+                        f"nev {cfg['nev']} (+{cfg['guard']} guard), resid<=1e-9",
+            "L": cfg["L"], "timeslices": cfg["T"], "nev": cfg["nev"], "guard": cfg["guard"], "deg": cfg["deg"],
+            "links": cfg["link_prec"], "filter": "fp32", "rayleigh_ritz": "fp64",
+            "l2": "inputs larger than L2 (each 64-timeslice block of vectors is 8 GB)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    ap.add_argument("--deg", type=int, default=None)
+    ap.add_argument("--link-prec", default=None, choices=["bf16", "fp32"])
+    ap.add_argument("--timeslices", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    cfg = dict(CONFIGS[args.config])
+    if args.deg:
+        cfg["deg"] = args.deg
+    if args.link_prec:
+        cfg["link_prec"] = args.link_prec
+    if args.timeslices:
+        cfg["T"] = args.timeslices
+    if args.impl == "reference":
+        return run_reference(args, cfg)
+
+    import torch
+    import laph_eigsys_b200 as lb
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    links = generate_links(cfg, seed_offset=rank * 1000)
+    T, L, nev = cfg["T"], cfg["L"], cfg["nev"]
+    solver = make_solver(cfg, local)
+    for i in range(T):
+        solver.set_links(i, links[i])
+    stream = torch.cuda.ExternalStream(solver.stream())
+
+    results = None
+    for _ in range(args.warmup):
+        st, results = solver.run()
+        if st != 0:
+            raise RuntimeError(f"solver did not converge: {results[:2]}")
+
+    # ---- value: links resident in HBM --------------------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    filt_ms, fsv, flaunch, launches, iters = 0.0, 0, 0, 0, []
+    e0.record(stream)
+    for _ in range(args.steps):
+        st, results = solver.run()
+        if st != 0:
+            raise RuntimeError("solver did not converge in a timed step")
+        tm = solver.timings()
+        cn = solver.counters()
+        filt_ms += tm[1]
+        fsv += cn[0]
+        flaunch += cn[1]
+        launches += cn[2]
+        iters.append(max(r["iters"] for r in results))
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms)
+    value = world * T * args.steps / (ms_max / 1000.0)
+    max_resid = max(r["max_resid"] for r in results)
+
+    # ---- roofline of lap_cheb_mrhs -----------------------------------------
+    m = cfg["deg"]
+    kb = 32
+    per_sv, _ = filter_bytes(m, kb, 0)
+    k = -(-(nev + cfg["guard"]) // 32) * 32
+    link_b = 112 if cfg["link_prec"] == "bf16" else 216
+    sv_iter = fsv / (m - 1)  # site-vectors per filter pass, summed over passes
+    site_blocks = sv_iter / kb  # site x column-block pairs per pass
+    alg_bytes = sv_iter * per_sv + site_blocks * (m - 1) * link_b
+    hbm, src = peaks()
+    achieved = alg_bytes / (filt_ms / 1000.0) / 1e9 if filt_ms > 0 else None
+    roofline = {"kernel": "k_cheb_mrhs (lap_cheb_mrhs)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm if achieved else None, "peak_source": src,
+                "traffic": None, "avg_launch_ms": filt_ms / max(flaunch, 1),
+                "bytes_per_launch": alg_bytes / max(flaunch, 1),
+                "filter_share_of_step": filt_ms / ms if ms > 0 else None}
+
+    # ---- e2e through the public API with host buffers ----------------------
+    e2e = None
+    if not args.no_e2e:
+        pin = torch.empty((T,) + links.shape[1:], dtype=torch.complex128, pin_memory=True)
+        pin.numpy()[...] = links
+        hl = pin.numpy()
+        dim = 3 * L ** 3
+        vbuf = torch.empty((nev, dim), dtype=torch.complex128, pin_memory=True).numpy().T  # column-major view
+        ebuf = np.empty(nev)
+        pbuf = np.empty(nev)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            for i in range(T):
+                solver.set_links(i, hl[i])
+            st, _ = solver.run()
+            for i in range(T):
+                solver.get_into(i, ebuf, vbuf, pbuf)
+        f1.record(stream)
+        barrier()
+        ems = max_over_ranks(f0.elapsed_time(f1))
+        e2e = {"value": world * T * args.steps / (ems / 1000.0), "unit": "timeslices/s",
+               "h2d_bytes_per_step": int(T * L ** 3 * 27 * 16),
+               "d2h_bytes_per_step": int(T * (nev * 8 + dim * nev * 16 + nev * 8)),
+               "ms_per_step": ems / args.steps}
+
+    # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ev0, _, _ = solver.get(0, vectors=False)
+        lam = -ev0
+        lam_c = float(1.1 * lam[-1])
+        threads = os.cpu_count() or 1
+        dt, info = cpu_reference_step(cfg, links[0], lam_c, 12, threads)
+        cpu = {"value": 1.0 / dt, "unit": "timeslices/s", "cores": threads, "kind": "port",
+               "sample": f"timeslice 0 of the workload: {cfg['smear']} smearing + Krylov-Schur on T_12(B), "
+                         f"LAM_L 12, LAM_C {lam_c:.4f} (1.1 x lambda_nev from this run), tol 1e-10",
+               "seconds": dt, "detail": info}
+
+    if rank == 0:
+        line = {"metric": "timeslices/s to nev pairs @resid<=1e-9", "value": value, "unit": "timeslices/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
+                "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "detail": {"outer_iterations": iters, "max_resid": max_resid, "filter_ms_per_step": filt_ms / args.steps,
+                           "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
+                                                       solver.timings()))}}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -154,6 +154,9 @@ int laph_solver_run(laph_solver* s, laph_result* results);
 /* Fetch problem i: evals[nev] (reference convention, see top), evecs column-major
  * complex128 [3*V3][nev] (may be NULL), phases[nev] (may be NULL). */
 int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double* phases, int on_device);
+/* The CUDA stream (cudaStream_t) every kernel and copy of the solver runs on,
+ * for callers that time or order work around laph_solver_run. */
+int laph_solver_stream(laph_solver* s, void** stream);
 /* Device-side timing of the last run (ms): smearing, filter, dense, total. */
 int laph_solver_timings(laph_solver* s, double* ms4);
 /* Counters of the last run for roofline accounting: filter site-vector-steps,

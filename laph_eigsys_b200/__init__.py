@@ -243,6 +243,16 @@ class Solver:
                                   _ptr(ph), 0), "laph_solver_get")
         return ev, V, ph
 
+    def stream(self):
+        h = ctypes.c_void_p()
+        check(lib.laph_solver_stream(self._h, ctypes.byref(h)), "laph_solver_stream")
+        return h.value
+
+    def get_into(self, i, evals, evecs, phases):
+        """Fetch problem i into caller-provided host arrays (e.g. pinned)."""
+        check(lib.laph_solver_get(self._h, i, _ptr(evals), ctypes.c_void_p(evecs.ctypes.data) if evecs is not None
+                                  else None, _ptr(phases), 0), "laph_solver_get")
+
     def timings(self):
         t = (ctypes.c_double * 4)()
         check(lib.laph_solver_timings(self._h, t), "laph_solver_timings")

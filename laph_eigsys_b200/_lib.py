@@ -84,6 +84,7 @@ _sig("laph_solver_destroy", c_int, c_void_p)
 _sig("laph_solver_set_links", c_int, c_void_p, c_int, c_void_p, c_int, c_int)
 _sig("laph_solver_run", c_int, c_void_p, P(laph_result))
 _sig("laph_solver_get", c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int)
+_sig("laph_solver_stream", c_int, c_void_p, P(c_void_p))
 _sig("laph_solver_timings", c_int, c_void_p, P(c_double))
 _sig("laph_solver_counters", c_int, c_void_p, P(c_ll))
 _sig("laph_gauge_random", c_int, c_void_p, c_int, c_int, c_double, c_u64)

@@ -48,7 +48,7 @@ struct laph_solver {
       *st_rot = nullptr, *st_rand = nullptr, *st_col = nullptr;
   int nb_site = 0, nb_filt = 0, nb_nl = 0, nb_gram = 0, nb_gred = 0, nb_rot = 0, nb_rand = 0, nb_col = 0;
   // pools
-  double2 *U64 = nullptr, *Utmp = nullptr, *dec = nullptr;
+  double2 *U64raw = nullptr, *U64 = nullptr, *Utmp = nullptr, *dec = nullptr, *stage = nullptr;
   float2* Uf32 = nullptr;
   void* Ubf = nullptr;
   float* scale = nullptr;
@@ -114,7 +114,7 @@ int laph_solver_destroy(laph_solver* s) {
   cudaSetDevice(s->dev);
   if (s->st) cudaStreamSynchronize(s->st);
   void* ptrs[] = {s->d_pd, s->d_ps, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
-                  s->st_col, s->U64, s->Utmp, s->dec, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
+                  s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
                   s->phases, s->norms, s->d_nactive};
   for (void* p : ptrs)
@@ -169,7 +169,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   }
   // descriptors and pool offsets
   long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
-  size_t max_run = 0;
+  size_t max_run = 0, max_v3 = 0;
   std::vector<int> per_site, per_filt, per_nl, per_gram, per_gred, per_rot, per_rand, per_col;
   for (int i = 0; i < n; ++i) {
     ProbDesc d{};
@@ -202,6 +202,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     o_rp += (long long)d.nrt * d.k;
     o_tc += (long long)(s->mdeg + 1) * 3 * d.k;
     s->hd.push_back(d);
+    max_v3 = std::max(max_v3, (size_t)d.V3);
     const int nst = (d.V3 + 127) / 128;
     per_site.push_back(nst);
     per_filt.push_back(nst * ((d.k + s->kb - 1) / s->kb));
@@ -221,8 +222,8 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   }
   s->blk_total = (size_t)o_blk;
   int rc = LAPH_OK;
-  if ((rc = dalloc(&s->d_pd, n)) || (rc = dalloc(&s->d_ps, n)) || (rc = dalloc(&s->U64, o_u64)) ||
-      (rc = dalloc(&s->Utmp, max_run)) || (rc = dalloc(&s->dec, max_run * 2)) ||
+  if ((rc = dalloc(&s->d_pd, n)) || (rc = dalloc(&s->d_ps, n)) || (rc = dalloc(&s->U64, o_u64)) || (rc = dalloc(&s->U64raw, o_u64)) ||
+      (rc = dalloc(&s->Utmp, max_run)) || (rc = dalloc(&s->stage, 36 * max_v3)) || (rc = dalloc(&s->dec, max_run * 2)) ||
       (rc = dalloc(&s->scale, o_sc)) || (rc = dalloc(&s->V, o_blk)) || (rc = dalloc(&s->W, o_blk)) ||
       (rc = dalloc(&s->Y, o_blk)) || (rc = dalloc(&s->S, o_blk)) || (rc = dalloc(&s->E[0], o_blk)) ||
       (rc = dalloc(&s->E[1], o_blk)) || (rc = dalloc(&s->E[2], o_blk)) || (rc = dalloc(&s->KK, o_kk)) ||
@@ -265,7 +266,7 @@ int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout
   }
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const ProbDesc& d = s->hd[i];
-  double2* dst = s->U64 + d.u64;
+  double2* dst = s->U64raw + d.u64;  // pristine copy; run() smears a working copy
   if (on_device) {
     if (layout != LAPH_LAYOUT_ROWMAJOR && layout != LAPH_LAYOUT_CONF) {
       set_error("laph_solver_set_links: device links must be ROWMAJOR or CONF");
@@ -274,6 +275,11 @@ int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout
     // device-side reorder to site-minor order through a host-free path:
     // copy to the scratch and transpose with a small kernel
     LAPH_TRY(links_to_soa_device(links, layout, d.V3, dst, s->st));
+  } else if (layout == LAPH_LAYOUT_ROWMAJOR || layout == LAPH_LAYOUT_CONF) {
+    // raw copy into the staging area, reorder on the device
+    const size_t n = (layout == LAPH_LAYOUT_CONF ? 36 : 27) * (size_t)d.V3;
+    LAPH_CUDA_TRY(cudaMemcpyAsync(s->stage, links, n * sizeof(double2), cudaMemcpyHostToDevice, s->st));
+    LAPH_TRY(links_to_soa_device(reinterpret_cast<const double*>(s->stage), layout, d.V3, dst, s->st));
   } else {
     std::vector<double2> soa(27 * (size_t)d.V3);
     LAPH_TRY(links_to_soa(links, layout, d.V3, soa.data()));
@@ -326,12 +332,16 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const laph_solve_opts& o = s->o;
   LAPH_CUDA_TRY(cudaEventRecord(s->ev0, s->st));
+  long long nlaunch = 0;
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->U64, s->U64raw, s->hd.back().u64 * sizeof(double2) + 27 * sizeof(double2) * s->hd.back().V3,
+                                cudaMemcpyDeviceToDevice, s->st));
   // smearing, per run of equal L
   for (int i = 0; i < s->np;) {
     int j = i;
     while (j < s->np && s->hd[j].L == s->hd[i].L) ++j;
     LAPH_TRY(smear_batch(s->U64 + s->hd[i].u64, s->Utmp, s->dec, s->hd[i].L, j - i, o.smear_kind, o.smear_p1,
                          o.smear_p2, o.smear_iters, o.smear_compat, s->st));
+    if (o.smear_kind != LAPH_SMEAR_NONE) nlaunch += (long long)o.smear_iters * (o.smear_kind == LAPH_SMEAR_HYP ? 2 : 1);
     i = j;
   }
   LAPH_TRY(pack_links(s->d_pd, s->st_site, s->np, s->nb_site, s->U64, s->Uf32, s->Ubf, s->scale,
@@ -348,6 +358,7 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->W, o.seed, s->st));
   LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
   LAPH_TRY(iteration_rr(s, 1));
+  nlaunch += 2 + 6;  // pack, random block, first Rayleigh-Ritz
   s->cnt[0] = s->cnt[1] = s->cnt[2] = 0;
   double filt_ms = 0.0;
   if (s->evf.empty()) {
@@ -368,13 +379,14 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     LAPH_TRY(filter(s));
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[1], s->st));
     LAPH_TRY(iteration_rr(s, 0));
-    s->cnt[2] += (s->mdeg - 1) + 6;
+    nlaunch += (s->mdeg - 1) + 6;
     float f = 0.f;
     LAPH_CUDA_TRY(cudaEventSynchronize(s->evf[1]));
     LAPH_CUDA_TRY(cudaEventElapsedTime(&f, s->evf[0], s->evf[1]));
     filt_ms += f;
   }
   LAPH_TRY(phase_fix(s->d_pd, s->st_col, s->np, s->nb_col, s->V, s->phases, s->norms, o.phase_fix, s->st));
+  s->cnt[2] = nlaunch + 1;
   LAPH_CUDA_TRY(cudaEventRecord(s->ev2, s->st));
   LAPH_CUDA_TRY(cudaMemcpyAsync(s->hps.data(), s->d_ps, s->np * sizeof(ProbState), cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
@@ -421,12 +433,24 @@ int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double*
   const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (evals) {
     std::vector<double> th(d.nev);
-    LAPH_CUDA_TRY(cudaMemcpy(th.data(), s->theta + d.kv, d.nev * sizeof(double), cudaMemcpyDeviceToHost));
+    LAPH_CUDA_TRY(cudaMemcpyAsync(th.data(), s->theta + d.kv, d.nev * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
     for (auto& v : th) v = -v;  // eigenvalues of Delta (recover_spectrum convention)
     LAPH_CUDA_TRY(cudaMemcpy(evals, th.data(), d.nev * sizeof(double), on_device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost));
   }
-  if (evecs) LAPH_CUDA_TRY(cudaMemcpy(evecs, s->V + d.blk, (size_t)d.dim * d.nev * sizeof(double2), kd));
-  if (phases) LAPH_CUDA_TRY(cudaMemcpy(phases, s->phases + d.kv, d.nev * sizeof(double), kd));
+  if (evecs)
+    LAPH_CUDA_TRY(cudaMemcpyAsync(evecs, s->V + d.blk, (size_t)d.dim * d.nev * sizeof(double2), kd, s->st));
+  if (phases) LAPH_CUDA_TRY(cudaMemcpyAsync(phases, s->phases + d.kv, d.nev * sizeof(double), kd, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return LAPH_OK;
+}
+
+int laph_solver_stream(laph_solver* s, void** stream) {
+  if (!s || !stream) {
+    set_error("laph_solver_stream: bad argument");
+    return LAPH_EINVAL;
+  }
+  *stream = static_cast<void*>(s->st);
   return LAPH_OK;
 }
 

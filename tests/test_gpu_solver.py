@@ -89,3 +89,17 @@ def test_block_solver_repeatable(gpu):
         out.append(s.get(0))
         s.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_same_solver_runs_twice(gpu):
+    """run() smears a fresh copy of the stored links every time."""
+    L, nev = 6, 12
+    U = random_links(L, 0.4, 6)
+    s = gpu.Solver([(L, nev)], tol=1e-10, deg=8, smear_kind=gpu.SMEAR_APE, smear_p1=0.5, smear_iters=2)
+    s.set_links(0, U)
+    s.run()
+    a = s.get(0)
+    s.run()
+    b = s.get(0)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    s.close()
