@@ -93,6 +93,20 @@ int laph_smear(laph_ctx* ctx, int kind, double p1, double p2, int iters, int com
  * :226-244).  deg >= 1 (deg = 1 gives B x).  x, y: complex128[3*V3];
  * on_device = 0 for host pointers (staged), 1 for device pointers. */
 int laph_matmult(laph_ctx* ctx, const double* x, double* y, int deg, int on_device);
+/* laph_matmult_noalloc: the same y = T_deg(B) x in FP64 without any device
+ * allocation, for callers that cannot call cudaMalloc (inside another
+ * library's stream capture, under a framework that owns the device memory
+ * budget, or after a service's start-up).  No counterpart in the reference.
+ * links: device pointer, LAPH_LAYOUT_ROWMAJOR, one timeslice of L^3 sites;
+ * x, y: device pointers, complex128[3*L^3]; work is queued on `stream`
+ * (a cudaStream_t, 0 = legacy default) and the call returns without waiting.
+ * The two Chebyshev temporaries live in a fixed file-scope device array of
+ * 3 MiB that holds timeslices up to L = 32; larger L returns LAPH_EINVAL.
+ * The first call on each device resolves that array's address (make it
+ * before any stream capture).  Calls that overlap on the GPU share the array
+ * and race: serialise them on one stream. */
+int laph_matmult_noalloc(const double* links, int L, double lam_l, double lam_c, int deg, const double* x,
+                         double* y, void* stream);
 /* y = (-Delta) x = 6x - hop(x) in FP64 (for residuals). */
 int laph_apply_neglap(laph_ctx* ctx, const double* x, double* y, int on_device);
 /* MatGetDiagonal_Laplacian2D (shell_matop.cpp:248-255): fills diag with -6. */

@@ -75,6 +75,7 @@ _sig("laph_set_links", c_int, c_void_p, c_void_p, c_int)
 _sig("laph_get_links", c_int, c_void_p, c_void_p, c_int)
 _sig("laph_smear", c_int, c_void_p, c_int, c_double, c_double, c_int, c_int)
 _sig("laph_matmult", c_int, c_void_p, c_void_p, c_void_p, c_int, c_int)
+_sig("laph_matmult_noalloc", c_int, c_void_p, c_int, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p)
 _sig("laph_apply_neglap", c_int, c_void_p, c_void_p, c_void_p, c_int)
 _sig("laph_get_diagonal", c_int, c_void_p, c_void_p, c_int)
 _sig("laph_plaquette", c_int, c_void_p, P(c_double))
