@@ -142,7 +142,8 @@ def make_solver(cfg, device):
     return lb.Solver(probs, device=device, smear_kind=kinds[cfg["smear"]], smear_p1=cfg["p1"], smear_p2=cfg["p2"],
                      smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
                      link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
-                     max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227)
+                     max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
+                     filter_kernel=cfg.get("filter_kernel", 0))
 
 
 def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
@@ -163,6 +164,38 @@ def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
     Vf, ph = orc.fix_phase(V)
     dt = time.perf_counter() - t0
     return dt, dict(status=st, nconv=nconv, restarts=its, matvecs=nmv)
+
+
+def plain_gpu(cfg, links, lam_c, ntimeslices, device, deg_ref=12):
+    """The plain GPU form of the same workload: per timeslice, links into a
+    MatShell context, smearing on the device, SLEPc-style Krylov-Schur on
+    T_DEG(B) with the Krylov basis in device memory driving the GPU MatMult,
+    then recover_spectrum and fix_phase -- the reference's ev_ts loop body with
+    the MatShell product on the GPU."""
+    import torch
+    import laph_eigsys_b200 as lb
+    kinds = {"stout": lb.SMEAR_STOUT, "ape": lb.SMEAR_APE, "hyp": lb.SMEAR_HYP, "none": lb.SMEAR_NONE}
+    L, nev = cfg["L"], cfg["nev"]
+    ctx = lb.Context(L, 12.0, lam_c, deg_ref, device=device)
+    out = {"unit": "timeslices/s", "timeslices": ntimeslices, "basis": "device", "deg": deg_ref, "lam_l": 12.0,
+           "lam_c": lam_c, "tol": 1e-10, "ncv": "max(2 nev, nev+15)"}
+    t0 = time.perf_counter()
+    nmv, rs = 0, 0
+    for t in range(ntimeslices):
+        ctx.set_links(links[t])
+        ctx.smear(kinds[cfg["smear"]], cfg["p1"], cfg["p2"], cfg["iters"], cfg["compat"])
+        st, theta, V, nconv, its, nm = ctx.eps_solve(nev, tol=1e-10, max_it=100, device_basis=True)
+        if st != 0:
+            out["status"] = f"not converged on timeslice {t}"
+        lb.recover_spectrum(theta, deg_ref, 12.0, lam_c)
+        lb.fix_phase(V)
+        nmv += nm
+        rs += its
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    ctx.close()
+    out.update({"value": ntimeslices / dt, "seconds": dt, "matvecs": nmv, "restarts": rs})
+    return out
 
 
 def run_reference(args, cfg):
@@ -212,8 +245,12 @@ def main():
     ap.add_argument("--deg", type=int, default=None)
     ap.add_argument("--link-prec", default=None, choices=["bf16", "fp32"])
     ap.add_argument("--timeslices", type=int, default=None)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--filter-kernel", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--plain-timeslices", type=int, default=2)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
@@ -223,6 +260,8 @@ def main():
         cfg["link_prec"] = args.link_prec
     if args.timeslices:
         cfg["T"] = args.timeslices
+    cfg["block"] = args.block
+    cfg["filter_kernel"] = args.filter_kernel
     if args.impl == "reference":
         return run_reference(args, cfg)
 
@@ -291,7 +330,7 @@ def main():
 
     # ---- roofline of lap_cheb_mrhs -----------------------------------------
     m = cfg["deg"]
-    kb = 32
+    kb = cfg["block"] or 32
     per_sv, _ = filter_bytes(m, kb, 0)
     k = -(-(nev + cfg["guard"]) // 32) * 32
     link_b = 112 if cfg["link_prec"] == "bf16" else 216
@@ -333,6 +372,13 @@ def main():
                "d2h_bytes_per_step": int(T * (nev * 8 + dim * nev * 16 + nev * 8)),
                "ms_per_step": ems / args.steps}
 
+    # ---- plain GPU form: MatShell MatMult + Krylov-Schur, one timeslice at a time
+    plain = None
+    if rank == 0 and world == 1 and not args.no_plain:
+        ev0, _, _ = solver.get(0, vectors=False)
+        plain = plain_gpu(cfg, links, float(1.1 * (-ev0)[-1]), args.plain_timeslices, local)
+        plain["chosen_over_plain"] = value / plain["value"] if plain.get("value") else None
+
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -351,7 +397,7 @@ def main():
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid, "filter_ms_per_step": filt_ms / args.steps,
                            "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
                                                        solver.timings()))}}

@@ -114,6 +114,19 @@ int laph_get_diagonal(laph_ctx* ctx, double* diag, int on_device);
 /* Average spatial plaquette of the context's links (config_utils.cpp:388-426). */
 int laph_plaquette(laph_ctx* ctx, double* plaq);
 
+/* The plain form: SLEPc-style Krylov-Schur (EPS_HEP, EPS_LARGEST_MAGNITUDE,
+ * ncv <= 0 -> max(2 nev, nev + 15), convergence |beta s_i| <= tol |theta_i|)
+ * on T_deg(B) of the context (window and deg of laph_ctx_set_window), the
+ * EPSSolve of src/ev_ts.cpp:231-263 driving this library's MatMult.
+ * device_basis = 0: Krylov basis in host memory, every product through
+ * laph_matmult with host vectors (the reference's data flow); 1: basis in
+ * device memory (SLEPc with CUDA vectors).  theta_out[nev]: eigenvalues of
+ * T_deg(B) by decreasing |theta|; V_out (host, may be NULL): column-major
+ * complex128 [3 V3][nev] Ritz vectors.  LAPH_ENOTCONV if max_it restarts did
+ * not converge nev pairs (the reference silently sets nconv = nev). */
+int laph_eps_solve(laph_ctx* ctx, int nev, int ncv, double tol, int max_it, int device_basis, uint64_t seed,
+                   double* theta_out, double* V_out, int* nconv, int* restarts, long long* nmatvec);
+
 /* ---- batched block eigensolver (the "chosen" form) ------------------------
  * Solves many timeslices (possibly of different L and nev) in one batched,
  * device-resident Chebyshev-filtered subspace iteration: FP32 filter matvecs
@@ -144,6 +157,9 @@ typedef struct {
   int deg;              /* filter degree (<= 0: default)                          */
   int phase_fix;        /* apply fix_phase to the output eigenvectors             */
   uint64_t seed;        /* start block                                            */
+  int block;            /* columns per CTA of the filter kernel, 8..64 (0: 32)     */
+  int filter_kernel;    /* 0 auto, 1 register-resident links + L2 bulk prefetch,
+                           2 shared-memory staged rows (even L only)              */
 } laph_solve_opts;
 void laph_solve_opts_default(laph_solve_opts* o);
 

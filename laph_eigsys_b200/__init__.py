@@ -181,6 +181,19 @@ class Context:
         check(lib.laph_get_diagonal(self._h, _ptr(d), 0), "laph_get_diagonal")
         return d
 
+    def eps_solve(self, nev, ncv=0, tol=1e-10, max_it=100, device_basis=True, seed=1227, vectors=True):
+        """Plain form: Krylov-Schur on T_deg(B) driving this context's MatMult (laph_eps_solve).
+        Returns (status, theta[nev], V or None, nconv, restarts, nmatvec)."""
+        theta = np.empty(nev)
+        V = np.empty((self.dim, nev), dtype=np.complex128, order="F") if vectors else None
+        nconv, its, nmv = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        st = lib.laph_eps_solve(self._h, nev, ncv, tol, max_it, int(device_basis), seed, _ptr(theta),
+                                ctypes.c_void_p(V.ctypes.data) if vectors else None, ctypes.byref(nconv),
+                                ctypes.byref(its), ctypes.byref(nmv))
+        if st not in (_lib.LAPH_OK, _lib.LAPH_ENOTCONV):
+            check(st, "laph_eps_solve")
+        return st, theta, V, nconv.value, its.value, nmv.value
+
     def plaquette(self):
         p = ctypes.c_double()
         check(lib.laph_plaquette(self._h, ctypes.byref(p)), "laph_plaquette")

@@ -40,7 +40,7 @@ class laph_solve_opts(ctypes.Structure):
     _fields_ = [("smear_kind", c_int), ("smear_p1", c_double), ("smear_p2", c_double), ("smear_iters", c_int),
                 ("smear_compat", c_int), ("guard", c_int), ("link_prec", c_int), ("tol", c_double),
                 ("max_it", c_int), ("window", c_int), ("lam_cut", c_double), ("lam_max", c_double),
-                ("deg", c_int), ("phase_fix", c_int), ("seed", c_u64)]
+                ("deg", c_int), ("phase_fix", c_int), ("seed", c_u64), ("block", c_int), ("filter_kernel", c_int)]
 
 
 class laph_result(ctypes.Structure):
@@ -79,6 +79,7 @@ _sig("laph_matmult_noalloc", c_int, c_void_p, c_int, c_double, c_double, c_int, 
 _sig("laph_apply_neglap", c_int, c_void_p, c_void_p, c_void_p, c_int)
 _sig("laph_get_diagonal", c_int, c_void_p, c_void_p, c_int)
 _sig("laph_plaquette", c_int, c_void_p, P(c_double))
+_sig("laph_eps_solve", c_int, c_void_p, c_int, c_int, c_double, c_int, c_int, c_u64, c_void_p, c_void_p, P(c_int), P(c_int), P(c_ll))
 _sig("laph_solve_opts_default", None, P(laph_solve_opts))
 _sig("laph_solver_create", c_int, P(c_void_p), P(laph_problem), c_int, P(laph_solve_opts), c_int)
 _sig("laph_solver_destroy", c_int, c_void_p)

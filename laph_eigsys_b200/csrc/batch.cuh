@@ -21,6 +21,8 @@ struct ProbDesc {
   long long tc;    // Chebyshev coefficient table [(mdeg+1)][k]
   int nchunk;      // row chunks of the Gram reduction
   int nrt;         // row tiles of the rotation
+  int zr;          // z-rows per CTA of the staged filter (zr | L, zr*L <= 128)
+  int pad_;
 };
 
 // Window/state per problem, written by the device.
@@ -28,6 +30,7 @@ struct ProbState {
   double lam_cut, lam_max;   // Chebyshev window of this iteration
   double c_hop, c_diag;      // B = c_hop*hop + c_diag (maps [lam_cut, lam_max] -> [1, -1])
   double max_resid;          // max over wanted pairs of ||r|| / lam_max
+  double theta_min;          // smallest Ritz value
   int active;                // 1 while iterating
   int nconv;                 // wanted pairs at tolerance
   int iters;                 // outer iterations done

@@ -25,6 +25,26 @@ struct laph_ctx {
 
 using namespace laph;
 
+namespace laph {
+// Device view of a context for the in-library Krylov-Schur driver.
+int ctx_device_links(laph_ctx* c, const double2** U, int* L, double* lam_l, double* lam_c, int* deg, cudaStream_t* st,
+                     int* dev) {
+  if (!c) {
+    set_error("null context");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(c->dev));
+  *U = c->U;
+  *L = c->g.L;
+  *lam_l = c->lam_l;
+  *lam_c = c->lam_c;
+  *deg = c->deg;
+  *st = c->st;
+  *dev = c->dev;
+  return LAPH_OK;
+}
+}  // namespace laph
+
 namespace {
 int ctx_check(laph_ctx* c) {
   if (!c) {

@@ -4,8 +4,9 @@
 //   k_small       per problem: column scaling, Cholesky, triangular inverse,
 //                 projected Hermitian matrix, Jacobi eigensolve, sort, C,
 //                 next Chebyshev window and coefficient table
-//   k_rotate      V = W C,  R = Y C - V diag(theta),  S = s_j R (FP32),
-//                 residual partial sums
+//   k_rotate      V = W C
+//   k_residual64  R = (-Delta) V - V diag(theta) (FP64 stencil), S = -2 c_hop R
+//                 (FP32), residual partial sums
 //   k_resid       residual norms, convergence mask
 // These replace SLEPc's BV orthogonalisation and DS dense eigensolve inside
 // EPSSolve (src/ev_ts.cpp:263).  Complex FP64 on CUDA cores: B200 has no FP64
@@ -370,63 +371,69 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     S.c_hop = al;
     S.c_diag = (S.lam_max + cut - 12.0) / (S.lam_max - cut);
     S.chol_fail = s_flag;
+    S.theta_min = th[0];
   }
-  __syncthreads();
-  {
-    // Scaled recurrence.  With E_1 = S/2, E_0 = 0 and
-    //   E_{n+1} = 2B E_n - E_{n-1} + T_n(theta_B) S,
-    // T_m(B) V = V T_m(Theta_B) + E_m exactly (S = 2(BV - V Theta_B)).  Each
-    // column is carried as E'_n = E_n / nu_n, nu_n = max(1, |T_n|), so that
-    // every FP32 value stays O(|S|):
-    //   step 1: E'_2 = (B S + T_1 S) / nu_2
-    //   step 2: E'_3 = (2 nu_2 B E'_2 + (T_2 - 1/2) S) / nu_3
-    //   step n: E'_{n+1} = (2 nu_n B E'_n - nu_{n-1} E'_{n-1} + T_n S) / nu_{n+1}
-    //   final : W' = (T_m / nu_m) V + E'_m   (= W / nu_m)
-    const ProbState S = ps[p];
-    const int m = d.mdeg;
-    double* tc = tcoef + d.tc;
-    for (int j = tid; j < k; j += nt) {
-      const double tb = 1.0 + 2.0 * (S.lam_cut - th[j]) / (S.lam_max - S.lam_cut);
-      double tn[66], nu[66];
-      tn[0] = 1.0;
-      tn[1] = tb;
-      for (int n = 2; n <= m; ++n) tn[n] = 2.0 * tb * tn[n - 1] - tn[n - 2];
-      for (int n = 0; n <= m; ++n) nu[n] = fmax(1.0, fabs(tn[n]));
-      for (int n = 1; n < m; ++n) {
-        double a, z, g;
-        if (n == 1) {
-          a = 1.0 / nu[2];
-          z = 0.0;
-          g = tn[1] / nu[2];
-        } else if (n == 2) {
-          a = 2.0 * nu[2] / nu[3];
-          z = 0.0;
-          g = (tn[2] - 0.5) / nu[3];
-        } else {
-          a = 2.0 * nu[n] / nu[n + 1];
-          z = -nu[n - 1] / nu[n + 1];
-          g = tn[n] / nu[n + 1];
-        }
-        tc[((size_t)n * 3 + 0) * k + j] = a;
-        tc[((size_t)n * 3 + 1) * k + j] = z;
-        tc[((size_t)n * 3 + 2) * k + j] = g;
+}
+
+// ------------------------------------------------- Chebyshev coefficients --
+// Scaled recurrence for a filter of degree m (chosen by the host each
+// iteration).  With E_1 = S/2, E_0 = 0 and
+//   E_{n+1} = 2B E_n - E_{n-1} + T_n(theta_B) S,
+// T_m(B) V = V T_m(Theta_B) + E_m exactly (S = 2(BV - V Theta_B)).  Each
+// column is carried as E'_n = E_n / nu_n, nu_n = max(1, |T_n|), so every FP32
+// value stays O(|S|):
+//   step 1: E'_2 = (B S + T_1 S) / nu_2
+//   step 2: E'_3 = (2 nu_2 B E'_2 + (T_2 - 1/2) S) / nu_3
+//   step n: E'_{n+1} = (2 nu_n B E'_n - nu_{n-1} E'_{n-1} + T_n S) / nu_{n+1}
+//   final : W' = (T_m / nu_m) V + E'_m   (= W / nu_m)
+__global__ void k_coef(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, int np,
+                       const double* __restrict__ theta, double* __restrict__ tcoef, double* __restrict__ scol, int m) {
+  const int p = blockIdx.x;
+  if (p >= np || !ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const ProbState S = ps[p];
+  const int k = d.k;
+  const double* th = theta + d.kv;
+  double* tc = tcoef + d.tc;
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    const double tb = 1.0 + 2.0 * (S.lam_cut - th[j]) / (S.lam_max - S.lam_cut);
+    double tn[66], nu[66];
+    tn[0] = 1.0;
+    tn[1] = tb;
+    for (int n = 2; n <= m; ++n) tn[n] = 2.0 * tb * tn[n - 1] - tn[n - 2];
+    for (int n = 0; n <= m; ++n) nu[n] = fmax(1.0, fabs(tn[n]));
+    for (int n = 1; n < m; ++n) {
+      double a, z, g;
+      if (n == 1) {
+        a = 1.0 / nu[2];
+        z = 0.0;
+        g = tn[1] / nu[2];
+      } else if (n == 2) {
+        a = 2.0 * nu[2] / nu[3];
+        z = 0.0;
+        g = (tn[2] - 0.5) / nu[3];
+      } else {
+        a = 2.0 * nu[n] / nu[n + 1];
+        z = -nu[n - 1] / nu[n + 1];
+        g = tn[n] / nu[n + 1];
       }
-      tc[((size_t)m * 3 + 0) * k + j] = tn[m] / nu[m];
-      scol[d.kv + j] = -2.0 * S.c_hop;
+      tc[((size_t)n * 3 + 0) * k + j] = a;
+      tc[((size_t)n * 3 + 1) * k + j] = z;
+      tc[((size_t)n * 3 + 2) * k + j] = g;
     }
+    tc[((size_t)m * 3 + 0) * k + j] = tn[m] / nu[m];
+    scol[d.kv + j] = -2.0 * S.c_hop;
   }
 }
 
 // ---------------------------------------------------------------- rotate ---
-// CTA: 128 threads, tile 64 rows x 32 columns; thread: rows ty+16i, cols tx+8j.
+// V = W C.  CTA: 128 threads, tile 64 rows x 32 columns; thread: rows ty+16i,
+// columns tx+8j (4 x 4 complex accumulators).
 constexpr int RR = 64, RC = 32, RK = 16;
 
 __global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
                                                 const int* __restrict__ start, int np, const double2* __restrict__ Wp,
-                                                const double2* __restrict__ Yp, const double2* __restrict__ KK,
-                                                const double* __restrict__ theta, const double* __restrict__ scol,
-                                                double2* __restrict__ Vp, float2* __restrict__ Sp,
-                                                double* __restrict__ rpart) {
+                                                const double2* __restrict__ KK, double2* __restrict__ Vp) {
   const int p = find_prob(start, np, blockIdx.x);
   if (!ps[p].active) return;
   const ProbDesc d = pd[p];
@@ -437,82 +444,114 @@ __global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd,
   const int k = d.k;
   const double2* C = KK + d.kk;  // C in G storage, column-major k x k
   const double2* Wb = Wp + d.blk;
-  const double2* Yb = Yp + d.blk;
-  __shared__ double2 sW[RK][RR], sY[RK][RR], sC[RK][RC + 1];
+  __shared__ double2 sW[2][RK][RR], sC[2][RK][RC];
   const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
-  double2 av[4][4], ay[4][4];
+  double2 av[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) av[i][j] = ay[i][j] = make_double2(0.0, 0.0);
-  for (int q0 = 0; q0 < k; q0 += RK) {
-    // W, Y tiles: 16 columns x 64 rows each (coalesced along rows)
+    for (int j = 0; j < 4; ++j) av[i][j] = make_double2(0.0, 0.0);
+  auto load = [&](int q0, int b) {
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const int idx = threadIdx.x + 128 * e;
       const int c = idx >> 6, r = idx & 63;
       const int row = row0 + r;
-      const bool ok = row < d.dim;
-      sW[c][r] = ok ? __ldg(Wb + (size_t)(q0 + c) * d.dim + row) : make_double2(0.0, 0.0);
-      sY[c][r] = ok ? __ldg(Yb + (size_t)(q0 + c) * d.dim + row) : make_double2(0.0, 0.0);
+      sW[b][c][r] = row < d.dim ? __ldg(Wb + (size_t)(q0 + c) * d.dim + row) : make_double2(0.0, 0.0);
     }
-    // C tile: rows q0..q0+15, columns col0..col0+31
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int idx = threadIdx.x + 128 * e;
-      const int c = idx >> 4, r = idx & 15;
-      sC[r][c] = __ldg(C + (size_t)(col0 + c) * k + q0 + r);
+      const int c = idx & 31, r = idx >> 5;
+      sC[b][r][c] = __ldg(C + (size_t)(col0 + c) * k + q0 + r);
     }
-    __syncthreads();
+  };
+  load(0, 0);
+  __syncthreads();
+  for (int q0 = 0, b = 0; q0 < k; q0 += RK, b ^= 1) {
+    if (q0 + RK < k) load(q0 + RK, b ^ 1);
 #pragma unroll
     for (int q = 0; q < RK; ++q) {
-      double2 w[4], y[4], c[4];
+      double2 w[4], c[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        w[i] = sW[q][ty + 16 * i];
-        y[i] = sY[q][ty + 16 * i];
-      }
+      for (int i = 0; i < 4; ++i) w[i] = sW[b][q][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) c[j] = sC[q][tx + 8 * j];
+      for (int j = 0; j < 4; ++j) c[j] = sC[b][q][tx + 8 * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          cfma(av[i][j], w[i], c[j]);
-          cfma(ay[i][j], y[i], c[j]);
-        }
+        for (int j = 0; j < 4; ++j) cfma(av[i][j], w[i], c[j]);
     }
     __syncthreads();
   }
-  // epilogue
-  __shared__ double sres[16][RC + 1];
-  double rs[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int col = col0 + tx + 8 * j;
-    const double th = __ldg(theta + d.kv + col);
-    const double sc = __ldg(scol + d.kv + col);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int row = row0 + ty + 16 * i;
-      if (row < d.dim) {
-        const size_t o = (size_t)d.blk + (size_t)col * d.dim + row;
-        const double2 v = av[i][j];
-        const double2 r = make_double2(ay[i][j].x - th * v.x, ay[i][j].y - th * v.y);
-        Vp[o] = v;
-        Sp[o] = make_float2((float)(sc * r.x), (float)(sc * r.y));
-        rs[j] += r.x * r.x + r.y * r.y;
-      }
+      if (row < d.dim) Vp[(size_t)d.blk + (size_t)col * d.dim + row] = av[i][j];
     }
   }
+}
+
+// R = A V - V Theta in FP64 (A = -Delta), S = -2 c_hop R in FP32 for the next
+// filter, and per-CTA partial sums of |R_j|^2.  One thread per (site,
+// column); CTA = 128 sites of one column.
+__global__ void __launch_bounds__(128) k_residual64(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
+                                                    const int* __restrict__ start, int np,
+                                                    const double2* __restrict__ U64, const double2* __restrict__ Vp,
+                                                    const double* __restrict__ theta, float2* __restrict__ Sp,
+                                                    double* __restrict__ rpart) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int nst = (d.V3 + 127) >> 7;
+  const int t = blockIdx.x - start[p];
+  const int st = t % nst, j = t / nst;
+  const int s = st * 128 + threadIdx.x;
+  double rr = 0.0;
+  if (s < d.V3) {
+    const Lat g{d.L, d.L * d.L, d.V3};
+    const double2* U = U64 + d.u64;
+    const size_t col = (size_t)d.blk + (size_t)j * d.dim;
+    const double2* x = Vp + col;
+    int sx, sy, sz;
+    site_xyz(g, s, sx, sy, sz);
+    double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
 #pragma unroll
-  for (int j = 0; j < 4; ++j) sres[ty][tx + 8 * j] = rs[j];
-  __syncthreads();
-  if (threadIdx.x < RC) {
-    double s = 0.0;
-    for (int r = 0; r < 16; ++r) s += sres[r][threadIdx.x];
-    rpart[d.rp + (size_t)rt * k + col0 + threadIdx.x] = s;
+    for (int mu = 0; mu < 3; ++mu) {
+      const int u = nb_up(g, sx, sy, sz, mu), dn = nb_dn(g, sx, sy, sz, mu);
+      double2 xu[3], xd[3];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        xu[b] = __ldg(x + 3 * (size_t)u + b);
+        xd[b] = __ldg(x + 3 * (size_t)dn + b);
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          cfma(acc[a], __ldg(U + (size_t)(mu * 9 + 3 * a + b) * d.V3 + s), xu[b]);
+          cfmac(acc[a], __ldg(U + (size_t)(mu * 9 + 3 * b + a) * d.V3 + dn), xd[b]);
+        }
+    }
+    const double th = __ldg(theta + d.kv + j);
+    const double sc = -2.0 * ps[p].c_hop;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double2 xs = __ldg(x + 3 * (size_t)s + a);
+      const double2 r = make_double2((6.0 - th) * xs.x - acc[a].x, (6.0 - th) * xs.y - acc[a].y);
+      rr += r.x * r.x + r.y * r.y;
+      Sp[col + 3 * (size_t)s + a] = make_float2((float)(sc * r.x), (float)(sc * r.y));
+    }
   }
+  // block reduction (fixed order)
+  for (int o = 16; o > 0; o >>= 1) rr += __shfl_xor_sync(0xffffffffu, rr, o);
+  __shared__ double red[4];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rr;
+  __syncthreads();
+  if (threadIdx.x == 0) rpart[d.rp + (size_t)st * d.k + j] = red[0] + red[1] + red[2] + red[3];
 }
 
 // ------------------------------------------------------- residuals/conv ----
@@ -616,10 +655,21 @@ int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* 
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }
+int coef(const ProbDesc* pd, const ProbState* ps, int np, const double* theta, double* tcoef, double* scol, int m,
+         cudaStream_t st) {
+  k_coef<<<np, 256, 0, st>>>(pd, ps, np, theta, tcoef, scol, m);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
 int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* W,
-           const double2* Y, const double2* KK, const double* theta, const double* scol, double2* V, float2* S,
-           double* rpart, cudaStream_t st) {
-  k_rotate<<<nblk, 128, 0, st>>>(pd, ps, start, np, W, Y, KK, theta, scol, V, S, rpart);
+           const double2* KK, double2* V, cudaStream_t st) {
+  k_rotate<<<nblk, 128, 0, st>>>(pd, ps, start, np, W, KK, V);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+int residual64(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
+               const double2* V, const double* theta, float2* S, double* rpart, cudaStream_t st) {
+  k_residual64<<<nblk, 128, 0, st>>>(pd, ps, start, np, U64, V, theta, S, rpart);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

@@ -11,9 +11,13 @@ int gram_reduce(const ProbDesc* pd, const ProbState* ps, const int* start, int n
                 double2* KK, cudaStream_t st);
 int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* theta, double* tcoef, double* scol,
                 double* dwork, int first_iter, int fixed_cut, int max_sweeps, cudaStream_t st);
+// Chebyshev coefficient table and S scaling for a filter of degree m.
+int coef(const ProbDesc* pd, const ProbState* ps, int np, const double* theta, double* tcoef, double* scol, int m,
+         cudaStream_t st);
 int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* W,
-           const double2* Y, const double2* KK, const double* theta, const double* scol, double2* V, float2* S,
-           double* rpart, cudaStream_t st);
+           const double2* KK, double2* V, cudaStream_t st);
+int residual64(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
+               const double2* V, const double* theta, float2* S, double* rpart, cudaStream_t st);
 int resid_check(const ProbDesc* pd, ProbState* ps, int np, const double* rpart, double* resid, double tol,
                 int* n_active, cudaStream_t st);
 int phase_fix(const ProbDesc* pd, const int* start, int np, int nblk, double2* V, double* phases, double* norms,

@@ -22,6 +22,7 @@
 // This replaces, per timeslice, MatCreateShell + EPSSolve + EPSGetEigenpair +
 // fix_phase + recover_spectrum of the reference (src/ev_ts.cpp:197-319).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -44,8 +45,9 @@ struct laph_solver {
   ProbState* d_ps = nullptr;
   std::vector<ProbState> hps;
   // CTA -> problem prefix tables
-  int *st_site = nullptr, *st_filt = nullptr, *st_nl = nullptr, *st_gram = nullptr, *st_gred = nullptr,
+  int *st_tile = nullptr, *st_site = nullptr, *st_filt = nullptr, *st_nl = nullptr, *st_gram = nullptr, *st_gred = nullptr,
       *st_rot = nullptr, *st_rand = nullptr, *st_col = nullptr;
+  int nb_tile = 0, stage_f2 = 0, all_even = 1;
   int nb_site = 0, nb_filt = 0, nb_nl = 0, nb_gram = 0, nb_gred = 0, nb_rot = 0, nb_rand = 0, nb_col = 0;
   // pools
   double2 *U64raw = nullptr, *U64 = nullptr, *Utmp = nullptr, *dec = nullptr, *stage = nullptr;
@@ -61,6 +63,7 @@ struct laph_solver {
   int* h_nactive = nullptr;
   size_t blk_total = 0;
   std::vector<int> links_set;
+  std::vector<int> degs;  // filter degree of each pass of the last run
   double ms[4] = {0, 0, 0, 0};
   long long cnt[3] = {0, 0, 0};
   std::vector<cudaEvent_t> evf;
@@ -113,7 +116,7 @@ int laph_solver_destroy(laph_solver* s) {
   if (!s) return LAPH_OK;
   cudaSetDevice(s->dev);
   if (s->st) cudaStreamSynchronize(s->st);
-  void* ptrs[] = {s->d_pd, s->d_ps, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
+  void* ptrs[] = {s->d_pd, s->d_ps, s->st_tile, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
                   s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
                   s->phases, s->norms, s->d_nactive};
@@ -140,8 +143,10 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     set_error("laph_solver_create: no CUDA device");
     return LAPH_ENODEV;
   }
-  if (opts->deg < 2 || opts->deg > 64 || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1) {
-    set_error("laph_solver_create: need 2 <= deg <= 64, guard >= 0, tol > 0, max_it >= 1");
+  if (opts->deg < 2 || opts->deg > 64 || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1 ||
+      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 2) {
+    set_error("laph_solver_create: need 2 <= deg <= 64, guard >= 0, tol > 0, max_it >= 1, 0 <= block <= 512, "
+              "filter_kernel in {0, 1, 2}");
     return LAPH_EINVAL;
   }
   for (int i = 0; i < n; ++i) {
@@ -161,7 +166,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   s->o = *opts;
   s->np = n;
   s->mdeg = opts->deg;
-  s->kb = 32;
+  s->kb = opts->block > 0 ? opts->block : 32;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     set_error("laph_solver_create: cannot use device %d", device);
@@ -170,7 +175,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   // descriptors and pool offsets
   long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
   size_t max_run = 0, max_v3 = 0;
-  std::vector<int> per_site, per_filt, per_nl, per_gram, per_gred, per_rot, per_rand, per_col;
+  std::vector<int> per_tile, per_site, per_filt, per_nl, per_gram, per_gred, per_rot, per_rand, per_col;
   for (int i = 0; i < n; ++i) {
     ProbDesc d{};
     d.L = probs[i].L;
@@ -190,7 +195,12 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     d.tc = o_tc;
     const int chunk_rows = 8192;
     d.nchunk = (d.dim + chunk_rows - 1) / chunk_rows;
-    d.nrt = (d.dim + kRotRows - 1) / kRotRows;
+    d.nrt = (d.V3 + 127) / 128;  // site tiles of the residual kernel
+    d.zr = 1;
+    for (int r = 1; r <= d.L; ++r)
+      if (d.L % r == 0 && r * d.L <= 128) d.zr = r;
+    if (d.L % 2) s->all_even = 0;
+    s->stage_f2 = std::max(s->stage_f2, (5 * d.zr + 2) * 3 * d.L);
     const int T = d.k / kGramTile, npair = T * (T + 1) / 2;
     o_u64 += 27LL * d.V3;
     o_uf += 27LL * d.V3;
@@ -206,10 +216,11 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     const int nst = (d.V3 + 127) / 128;
     per_site.push_back(nst);
     per_filt.push_back(nst * ((d.k + s->kb - 1) / s->kb));
+    per_tile.push_back((d.L * d.L / d.zr) * ((d.k + s->kb - 1) / s->kb));
     per_nl.push_back(nst * d.k);
     per_gram.push_back(d.nchunk * 2 * npair);
     per_gred.push_back((2 * npair * kGramTile * kGramTile + 255) / 256);
-    per_rot.push_back(d.nrt * (d.k / 32));
+    per_rot.push_back(((d.dim + kRotRows - 1) / kRotRows) * (d.k / 32));
     per_rand.push_back((int)(((long long)d.dim * d.k + 255) / 256));
     per_col.push_back(d.nev);
   }
@@ -241,7 +252,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     cudaGetLastError();
     return fail(LAPH_ENOMEM);
   }
-  if ((rc = upload_prefix(per_site, &s->st_site, &s->nb_site)) || (rc = upload_prefix(per_filt, &s->st_filt, &s->nb_filt)) ||
+  if ((rc = upload_prefix(per_tile, &s->st_tile, &s->nb_tile)) || (rc = upload_prefix(per_site, &s->st_site, &s->nb_site)) || (rc = upload_prefix(per_filt, &s->st_filt, &s->nb_filt)) ||
       (rc = upload_prefix(per_nl, &s->st_nl, &s->nb_nl)) || (rc = upload_prefix(per_gram, &s->st_gram, &s->nb_gram)) ||
       (rc = upload_prefix(per_gred, &s->st_gred, &s->nb_gred)) || (rc = upload_prefix(per_rot, &s->st_rot, &s->nb_rot)) ||
       (rc = upload_prefix(per_rand, &s->st_rand, &s->nb_rand)) || (rc = upload_prefix(per_col, &s->st_col, &s->nb_col)))
@@ -297,15 +308,15 @@ static int iteration_rr(laph_solver* s, int first_iter) {
   LAPH_TRY(gram_reduce(s->d_pd, s->d_ps, s->st_gred, s->np, s->nb_gred, s->gpart, s->KK, s->st));
   LAPH_TRY(small_dense(s->d_pd, s->d_ps, s->np, s->KK, s->theta, s->tcoef, s->scol, s->dwork, first_iter, fixed ? 1 : 0,
                        30, s->st));
-  LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->Y, s->KK, s->theta, s->scol, s->V, s->S,
-                  s->rpart, s->st));
+  LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->KK, s->V, s->st));
+  LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
   LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
   LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
   return LAPH_OK;
 }
 
-static int filter(laph_solver* s) {
-  const int m = s->mdeg;
+static int filter(laph_solver* s, int m) {
+  LAPH_TRY(coef(s->d_pd, s->d_ps, s->np, s->theta, s->tcoef, s->scol, m, s->st));
   const int bf = s->o.link_prec == LAPH_LINKS_BF16;
   const void* links = bf ? s->Ubf : static_cast<const void*>(s->Uf32);
   for (int n = 1; n < m; ++n) {
@@ -313,8 +324,12 @@ static int filter(laph_solver* s) {
     const float2* X = (n == 1) ? s->S : s->E[(n - 2) % 3];
     const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
     float2* Yo = s->E[(n - 1) % 3];
-    LAPH_TRY(cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo,
-                       s->V, s->W, s->tcoef, n, fin, s->st));
+    if (s->all_even && s->o.filter_kernel == 2)
+      LAPH_TRY(cheb_step_tiled(s->d_pd, s->d_ps, s->st_tile, s->np, s->nb_tile, s->kb, s->stage_f2, bf, links, s->scale,
+                               X, Z, s->S, Yo, s->V, s->W, s->tcoef, n, fin, s->st));
+    else
+      LAPH_TRY(cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo,
+                         s->V, s->W, s->tcoef, n, fin, s->st));
   }
   return LAPH_OK;
 }
@@ -358,8 +373,9 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->W, o.seed, s->st));
   LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
   LAPH_TRY(iteration_rr(s, 1));
-  nlaunch += 2 + 6;  // pack, random block, first Rayleigh-Ritz
+  nlaunch += 2 + 7;  // pack, random block, first Rayleigh-Ritz
   s->cnt[0] = s->cnt[1] = s->cnt[2] = 0;
+  s->degs.clear();
   double filt_ms = 0.0;
   if (s->evf.empty()) {
     s->evf.resize(2);
@@ -372,14 +388,29 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     LAPH_CUDA_TRY(cudaMemcpyAsync(s->hps.data(), s->d_ps, s->np * sizeof(ProbState), cudaMemcpyDeviceToHost, s->st));
     LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
     if (*s->h_nactive == 0) break;
+    // Degree of this pass.  While the Ritz vectors are still poor (largest
+    // wanted residual > 1e-2) the amplification of the filter is capped at
+    // 1e6 relative to the damped interval -- taken at lambda = 0, the bottom
+    // of the spectrum of -Delta -- so the filtered block cannot collapse onto
+    // the lowest eigenvectors and break the Cholesky QR; afterwards the
+    // correction form keeps the block well conditioned at any degree.
+    int m = s->mdeg;
+    for (int i = 0; i < s->np; ++i) {
+      const ProbState& p = s->hps[i];
+      if (!p.active || !(p.max_resid > 1e-2)) continue;
+      const double tb0 = 1.0 + 2.0 * p.lam_cut / (p.lam_max - p.lam_cut);
+      const int m_safe = (int)std::floor(std::acosh(1e6) / std::acosh(std::max(tb0, 1.0 + 1e-12)));
+      m = std::min(m, std::max(2, m_safe));
+    }
     for (int i = 0; i < s->np; ++i)
-      if (s->hps[i].active) s->cnt[0] += (long long)s->hd[i].V3 * s->hd[i].k * (s->mdeg - 1);
-    s->cnt[1] += s->mdeg - 1;
+      if (s->hps[i].active) s->cnt[0] += (long long)s->hd[i].V3 * s->hd[i].k * (m - 1);
+    s->cnt[1] += m - 1;
+    s->degs.push_back(m);
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[0], s->st));
-    LAPH_TRY(filter(s));
+    LAPH_TRY(filter(s, m));
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[1], s->st));
     LAPH_TRY(iteration_rr(s, 0));
-    nlaunch += (s->mdeg - 1) + 6;
+    nlaunch += 1 + (m - 1) + 7;
     float f = 0.f;
     LAPH_CUDA_TRY(cudaEventSynchronize(s->evf[1]));
     LAPH_CUDA_TRY(cudaEventElapsedTime(&f, s->evf[0], s->evf[1]));
