@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     # 32^3 x 64, eps 0.3, stout 5 x 0.1, nev 120 (+16 guard), BF16 links
     "c3": dict(L=32, T=64, eps=0.3, seed=1229, smear="stout", p1=0.1, p2=0.0, iters=5, compat=1, nev=120,
-               guard=16, link_prec="bf16", tol=1e-9, deg=32),
+               guard=16, link_prec="bf16", tol=1e-9, deg=48),
     # 24^3 x 48, eps 0.3, HYP 0.62/0.62 x 1, nev 120
     "c2": dict(L=24, T=48, eps=0.3, seed=1228, smear="hyp", p1=0.62, p2=0.62, iters=1, compat=0, nev=120,
                guard=16, link_prec="fp32", tol=1e-9, deg=12),
@@ -143,7 +143,7 @@ def make_solver(cfg, device):
                      smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
                      link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
                      max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
-                     filter_kernel=cfg.get("filter_kernel", 0))
+                     filter_kernel=cfg.get("filter_kernel", 0), jacobi_sweeps=cfg.get("sweeps", 0))
 
 
 def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
@@ -247,6 +247,8 @@ def main():
     ap.add_argument("--timeslices", type=int, default=None)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--filter-kernel", type=int, default=0)
+    ap.add_argument("--guard", type=int, default=None)
+    ap.add_argument("--sweeps", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -261,6 +263,9 @@ def main():
     if args.timeslices:
         cfg["T"] = args.timeslices
     cfg["block"] = args.block
+    cfg["sweeps"] = args.sweeps
+    if args.guard is not None:
+        cfg["guard"] = args.guard
     cfg["filter_kernel"] = args.filter_kernel
     if args.impl == "reference":
         return run_reference(args, cfg)

@@ -160,6 +160,9 @@ typedef struct {
   int block;            /* columns per CTA of the filter kernel, 8..64 (0: 32)     */
   int filter_kernel;    /* 0 auto, 1 register-resident links + L2 bulk prefetch,
                            2 shared-memory staged rows (even L only)              */
+  int jacobi_sweeps;    /* cap on Jacobi sweeps per Rayleigh-Ritz (0: 2); an
+                           unfinished sweep set only delays convergence, since
+                           residuals are always computed from the new vectors   */
 } laph_solve_opts;
 void laph_solve_opts_default(laph_solve_opts* o);
 

@@ -40,7 +40,8 @@ class laph_solve_opts(ctypes.Structure):
     _fields_ = [("smear_kind", c_int), ("smear_p1", c_double), ("smear_p2", c_double), ("smear_iters", c_int),
                 ("smear_compat", c_int), ("guard", c_int), ("link_prec", c_int), ("tol", c_double),
                 ("max_it", c_int), ("window", c_int), ("lam_cut", c_double), ("lam_max", c_double),
-                ("deg", c_int), ("phase_fix", c_int), ("seed", c_u64), ("block", c_int), ("filter_kernel", c_int)]
+                ("deg", c_int), ("phase_fix", c_int), ("seed", c_u64), ("block", c_int), ("filter_kernel", c_int),
+                ("jacobi_sweeps", c_int)]
 
 
 class laph_result(ctypes.Structure):

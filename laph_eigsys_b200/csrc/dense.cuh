@@ -4,7 +4,7 @@
 
 namespace laph {
 constexpr int kGramTile = 32;   // block widths k are multiples of this
-constexpr int kRotRows = 64;    // rows per rotation tile
+constexpr int kRotRows = 128;   // rows per rotation tile
 int gram(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int chunk_rows,
          const double2* W, const double2* Y, double2* gpart, cudaStream_t st);
 int gram_reduce(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* gpart,

@@ -218,7 +218,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     per_filt.push_back(nst * ((d.k + s->kb - 1) / s->kb));
     per_tile.push_back((d.L * d.L / d.zr) * ((d.k + s->kb - 1) / s->kb));
     per_nl.push_back(nst * d.k);
-    per_gram.push_back(d.nchunk * 2 * npair);
+    per_gram.push_back(d.nchunk * npair);
     per_gred.push_back((2 * npair * kGramTile * kGramTile + 255) / 256);
     per_rot.push_back(((d.dim + kRotRows - 1) / kRotRows) * (d.k / 32));
     per_rand.push_back((int)(((long long)d.dim * d.k + 255) / 256));
@@ -307,7 +307,7 @@ static int iteration_rr(laph_solver* s, int first_iter) {
   LAPH_TRY(gram(s->d_pd, s->d_ps, s->st_gram, s->np, s->nb_gram, 8192, s->W, s->Y, s->gpart, s->st));
   LAPH_TRY(gram_reduce(s->d_pd, s->d_ps, s->st_gred, s->np, s->nb_gred, s->gpart, s->KK, s->st));
   LAPH_TRY(small_dense(s->d_pd, s->d_ps, s->np, s->KK, s->theta, s->tcoef, s->scol, s->dwork, first_iter, fixed ? 1 : 0,
-                       30, s->st));
+                       s->o.jacobi_sweeps > 0 ? s->o.jacobi_sweeps : 2, s->st));
   LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->KK, s->V, s->st));
   LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
   LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
