@@ -143,7 +143,8 @@ def make_solver(cfg, device):
                      smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
                      link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
                      max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
-                     filter_kernel=cfg.get("filter_kernel", 0), jacobi_sweeps=cfg.get("sweeps", 0))
+                     filter_kernel=cfg.get("filter_kernel", 0), jacobi_sweeps=cfg.get("sweeps", 0),
+                     lam_cut=cfg.get("lam_cut0", 0.0))
 
 
 def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
@@ -249,6 +250,7 @@ def main():
     ap.add_argument("--filter-kernel", type=int, default=0)
     ap.add_argument("--guard", type=int, default=None)
     ap.add_argument("--sweeps", type=int, default=0)
+    ap.add_argument("--lam-cut0", type=float, default=0.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -264,6 +266,7 @@ def main():
         cfg["T"] = args.timeslices
     cfg["block"] = args.block
     cfg["sweeps"] = args.sweeps
+    cfg["lam_cut0"] = args.lam_cut0
     if args.guard is not None:
         cfg["guard"] = args.guard
     cfg["filter_kernel"] = args.filter_kernel

@@ -127,6 +127,14 @@ int laph_plaquette(laph_ctx* ctx, double* plaq);
 int laph_eps_solve(laph_ctx* ctx, int nev, int ncv, double tol, int max_it, int device_basis, uint64_t seed,
                    double* theta_out, double* V_out, int* nconv, int* restarts, long long* nmatvec);
 
+/* The same Krylov-Schur on any Hermitian operator given as a host callback
+ * mult(user, x, y): y = Op x on host complex128 vectors of length dim (returns
+ * 0 on success) -- the EPSSolve that drives a registered MATOP_MULT.  Host
+ * memory only; needs no device.  Same outputs as laph_eps_solve. */
+int laph_eps_solve_cb(long long dim, int (*mult)(void* user, const double* x, double* y), void* user, int nev,
+                      int ncv, double tol, int max_it, uint64_t seed, double* theta_out, double* V_out, int* nconv,
+                      int* restarts, long long* nmatvec);
+
 /* ---- batched block eigensolver (the "chosen" form) ------------------------
  * Solves many timeslices (possibly of different L and nev) in one batched,
  * device-resident Chebyshev-filtered subspace iteration: FP32 filter matvecs

@@ -250,6 +250,24 @@ struct HostBasis : Basis {
   }
 };
 
+// Basis in host memory whose products call a user callback: what SLEPc's
+// EPSSolve does with any MatShell (MatMult -> the registered MATOP_MULT).
+struct CallbackBasis : HostBasis {
+  int (*mult)(void*, const double*, double*);
+  void* user;
+  CallbackBasis(long dim, int m, int (*f)(void*, const double*, double*), void* u)
+      : HostBasis(nullptr, dim, m, 0), mult(f), user(u) {}
+  int op(int j) override {
+    ++nmatvec;
+    const int rc = mult(user, reinterpret_cast<const double*>(col(j)), reinterpret_cast<double*>(w.data()));
+    if (rc != 0) {
+      set_error("laph_eps_solve_cb: operator callback returned %d", rc);
+      return LAPH_EINVAL;
+    }
+    return LAPH_OK;
+  }
+};
+
 #define LAPH_CUBLAS_TRY(expr)                                         \
   do {                                                                \
     cublasStatus_t _s = (expr);                                       \
@@ -355,38 +373,8 @@ struct DeviceBasis : Basis {
 
 }  // namespace
 
-extern "C" int laph_eps_solve(laph_ctx* ctx, int nev, int ncv, double tol, int max_it, int device_basis, uint64_t seed,
-                              double* theta_out, double* V_out, int* nconv_out, int* its_out, long long* nmatvec_out) {
-  const double2* U;
-  int L, deg, dev;
-  double lam_l, lam_c;
-  cudaStream_t st;
-  LAPH_TRY(ctx_device_links(ctx, &U, &L, &lam_l, &lam_c, &deg, &st, &dev));
-  const long dim = 3L * L * L * L;
-  if (nev < 1 || !theta_out || !(tol > 0.0) || max_it < 1 || deg < 1) {
-    set_error("laph_eps_solve: bad argument");
-    return LAPH_EINVAL;
-  }
-  if (ncv <= 0) ncv = std::max(2 * nev, nev + 15);
-  if (ncv > dim - 1) ncv = (int)dim - 1;
-  if (nev >= ncv) {
-    set_error("laph_eps_solve: nev %d too large for dim %ld", nev, dim);
-    return LAPH_EINVAL;
-  }
-  const int m = ncv;
-  Basis* B = nullptr;
-  if (device_basis) {
-    auto* db = new DeviceBasis(ctx, dim, m);
-    db->deg = deg;
-    if (!db->ok) {
-      delete db;
-      set_error("laph_eps_solve: device basis allocation failed");
-      return LAPH_ENOMEM;
-    }
-    B = db;
-  } else {
-    B = new HostBasis(ctx, dim, m, deg);
-  }
+static int krylov_schur(Basis* B, long dim, int nev, int m, double tol, int max_it, uint64_t seed, double* theta_out,
+                        double* V_out, int* nconv_out, int* its_out, long long* nmatvec_out) {
   int rc = LAPH_OK;
   {
     SplitMix rng(seed);
@@ -460,11 +448,67 @@ extern "C" int laph_eps_solve(laph_ctx* ctx, int nev, int ncv, double tol, int m
   if (nconv_out) *nconv_out = nconv;
   if (its_out) *its_out = std::min(it, max_it);
   if (nmatvec_out) *nmatvec_out = B->nmatvec;
-  delete B;
   if (rc != LAPH_OK) return rc;
   if (nconv < nev) {
     set_error("laph_eps_solve: %d of %d pairs converged after %d restarts", nconv, nev, max_it);
     return LAPH_ENOTCONV;
   }
   return LAPH_OK;
+}
+
+static int ncv_default(int nev, int ncv, long dim) {
+  if (ncv <= 0) ncv = std::max(2 * nev, nev + 15);
+  if (ncv > dim - 1) ncv = (int)dim - 1;
+  return ncv;
+}
+
+extern "C" int laph_eps_solve(laph_ctx* ctx, int nev, int ncv, double tol, int max_it, int device_basis, uint64_t seed,
+                              double* theta_out, double* V_out, int* nconv_out, int* its_out, long long* nmatvec_out) {
+  const double2* U;
+  int L, deg, dev;
+  double lam_l, lam_c;
+  cudaStream_t st;
+  LAPH_TRY(ctx_device_links(ctx, &U, &L, &lam_l, &lam_c, &deg, &st, &dev));
+  const long dim = 3L * L * L * L;
+  if (nev < 1 || !theta_out || !(tol > 0.0) || max_it < 1 || deg < 1) {
+    set_error("laph_eps_solve: bad argument");
+    return LAPH_EINVAL;
+  }
+  const int m = ncv_default(nev, ncv, dim);
+  if (nev >= m) {
+    set_error("laph_eps_solve: nev %d too large for dim %ld", nev, dim);
+    return LAPH_EINVAL;
+  }
+  Basis* B = nullptr;
+  if (device_basis) {
+    auto* db = new DeviceBasis(ctx, dim, m);
+    db->deg = deg;
+    if (!db->ok) {
+      delete db;
+      set_error("laph_eps_solve: device basis allocation failed");
+      return LAPH_ENOMEM;
+    }
+    B = db;
+  } else {
+    B = new HostBasis(ctx, dim, m, deg);
+  }
+  const int rc = krylov_schur(B, dim, nev, m, tol, max_it, seed, theta_out, V_out, nconv_out, its_out, nmatvec_out);
+  delete B;
+  return rc;
+}
+
+extern "C" int laph_eps_solve_cb(long long dim, int (*mult)(void* user, const double* x, double* y), void* user, int nev,
+                                 int ncv, double tol, int max_it, uint64_t seed, double* theta_out, double* V_out,
+                                 int* nconv_out, int* its_out, long long* nmatvec_out) {
+  if (dim < 2 || !mult || nev < 1 || !theta_out || !(tol > 0.0) || max_it < 1) {
+    set_error("laph_eps_solve_cb: bad argument");
+    return LAPH_EINVAL;
+  }
+  const int m = ncv_default(nev, ncv, (long)dim);
+  if (nev >= m) {
+    set_error("laph_eps_solve_cb: nev %d too large for dim %lld", nev, dim);
+    return LAPH_EINVAL;
+  }
+  CallbackBasis B((long)dim, m, mult, user);
+  return krylov_schur(&B, (long)dim, nev, m, tol, max_it, seed, theta_out, V_out, nconv_out, its_out, nmatvec_out);
 }

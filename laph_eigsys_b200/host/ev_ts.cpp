@@ -1,0 +1,205 @@
+// ev_ts.cpp -- laph_ev_ts, the command-line replacement for LapH_EigSys's
+// ev_ts (src/ev_ts.cpp): same flags (--conf N, --phase_reset), same
+// parameters.txt in the working directory, same input (<config_path>/conf.%04d
+// LIME/ILDG) and outputs (<result_path>/eigenvectors|eigenvalues|phases.%04d.%03d).
+//
+//   solver = plain (parameters.txt): the reference's loop body -- link map,
+//            smearing, MatShell with the GPU MatMult, EPS Krylov-Schur on
+//            T_DEG(B), fix_phase, recover_spectrum -- one timeslice at a time.
+//   solver = block (default): all timeslices of this process in one batched
+//            device solve (laph_solver), same outputs.
+// Timeslices are split across processes as the reference splits them across
+// MPI ranks (src/ev_ts.cpp:103-119): with LAPH_RANK / LAPH_WORLD_SIZE (or
+// RANK / WORLD_SIZE) set, rank r gets a contiguous block, the first LT % size
+// ranks one extra.  One JSON line per timeslice goes to stdout.
+#include <sys/stat.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/laph_gpu.h"
+#include "../../include/laph_matshell.h"
+
+namespace {
+
+void usage() {
+  std::fprintf(stderr,
+               "usage: laph_ev_ts --conf N [--phase_reset 0|1] [--parameters FILE]\n"
+               "  reads parameters.txt (keys of LapH_EigSys plus smear, rho, alpha, tol, guard, solver)\n");
+}
+
+int env_int(const char* a, const char* b, int def) {
+  const char* v = std::getenv(a);
+  if (!v) v = std::getenv(b);
+  return v ? std::atoi(v) : def;
+}
+
+// Contiguous timeslice blocks, first LT % size blocks one longer (src/ev_ts.cpp:103-119).
+void split(int LT, int size, int rank, int* t0, int* n) {
+  const int base = LT / size, extra = LT % size;
+  *n = base + (rank < extra ? 1 : 0);
+  *t0 = rank * base + (rank < extra ? rank : extra);
+}
+
+int die(int st, const char* what) {
+  std::fprintf(stderr, "laph_ev_ts: %s: %s (%s)\n", what, laph_strerror(st), laph_last_error());
+  return 1;
+}
+
+double trace_vdv(int dim, int nev, const double* V) {
+  double tr = 0.0, sum = 0.0;
+  laph_check_trace(dim, nev, V, &tr, &sum);
+  return tr;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  int config = -1, phase_reset = 0;
+  std::string params = "parameters.txt";
+  for (int i = 1; i < argc; ++i) {
+    const std::string a = argv[i];
+    if ((a == "--conf") && i + 1 < argc) config = std::atoi(argv[++i]);
+    else if (a.rfind("--conf=", 0) == 0) config = std::atoi(a.c_str() + 7);
+    else if (a == "--phase_reset" && i + 1 < argc) phase_reset = std::atoi(argv[++i]);
+    else if (a == "--parameters" && i + 1 < argc) params = argv[++i];
+    else if (a == "--help") {
+      usage();
+      return 1;
+    } else {
+      usage();
+      return 2;
+    }
+  }
+  if (config < 0) {
+    std::printf("No configuration number specified!\n");
+    usage();
+    return 2;
+  }
+  laph_config P;
+  int st = laph_parse_parameters(params.c_str(), &P);
+  if (st != LAPH_OK) return die(st, "parameters");
+  const int L = P.LX, LT = P.LT, nev = P.NEV;
+  const int V3 = L * L * L, dim = 3 * V3;
+  const int size = env_int("LAPH_WORLD_SIZE", "WORLD_SIZE", 1), rank = env_int("LAPH_RANK", "RANK", 0);
+  int t0, ntodo;
+  split(LT, size, rank, &t0, &ntodo);
+  const int device = env_int("LAPH_DEVICE", "LOCAL_RANK", 0);
+  char conf_name[1100];
+  std::snprintf(conf_name, sizeof conf_name, "%s/conf.%04d", P.config_path, config);
+  std::vector<double> conf((size_t)std::max(ntodo, 1) * V3 * 72);
+  if (ntodo > 0) {
+    st = laph_lime_read_gauge(conf_name, LT, L, t0, t0 + ntodo - 1, conf.data());
+    if (st != LAPH_OK) return die(st, "read gauge");
+  }
+  const double p1 = P.smear == LAPH_SMEAR_HYP ? P.alpha_1 : (P.smear == LAPH_SMEAR_STOUT ? P.rho : P.alpha);
+  const double p2 = P.smear == LAPH_SMEAR_HYP ? P.alpha_2 : 0.0;
+  std::vector<double> evals(nev), phases(nev), evec((size_t)dim * nev * 2), vfix((size_t)dim * nev * 2);
+  if (phase_reset) std::printf("Resetting old phases is overridden by fix_phase, as in the reference\n");
+
+  if (P.solver == 1) {  // ---- plain: the reference's loop body with the GPU MatShell
+    laph_params lp{L, P.LAM_L, P.LAM_C, P.DEG, device};
+    laph_ctx* ctx = nullptr;
+    st = laph_ctx_create(&ctx, &lp);
+    if (st != LAPH_OK) return die(st, "context");
+    for (int ts = 0; ts < ntodo; ++ts) {
+      PetscLogDouble v1, v2;
+      PetscTime(&v1);
+      st = laph_set_links(ctx, conf.data() + (size_t)ts * V3 * 72, LAPH_LAYOUT_CONF);
+      if (st == LAPH_OK) st = laph_smear(ctx, P.smear, p1, p2, P.iter, 1);
+      if (st != LAPH_OK) return die(st, "links");
+      laph_shell shell{ctx, P.DEG};
+      Mat A;
+      EPS eps;
+      Vec xr, xi;
+      PetscErrorCode ierr = MatCreateShell(PETSC_COMM_SELF, PETSC_DECIDE, PETSC_DECIDE, dim, dim, &shell, &A);
+      ierr |= MatShellSetOperation(A, MATOP_MULT, (void (*)(void))MatMult_Laplacian2D_GPU);
+      ierr |= MatShellSetOperation(A, MATOP_MULT_TRANSPOSE, (void (*)(void))MatMult_Laplacian2D_GPU);
+      ierr |= MatShellSetOperation(A, MATOP_GET_DIAGONAL, (void (*)(void))MatGetDiagonal_Laplacian2D_GPU);
+      ierr |= MatSetOption(A, MAT_HERMITIAN, PETSC_TRUE);
+      ierr |= MatCreateVecs(A, nullptr, &xr);
+      ierr |= MatCreateVecs(A, nullptr, &xi);
+      ierr |= EPSCreate(PETSC_COMM_SELF, &eps);
+      ierr |= EPSSetOperators(eps, A, nullptr);
+      ierr |= EPSSetProblemType(eps, EPS_HEP);
+      ierr |= EPSSetDimensions(eps, nev, PETSC_DECIDE, PETSC_DECIDE);
+      ierr |= EPSSetWhichEigenpairs(eps, EPS_LARGEST_MAGNITUDE);
+      ierr |= EPSSetTolerances(eps, P.tol > 0 ? P.tol : 1e-8, PETSC_DEFAULT);
+      ierr |= EPSSetFromOptions(eps);
+      ierr |= EPSSolve(eps);
+      if (ierr) return die(LAPH_EINVAL, "EPS");
+      PetscInt nconv;
+      EPSGetConverged(eps, &nconv);
+      std::vector<double> theta(nev);
+      for (PetscInt i = 0; i < nev; ++i) {
+        PetscScalar eigr, eigi;
+        EPSGetEigenpair(eps, i, &eigr, &eigi, xr, xi);
+        PetscScalar* p;
+        VecGetArray(xr, &p);
+        std::memcpy(evec.data() + (size_t)i * dim * 2, p, sizeof(double) * 2 * dim);
+        VecRestoreArray(xr, &p);
+        theta[i] = PetscRealPart(eigr);
+      }
+      laph_fix_phase_host(dim, nev, evec.data(), vfix.data(), phases.data());
+      st = laph_write_eigsys_bin(P.result_path, "eigenvectors", config, t0 + ts, dim, nev, vfix.data());
+      if (st != LAPH_OK) return die(st, "write eigenvectors");
+      laph_recover_spectrum(nev, theta.data(), P.DEG, P.LAM_L, P.LAM_C, evals.data());
+      laph_write_eigenvalues_bin(P.result_path, "eigenvalues", config, t0 + ts, nev, evals.data());
+      laph_write_eigenvalues_bin(P.result_path, "phases", config, t0 + ts, nev, phases.data());
+      PetscTime(&v2);
+      std::printf("{\"t\": %d, \"solver\": \"plain\", \"nconv\": %d, \"seconds\": %.4f, \"trace_vdv\": %.12f, "
+                  "\"eval0\": %.12f}\n",
+                  t0 + ts, nconv, v2 - v1, trace_vdv(dim, nev, vfix.data()), evals[0]);
+      EPSDestroy(&eps);
+      MatDestroy(&A);
+      VecDestroy(&xr);
+      VecDestroy(&xi);
+    }
+    laph_ctx_destroy(ctx);
+    return 0;
+  }
+
+  // ---- block: every timeslice of this process in one batched solve
+  if (ntodo == 0) return 0;
+  std::vector<laph_problem> probs(ntodo, laph_problem{L, nev});
+  laph_solve_opts o;
+  laph_solve_opts_default(&o);
+  o.smear_kind = P.smear;
+  o.smear_p1 = p1;
+  o.smear_p2 = p2;
+  o.smear_iters = P.iter;
+  o.smear_compat = 1;
+  o.guard = P.guard;
+  o.tol = P.tol > 0 ? P.tol : 1e-9;
+  o.window = P.window;
+  laph_solver* s = nullptr;
+  st = laph_solver_create(&s, probs.data(), ntodo, &o, device);
+  if (st != LAPH_OK) return die(st, "solver");
+  for (int ts = 0; ts < ntodo; ++ts) {
+    st = laph_solver_set_links(s, ts, conf.data() + (size_t)ts * V3 * 72, LAPH_LAYOUT_CONF, 0);
+    if (st != LAPH_OK) return die(st, "links");
+  }
+  std::vector<laph_result> res(ntodo);
+  st = laph_solver_run(s, res.data());
+  if (st != LAPH_OK && st != LAPH_ENOTCONV) return die(st, "solve");
+  double ms[4];
+  laph_solver_timings(s, ms);
+  for (int ts = 0; ts < ntodo; ++ts) {
+    st = laph_solver_get(s, ts, evals.data(), vfix.data(), phases.data(), 0);
+    if (st != LAPH_OK) return die(st, "fetch");
+    st = laph_write_eigsys_bin(P.result_path, "eigenvectors", config, t0 + ts, dim, nev, vfix.data());
+    if (st != LAPH_OK) return die(st, "write eigenvectors");
+    laph_write_eigenvalues_bin(P.result_path, "eigenvalues", config, t0 + ts, nev, evals.data());
+    laph_write_eigenvalues_bin(P.result_path, "phases", config, t0 + ts, nev, phases.data());
+    std::printf("{\"t\": %d, \"solver\": \"block\", \"status\": %d, \"iters\": %d, \"max_resid\": %.3e, "
+                "\"trace_vdv\": %.12f, \"eval0\": %.12f, \"batch_ms\": %.2f}\n",
+                t0 + ts, res[ts].status, res[ts].iters, res[ts].max_resid, res[ts].trace_vdv, evals[0], ms[3]);
+  }
+  laph_solver_destroy(s);
+  return 0;
+}

@@ -1,0 +1,47 @@
+"""laph_ev_ts end to end (the ev_ts replacement): LIME input, parameters.txt,
+the reference's output files, for both the plain MatShell + EPS loop and the
+batched solver; eigenvalues against the oracle pipeline (HYP smearing + dense
+eigendecomposition of -Delta)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import laph_eigsys_b200 as lb
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "laph_eigsys_b200", "laph_ev_ts")
+
+
+@pytest.mark.parametrize("solver", ["block", "plain"])
+def test_ev_ts_cli(gpu, orc, tmp_path, solver):
+    L, T, nev, cfgno = 6, 3, 10, 1227
+    conf = lb.gauge_random(L, T, 0.4, 1227)
+    gdir = tmp_path / "gauges"
+    gdir.mkdir()
+    lb.lime_write_gauge(gdir / f"conf.{cfgno:04d}", conf, L, T)
+    out = tmp_path / "out"
+    out.mkdir()
+    # LAM_C above lambda_nev of every timeslice
+    refs = []
+    for t in range(T):
+        Us = orc.smear_hyp(lb.spatial_links(conf[t]), L, 0.62, 0.52, 2)
+        refs.append(np.linalg.eigvalsh(orc.neglap_dense(Us, L)))
+    lam_c = max(0.5 * (r[nev + 2] + r[nev + 3]) for r in refs)
+    (tmp_path / "parameters.txt").write_text(
+        f"config_path = {gdir}\nresult_path = {out}\nLT = {T}\nLX = {L}\nNEV = {nev}\n"
+        f"alpha_1 = 0.62\nalpha_2 = 0.52\niter = 2\nLAM_L = 12.0\nLAM_C = {lam_c}\nDEG = 8\nOMP_THRDS = 2\n"
+        f"tol = 1e-11\nsolver = {solver}\n")
+    r = subprocess.run([EXE, "--conf", str(cfgno)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert len([ln for ln in r.stdout.splitlines() if ln.startswith("{")]) == T
+    for t in range(T):
+        ev = lb.read_eigenvalues_bin(out, "eigenvalues", cfgno, t, nev)
+        V = lb.read_eigsys_bin(out, "eigenvectors", cfgno, t, 3 * L ** 3, nev)  # runs check_trace
+        ph = lb.read_eigenvalues_bin(out, "phases", cfgno, t, nev)
+        tol = 1e-9 if solver == "block" else 1e-6  # recover_spectrum loses digits near theta ~ 1
+        assert np.abs(np.sort(-ev) - refs[t][:nev]).max() < tol
+        assert np.abs(V[0].imag).max() < 1e-12
+        assert ph.shape == (nev,)
