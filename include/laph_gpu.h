@@ -204,6 +204,29 @@ int laph_solver_timings(laph_solver* s, double* ms4);
  * number of filter kernel launches, total device kernel launches. */
 int laph_solver_counters(laph_solver* s, long long* c3);
 
+/* ---- learned Chebyshev window --------------------------------------------
+ * A 16 -> 64 -> 64 -> 3 tanh MLP (FP32) maps per-timeslice features -- the
+ * smeared plaquette's mean, variance, skewness, excess kurtosis, the 10 Ritz
+ * values of a 10-step Lanczos on -Delta (/12), log V3 / log 48^3, k / dim --
+ * to (log lambda_cut, lambda_max, degree) of the first filter pass.  No
+ * counterpart in the reference, whose window (LAM_L, LAM_C, DEG) is set by
+ * hand in parameters.txt.  Parameter layout: W1[64][16] b1[64] W2[64][64]
+ * b2[64] W3[3][64] b3[3]; a model is the parameters followed by feature
+ * mean[16], std[16], target mean[3], std[3]. */
+int laph_mlp_nparams(void);
+int laph_mlp_forward(const float* params, const float* X, int n, float* out, int device);
+/* Gradient (and loss) of the mean-squared loss over n samples at params. */
+int laph_mlp_grad(const float* params, const float* X, const float* Y, int n, float* grad, float* loss, int device);
+/* `epochs` full-batch Adam steps (beta 0.9 / 0.999), params updated in place. */
+int laph_mlp_train(float* params, const float* X, const float* Y, int n, int epochs, float lr, float* loss,
+                   int device);
+/* Model used by window = LAPH_WINDOW_MLP (nfloats = nparams + 38). */
+int laph_solver_set_window_model(laph_solver* s, const float* model, int nfloats);
+/* Features (np x 16) and 10-step Lanczos upper bounds (np) of the last run. */
+int laph_solver_features(laph_solver* s, float* feats, double* bound);
+/* All k Ritz values of problem i after the last run (k returned). */
+int laph_solver_ritz(laph_solver* s, int i, double* theta, int* k);
+
 /* ---- host-side utilities (no device needed) ------------------------------ */
 /* Seeded synthetic gauge field U = exp(i eps H), H = sum_a c_a lambda_a with
  * c_a ~ N(0,1) i.i.d. (Gell-Mann basis), for all 4 directions; output in the

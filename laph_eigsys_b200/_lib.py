@@ -88,6 +88,13 @@ _sig("laph_solver_set_links", c_int, c_void_p, c_int, c_void_p, c_int, c_int)
 _sig("laph_solver_run", c_int, c_void_p, P(laph_result))
 _sig("laph_solver_get", c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int)
 _sig("laph_solver_stream", c_int, c_void_p, P(c_void_p))
+_sig("laph_solver_set_window_model", c_int, c_void_p, c_void_p, c_int)
+_sig("laph_solver_features", c_int, c_void_p, c_void_p, c_void_p)
+_sig("laph_solver_ritz", c_int, c_void_p, c_int, c_void_p, P(c_int))
+_sig("laph_mlp_nparams", c_int)
+_sig("laph_mlp_forward", c_int, c_void_p, c_void_p, c_int, c_void_p, c_int)
+_sig("laph_mlp_grad", c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int)
+_sig("laph_mlp_train", c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, ctypes.c_float, c_void_p, c_int)
 _sig("laph_solver_timings", c_int, c_void_p, P(c_double))
 _sig("laph_solver_counters", c_int, c_void_p, P(c_ll))
 _sig("laph_gauge_random", c_int, c_void_p, c_int, c_int, c_double, c_u64)

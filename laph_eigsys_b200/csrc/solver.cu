@@ -31,6 +31,7 @@
 #include "dense.cuh"
 #include "filter.cuh"
 #include "links.cuh"
+#include "mlp.cuh"
 #include "smear.cuh"
 
 using namespace laph;
@@ -69,6 +70,13 @@ struct laph_solver {
   std::vector<cudaEvent_t> evf;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   int ran = 0;
+  // learned window / features
+  float* model = nullptr;   // device: params + normalisation
+  int have_model = 0;
+  float *feats = nullptr, *mwork = nullptr;
+  double *bound = nullptr, *plaq = nullptr;
+  int* wdeg = nullptr;
+  int deg0 = 0;             // degree cap of the first filter pass from the model
 };
 
 namespace {
@@ -119,7 +127,7 @@ int laph_solver_destroy(laph_solver* s) {
   void* ptrs[] = {s->d_pd, s->d_ps, s->st_tile, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
                   s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
-                  s->phases, s->norms, s->d_nactive};
+                  s->phases, s->norms, s->d_nactive, s->model, s->feats, s->mwork, s->bound, s->plaq, s->wdeg};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->h_nactive) cudaFreeHost(s->h_nactive);
@@ -241,7 +249,9 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
       (rc = dalloc(&s->gpart, o_gp)) || (rc = dalloc(&s->rpart, o_rp)) || (rc = dalloc(&s->theta, o_kv)) ||
       (rc = dalloc(&s->tcoef, o_tc)) || (rc = dalloc(&s->scol, o_kv)) || (rc = dalloc(&s->dwork, 4 * o_kv)) ||
       (rc = dalloc(&s->resid, o_kv)) || (rc = dalloc(&s->phases, o_kv)) || (rc = dalloc(&s->norms, o_kv)) ||
-      (rc = dalloc(&s->d_nactive, 1)))
+      (rc = dalloc(&s->d_nactive, 1)) || (rc = dalloc(&s->model, kMlpParams + kMlpNorm)) ||
+      (rc = dalloc(&s->feats, (size_t)n * kMlpIn)) || (rc = dalloc(&s->mwork, (size_t)n * (kMlpIn + kMlpOut))) ||
+      (rc = dalloc(&s->bound, n)) || (rc = dalloc(&s->plaq, 4 * (size_t)n)) || (rc = dalloc(&s->wdeg, n)))
     return fail(rc);
   if (opts->link_prec == LAPH_LINKS_BF16) {
     if ((rc = dalloc(reinterpret_cast<float2**>(&s->Ubf), (size_t)o_uf))) return fail(rc);  // 4 B per element
@@ -370,6 +380,31 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     p.active = 1;
   }
   LAPH_CUDA_TRY(cudaMemcpyAsync(s->d_ps, s->hps.data(), s->np * sizeof(ProbState), cudaMemcpyHostToDevice, s->st));
+  // per-timeslice features (plaquette moments + 10-step Lanczos); the learned
+  // window sets the first pass's lam_cut and degree from them
+  s->deg0 = 0;
+  if (o.window != LAPH_WINDOW_FIXED) {
+    for (int i = 0; i < s->np;) {
+      int j = i;
+      while (j < s->np && s->hd[j].L == s->hd[i].L) ++j;
+      LAPH_TRY(plaquette_moments_batch(s->U64 + s->hd[i].u64, s->hd[i].L, j - i, s->plaq + 4 * (size_t)i, s->st));
+      i = j;
+    }
+    LAPH_TRY(features(s->d_pd, s->np, s->U64, s->plaq, s->W, s->feats, s->bound, s->st));
+    nlaunch += 2;
+    if (o.window == LAPH_WINDOW_MLP) {
+      if (!s->have_model) {
+        set_error("laph_solver_run: window = MLP but no model set (laph_solver_set_window_model)");
+        return LAPH_EINVAL;
+      }
+      LAPH_TRY(window_infer(s->d_pd, s->d_ps, s->np, s->feats, s->model, s->mwork, s->bound, s->wdeg, s->st));
+      std::vector<int> dg(s->np);
+      LAPH_CUDA_TRY(cudaMemcpyAsync(dg.data(), s->wdeg, s->np * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+      LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+      for (int d : dg) s->deg0 = std::max(s->deg0, d);
+      nlaunch += 3;
+    }
+  }
   LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->W, o.seed, s->st));
   LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
   LAPH_TRY(iteration_rr(s, 1));
@@ -395,6 +430,7 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     // the lowest eigenvectors and break the Cholesky QR; afterwards the
     // correction form keeps the block well conditioned at any degree.
     int m = s->mdeg;
+    if (it == 1 && s->deg0 > 0) m = std::min(m, std::max(2, s->deg0));
     for (int i = 0; i < s->np; ++i) {
       const ProbState& p = s->hps[i];
       if (!p.active || !(p.max_resid > 1e-2)) continue;
@@ -473,6 +509,44 @@ int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double*
     LAPH_CUDA_TRY(cudaMemcpyAsync(evecs, s->V + d.blk, (size_t)d.dim * d.nev * sizeof(double2), kd, s->st));
   if (phases) LAPH_CUDA_TRY(cudaMemcpyAsync(phases, s->phases + d.kv, d.nev * sizeof(double), kd, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return LAPH_OK;
+}
+
+int laph_solver_set_window_model(laph_solver* s, const float* model, int nfloats) {
+  if (!s || !model || nfloats != kMlpParams + kMlpNorm) {
+    set_error("laph_solver_set_window_model: need %d floats (parameters + normalisation)", kMlpParams + kMlpNorm);
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->model, model, sizeof(float) * nfloats, cudaMemcpyHostToDevice, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  s->have_model = 1;
+  return LAPH_OK;
+}
+
+int laph_solver_features(laph_solver* s, float* feats, double* bound) {
+  if (!s || !s->ran) {
+    set_error("laph_solver_features: solver not run");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  if (feats)
+    LAPH_CUDA_TRY(cudaMemcpyAsync(feats, s->feats, sizeof(float) * kMlpIn * s->np, cudaMemcpyDeviceToHost, s->st));
+  if (bound) LAPH_CUDA_TRY(cudaMemcpyAsync(bound, s->bound, sizeof(double) * s->np, cudaMemcpyDeviceToHost, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return LAPH_OK;
+}
+
+int laph_solver_ritz(laph_solver* s, int i, double* theta, int* k) {
+  if (!s || !s->ran || i < 0 || i >= s->np || !theta) {
+    set_error("laph_solver_ritz: bad argument or solver not run");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  const ProbDesc& d = s->hd[i];
+  LAPH_CUDA_TRY(cudaMemcpyAsync(theta, s->theta + d.kv, sizeof(double) * d.k, cudaMemcpyDeviceToHost, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  if (k) *k = d.k;
   return LAPH_OK;
 }
 

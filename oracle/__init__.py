@@ -50,6 +50,7 @@ _sig("orc_eps_solve", _i, _vp, _i, _d, _d, _i, _i, _i, _d, _i, ctypes.c_uint64, 
 _sig("orc_recover_spectrum", None, _i, _vp, _i, _d, _d, _vp)
 _sig("orc_fix_phase", None, _i, _i, _vp, _vp, _vp)
 _sig("orc_build_neglap_dense", None, _vp, _i, _vp)
+_sig("orc_mlp_loss_grad", _d, _vp, _vp, _vp, _i, _vp)
 
 
 def _p(a):
@@ -179,3 +180,13 @@ def free_spectrum(L):
     k = 4.0 * np.sin(np.pi * np.arange(L) / L) ** 2
     ev = (k[:, None, None] + k[None, :, None] + k[None, None, :]).ravel()
     return np.sort(np.repeat(ev, 3))
+
+
+def mlp_loss_grad(params, X, Y):
+    """FP64 loss and gradient of the window MLP (16->64->64->3, tanh)."""
+    P = np.ascontiguousarray(params, dtype=np.float64)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    g = np.zeros_like(P)
+    loss = _lib.orc_mlp_loss_grad(_p(P), _p(X), _p(Y), X.shape[0], _p(g))
+    return loss, g

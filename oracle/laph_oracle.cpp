@@ -697,4 +697,59 @@ void orc_build_neglap_dense(const double* U, int L, double* Aout) {
   }
 }
 
+/* Loss and gradient of the window MLP (16 -> 64 -> 64 -> 3, tanh) in FP64:
+ * L = mean_{i,k} (O_ik - Y_ik)^2, parameters W1[64][16] b1 W2[64][64] b2
+ * W3[3][64] b3.  The CPU check for the device training kernels (this part
+ * has no counterpart in the reference). */
+double orc_mlp_loss_grad(const double* P, const double* X, const double* Y, int n, double* grad) {
+  const int I = 16, H = 64, O = 3;
+  const int oW1 = 0, ob1 = H * I, oW2 = ob1 + H, ob2 = oW2 + H * H, oW3 = ob2 + H, ob3 = oW3 + O * H, np_ = ob3 + O;
+  std::fill(grad, grad + np_, 0.0);
+  double loss = 0.0;
+  std::vector<double> h1(H), h2(H), d1(H), d2(H);
+  const double sc = 2.0 / (n * O);
+  for (int i = 0; i < n; ++i) {
+    const double* x = X + (size_t)i * I;
+    for (int j = 0; j < H; ++j) {
+      double z = P[ob1 + j];
+      for (int q = 0; q < I; ++q) z += P[oW1 + j * I + q] * x[q];
+      h1[j] = std::tanh(z);
+    }
+    for (int j = 0; j < H; ++j) {
+      double z = P[ob2 + j];
+      for (int q = 0; q < H; ++q) z += P[oW2 + j * H + q] * h1[q];
+      h2[j] = std::tanh(z);
+    }
+    double dout[3];
+    for (int k = 0; k < O; ++k) {
+      double o = P[ob3 + k];
+      for (int q = 0; q < H; ++q) o += P[oW3 + k * H + q] * h2[q];
+      const double d = o - Y[(size_t)i * O + k];
+      loss += d * d;
+      dout[k] = sc * d;
+    }
+    for (int j = 0; j < H; ++j) {
+      double dh = 0.0;
+      for (int k = 0; k < O; ++k) {
+        grad[oW3 + k * H + j] += dout[k] * h2[j];
+        dh += P[oW3 + k * H + j] * dout[k];
+      }
+      d2[j] = dh * (1.0 - h2[j] * h2[j]);
+    }
+    for (int k = 0; k < O; ++k) grad[ob3 + k] += dout[k];
+    for (int j = 0; j < H; ++j) {
+      for (int q = 0; q < H; ++q) grad[oW2 + j * H + q] += d2[j] * h1[q];
+      grad[ob2 + j] += d2[j];
+      double dh = 0.0;
+      for (int r = 0; r < H; ++r) dh += P[oW2 + r * H + j] * d2[r];
+      d1[j] = dh * (1.0 - h1[j] * h1[j]);
+    }
+    for (int j = 0; j < H; ++j) {
+      for (int q = 0; q < I; ++q) grad[oW1 + j * I + q] += d1[j] * x[q];
+      grad[ob1 + j] += d1[j];
+    }
+  }
+  return loss / (n * O);
+}
+
 }  // extern "C"

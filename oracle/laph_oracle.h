@@ -86,6 +86,9 @@ void orc_fix_phase(int dim, int nev, const double* V, double* Vfix, double* phas
  * modules/config_utils.cpp:18-58), complex128 row-major [dim][dim]. */
 void orc_build_neglap_dense(const double* links3, int L, double* A);
 
+/* Window MLP (16->64->64->3, tanh) mean-squared loss and gradient, FP64. */
+double orc_mlp_loss_grad(const double* params, const double* X, const double* Y, int n, double* grad);
+
 #ifdef __cplusplus
 }
 #endif
