@@ -144,7 +144,9 @@ def make_solver(cfg, device):
                      link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
                      max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
                      filter_kernel=cfg.get("filter_kernel", 0), jacobi_sweeps=cfg.get("sweeps", 0),
-                     lam_cut=cfg.get("lam_cut0", 0.0))
+                     lam_cut=cfg.get("lam_cut0", 0.0),
+                     window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
+                         cfg.get("window", "mlp")])
 
 
 def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
@@ -232,6 +234,7 @@ def workload_config(cfg):
     return {"workload": f"{cfg['L']}^3x{cfg['T']} eps {cfg['eps']} {cfg['smear']} {cfg['iters']}x{cfg['p1']}, "
                         f"nev {cfg['nev']} (+{cfg['guard']} guard), resid<=1e-9",
             "L": cfg["L"], "timeslices": cfg["T"], "nev": cfg["nev"], "guard": cfg["guard"], "deg": cfg["deg"],
+            "window": cfg.get("window", "mlp"),
             "links": cfg["link_prec"], "filter": "fp32", "rayleigh_ritz": "fp64",
             "l2": "inputs larger than L2 (each 64-timeslice block of vectors is 8 GB)"}
 
@@ -251,6 +254,7 @@ def main():
     ap.add_argument("--guard", type=int, default=None)
     ap.add_argument("--sweeps", type=int, default=0)
     ap.add_argument("--lam-cut0", type=float, default=0.0)
+    ap.add_argument("--window", default="mlp", choices=["mlp", "lanczos", "fixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -267,6 +271,7 @@ def main():
     cfg["block"] = args.block
     cfg["sweeps"] = args.sweeps
     cfg["lam_cut0"] = args.lam_cut0
+    cfg["window"] = args.window
     if args.guard is not None:
         cfg["guard"] = args.guard
     cfg["filter_kernel"] = args.filter_kernel
@@ -300,6 +305,9 @@ def main():
     links = generate_links(cfg, seed_offset=rank * 1000)
     T, L, nev = cfg["T"], cfg["L"], cfg["nev"]
     solver = make_solver(cfg, local)
+    if cfg.get("window", "mlp") == "mlp":
+        from laph_eigsys_b200 import window as lw
+        lw.set_model(solver, lw.load_model())
     for i in range(T):
         solver.set_links(i, links[i])
     stream = torch.cuda.ExternalStream(solver.stream())
