@@ -35,6 +35,7 @@ struct ProbState {
   int nconv;                 // wanted pairs at tolerance
   int iters;                 // outer iterations done
   int chol_fail;             // Cholesky pivot clamped in the last iteration
+  int nlock;                 // leading Ritz columns converged well below tol: not filtered
 };
 
 // Block index b -> problem p with start[p] <= b < start[p+1].

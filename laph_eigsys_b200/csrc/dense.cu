@@ -611,6 +611,12 @@ __global__ void k_resid(const ProbDesc* __restrict__ pd, ProbState* __restrict__
     S.max_resid = m;
     S.nconv = c;
     S.iters += 1;
+    // lock the leading columns whose residual is well below tol: the filter
+    // leaves them as they are (W_j = V_j); they stay in every Rayleigh-Ritz
+    // and are re-measured, so one that drifts up is unlocked next iteration
+    int nl = 0;
+    while (nl < d.nev && resid[d.kv + nl] <= 0.3 * tol) ++nl;
+    S.nlock = nl;
     if (c >= d.nev) S.active = 0;
     else atomicAdd(n_active, 1);
   }

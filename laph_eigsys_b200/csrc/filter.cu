@@ -83,8 +83,18 @@ __global__ void __launch_bounds__(128, 3)
   const int st = t % nst, cb = t / nst;
   const int s = st * 128 + threadIdx.x;
   if (s >= d.V3) return;
-  const int j0 = cb * kb;
-  const int j1 = min(j0 + kb, d.k);
+  const int j1 = min(cb * kb + kb, d.k);
+  const int nlock = ps[p].nlock;
+  if (FINAL) {
+    // locked columns: W_j = V_j
+    for (int j = cb * kb; j < min(j1, nlock); ++j) {
+      const size_t i = (size_t)d.blk + (size_t)j * d.dim + 3 * (size_t)s;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) Wp[i + a] = __ldg(Vp + i + a);
+    }
+  }
+  const int j0 = max(cb * kb, nlock);
+  if (j0 >= j1) return;
   const Lat g{d.L, d.L * d.L, d.V3};
   int sx, sy, sz;
   site_xyz(g, s, sx, sy, sz);
@@ -422,8 +432,14 @@ int cheb_step_tiled(const ProbDesc* pd, const ProbState* ps, const int* start, i
   const size_t smem = sizeof(float2) * (size_t)stage_f2 * kStages;
 #define LAPH_CHEBT(LT, HZ, FIN)                                                                                  \
   do {                                                                                                           \
-    LAPH_CUDA_TRY(cudaFuncSetAttribute(k_cheb_tile<LT, HZ, FIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                       100 * 1024));                                                             \
+    static int attr_dev = -1;                                                                                    \
+    int cur_dev = 0;                                                                                             \
+    cudaGetDevice(&cur_dev);                                                                                     \
+    if (attr_dev != cur_dev) {                                                                                   \
+      LAPH_CUDA_TRY(cudaFuncSetAttribute(k_cheb_tile<LT, HZ, FIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         100 * 1024));                                                           \
+      attr_dev = cur_dev;                                                                                        \
+    }                                                                                                            \
     k_cheb_tile<LT, HZ, FIN><<<nblk, 128, smem, st>>>(pd, ps, start, np, kb, stage_f2,                           \
                                                       reinterpret_cast<const LT*>(links), scale, X, Z, S, Y, V, W, \
                                                       tcoef, step);                                              \

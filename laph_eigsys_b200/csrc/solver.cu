@@ -23,6 +23,7 @@
 // fix_phase + recover_spectrum of the reference (src/ev_ts.cpp:197-319).
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <cstring>
 #include <vector>
 
@@ -77,6 +78,10 @@ struct laph_solver {
   double *bound = nullptr, *plaq = nullptr;
   int* wdeg = nullptr;
   int deg0 = 0;             // degree cap of the first filter pass from the model
+  // CUDA graphs of one outer iteration: the filter pass (one per degree) and
+  // the Rayleigh-Ritz pass, captured on first use and replayed
+  std::map<int, cudaGraphExec_t> g_filter;
+  cudaGraphExec_t g_rr = nullptr;
 };
 
 namespace {
@@ -131,6 +136,8 @@ int laph_solver_destroy(laph_solver* s) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->h_nactive) cudaFreeHost(s->h_nactive);
+  for (auto& kv : s->g_filter) cudaGraphExecDestroy(kv.second);
+  if (s->g_rr) cudaGraphExecDestroy(s->g_rr);
   for (auto e : s->evf) cudaEventDestroy(e);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
@@ -344,6 +351,51 @@ static int filter(laph_solver* s, int m) {
   return LAPH_OK;
 }
 
+}  // extern "C"
+
+// Capture `body` on the solver's stream into an executable graph.
+template <typename F>
+static int capture(laph_solver* s, cudaGraphExec_t* exec, F body) {
+  LAPH_CUDA_TRY(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+  const int rc = body();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s->st, &g);
+  if (rc != LAPH_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) {
+    set_error("graph capture failed: %s", cudaGetErrorString(e));
+    return LAPH_ECUDA;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    set_error("graph instantiation failed: %s", cudaGetErrorString(ei));
+    return LAPH_ECUDA;
+  }
+  return LAPH_OK;
+}
+
+static int filter_graph(laph_solver* s, int m) {
+  auto it = s->g_filter.find(m);
+  if (it == s->g_filter.end()) {
+    cudaGraphExec_t ex = nullptr;
+    LAPH_TRY(capture(s, &ex, [&] { return filter(s, m); }));
+    it = s->g_filter.emplace(m, ex).first;
+  }
+  LAPH_CUDA_TRY(cudaGraphLaunch(it->second, s->st));
+  return LAPH_OK;
+}
+
+static int rr_graph(laph_solver* s) {
+  if (!s->g_rr) LAPH_TRY(capture(s, &s->g_rr, [&] { return iteration_rr(s, 0); }));
+  LAPH_CUDA_TRY(cudaGraphLaunch(s->g_rr, s->st));
+  return LAPH_OK;
+}
+
+extern "C" {
+
 int laph_solver_run(laph_solver* s, laph_result* res) {
   if (!s) {
     set_error("null solver");
@@ -439,13 +491,13 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
       m = std::min(m, std::max(2, m_safe));
     }
     for (int i = 0; i < s->np; ++i)
-      if (s->hps[i].active) s->cnt[0] += (long long)s->hd[i].V3 * s->hd[i].k * (m - 1);
+      if (s->hps[i].active) s->cnt[0] += (long long)s->hd[i].V3 * (s->hd[i].k - s->hps[i].nlock) * (m - 1);
     s->cnt[1] += m - 1;
     s->degs.push_back(m);
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[0], s->st));
-    LAPH_TRY(filter(s, m));
+    LAPH_TRY(filter_graph(s, m));
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[1], s->st));
-    LAPH_TRY(iteration_rr(s, 0));
+    LAPH_TRY(rr_graph(s));
     nlaunch += 1 + (m - 1) + 7;
     float f = 0.f;
     LAPH_CUDA_TRY(cudaEventSynchronize(s->evf[1]));
