@@ -47,6 +47,12 @@ CONFIGS = {
     # 8^3 x 16, eps 0.4, stout 3 x 0.1, nev 60
     "c1": dict(L=8, T=16, eps=0.4, seed=1227, smear="stout", p1=0.1, p2=0.0, iters=3, compat=1, nev=60,
                guard=16, link_prec="fp32", tol=1e-9, deg=8),
+    # one launch mixing 16^3 x 32 (nev 60), 24^3 x 48 (nev 120), 32^3 x 64 (nev 180), APE 0.5 x 10
+    "c4": dict(mixed=[(16, 32, 60, 1230), (24, 48, 120, 1231), (32, 64, 180, 1232)], eps=0.3, smear="ape", p1=0.5,
+               p2=0.0, iters=10, compat=1, guard=16, link_prec="bf16", tol=1e-9, deg=48, L=32, T=144, nev=180),
+    # 48^3 x 96, eps 0.25, stout 6 x 0.1, nev 220, solved in memory-bounded waves
+    "c5": dict(L=48, T=96, eps=0.25, seed=1233, smear="stout", p1=0.1, p2=0.0, iters=6, compat=1, nev=220,
+               guard=16, link_prec="bf16", tol=1e-9, deg=48, wave=16),
 }
 HBM_FALLBACK = 6650.0
 
@@ -130,15 +136,20 @@ def filter_bytes(m, kb, link_bytes):
 
 
 def generate_links(cfg, seed_offset=0):
+    """Spatial links of one batch: list of (L, nev, links (V3, 3, 3, 3))."""
     import laph_eigsys_b200 as lb
-    conf = lb.gauge_random(cfg["L"], cfg["T"], cfg["eps"], cfg["seed"] + seed_offset)
-    return np.ascontiguousarray(conf[:, :, 1:4])  # (T, V3, 3, 3, 3) spatial links
+    out = []
+    for L, T, nev, seed in cfg.get("mixed") or [(cfg["L"], cfg.get("wave") or cfg["T"], cfg["nev"], cfg["seed"])]:
+        conf = lb.gauge_random(L, T, cfg["eps"], seed + seed_offset)
+        for t in range(T):
+            out.append((L, nev, np.ascontiguousarray(conf[t, :, 1:4])))
+    return out
 
 
-def make_solver(cfg, device):
+def make_solver(cfg, device, batch):
     import laph_eigsys_b200 as lb
     kinds = {"stout": lb.SMEAR_STOUT, "ape": lb.SMEAR_APE, "hyp": lb.SMEAR_HYP, "none": lb.SMEAR_NONE}
-    probs = [(cfg["L"], cfg["nev"])] * cfg["T"]
+    probs = [(L, nev) for L, nev, _ in batch]
     return lb.Solver(probs, device=device, smear_kind=kinds[cfg["smear"]], smear_p1=cfg["p1"], smear_p2=cfg["p2"],
                      smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
                      link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
@@ -149,11 +160,12 @@ def make_solver(cfg, device):
                          cfg.get("window", "mlp")])
 
 
-def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
+def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads, L=None, nev=None):
     """One timeslice of the reference ev_ts path on the CPU oracle: smear + Krylov-Schur on T_DEG(B)."""
     import oracle as orc
     orc.set_threads(threads)
-    L = cfg["L"]
+    L = L or cfg["L"]
+    nev = nev or cfg["nev"]
     t0 = time.perf_counter()
     if cfg["smear"] == "stout":
         Us = orc.smear_stout(links_ts, L, cfg["p1"], cfg["iters"], cfg["compat"])
@@ -163,13 +175,13 @@ def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads):
         Us = orc.smear_hyp(links_ts, L, cfg["p1"], cfg["p2"], cfg["iters"])
     else:
         Us = links_ts
-    st, theta, V, nconv, its, nmv = orc.eps_solve(Us, L, 12.0, lam_c, deg_ref, cfg["nev"], tol=1e-10, max_it=100)
+    st, theta, V, nconv, its, nmv = orc.eps_solve(Us, L, 12.0, lam_c, deg_ref, nev, tol=1e-10, max_it=100)
     Vf, ph = orc.fix_phase(V)
     dt = time.perf_counter() - t0
     return dt, dict(status=st, nconv=nconv, restarts=its, matvecs=nmv)
 
 
-def plain_gpu(cfg, links, lam_c, ntimeslices, device, deg_ref=12):
+def plain_gpu(cfg, batch, lam_c, ntimeslices, device, deg_ref=12):
     """The plain GPU form of the same workload: per timeslice, links into a
     MatShell context, smearing on the device, SLEPc-style Krylov-Schur on
     T_DEG(B) with the Krylov basis in device memory driving the GPU MatMult,
@@ -178,14 +190,14 @@ def plain_gpu(cfg, links, lam_c, ntimeslices, device, deg_ref=12):
     import torch
     import laph_eigsys_b200 as lb
     kinds = {"stout": lb.SMEAR_STOUT, "ape": lb.SMEAR_APE, "hyp": lb.SMEAR_HYP, "none": lb.SMEAR_NONE}
-    L, nev = cfg["L"], cfg["nev"]
+    L, nev = batch[0][0], batch[0][1]
     ctx = lb.Context(L, 12.0, lam_c, deg_ref, device=device)
     out = {"unit": "timeslices/s", "timeslices": ntimeslices, "basis": "device", "deg": deg_ref, "lam_l": 12.0,
            "lam_c": lam_c, "tol": 1e-10, "ncv": "max(2 nev, nev+15)"}
     t0 = time.perf_counter()
     nmv, rs = 0, 0
     for t in range(ntimeslices):
-        ctx.set_links(links[t])
+        ctx.set_links(batch[t][2])
         ctx.smear(kinds[cfg["smear"]], cfg["p1"], cfg["p2"], cfg["iters"], cfg["compat"])
         st, theta, V, nconv, its, nm = ctx.eps_solve(nev, tol=1e-10, max_it=100, device_basis=True)
         if st != 0:
@@ -206,18 +218,19 @@ def run_reference(args, cfg):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    links = generate_links(cfg)
+    batch = generate_links(cfg)
     lam_c = cfg.get("lam_c_ref", 0.65)
     deg_ref = 12
     for _ in range(args.warmup):
-        cpu_reference_step(cfg, links[0], lam_c, deg_ref, threads)
+        cpu_reference_step(cfg, batch[0][2], lam_c, deg_ref, threads, batch[0][0], batch[0][1])
     tot = 0.0
     info = None
     for k in range(args.steps):
-        dt, info = cpu_reference_step(cfg, links[k % cfg["T"]], lam_c, deg_ref, threads)
+        L, nev, U = batch[k % len(batch)]
+        dt, info = cpu_reference_step(cfg, U, lam_c, deg_ref, threads, L, nev)
         tot += dt
     value = args.steps / tot
-    sample = (f"1 timeslice per step ({cfg['L']}^3, nev {cfg['nev']}, smear + Krylov-Schur on T_{deg_ref}(B), "
+    sample = (f"1 timeslice per step ({batch[0][0]}^3, nev {batch[0][1]}, smear + Krylov-Schur on T_{deg_ref}(B), "
               f"LAM_L 12, LAM_C {lam_c}, tol 1e-10)")
     line = {"impl": "reference", "metric": "timeslices/s to nev pairs @resid<=1e-9", "value": value,
             "unit": "timeslices/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -231,8 +244,14 @@ def run_reference(args, cfg):
 
 
 def workload_config(cfg):
-    return {"workload": f"{cfg['L']}^3x{cfg['T']} eps {cfg['eps']} {cfg['smear']} {cfg['iters']}x{cfg['p1']}, "
-                        f"nev {cfg['nev']} (+{cfg['guard']} guard), resid<=1e-9",
+    if cfg.get("mixed"):
+        shape = " + ".join(f"{L}^3x{T} (nev {nev})" for L, T, nev, _ in cfg["mixed"]) + " in one batch"
+    elif cfg.get("wave"):
+        shape = f"{cfg['L']}^3x{cfg['T']} in waves of {cfg['wave']} timeslices (one wave per step), nev {cfg['nev']}"
+    else:
+        shape = f"{cfg['L']}^3x{cfg['T']}, nev {cfg['nev']}"
+    return {"workload": f"{shape}, eps {cfg['eps']} {cfg['smear']} {cfg['iters']}x{cfg['p1']}, "
+                        f"+{cfg['guard']} guard, resid<=1e-9",
             "L": cfg["L"], "timeslices": cfg["T"], "nev": cfg["nev"], "guard": cfg["guard"], "deg": cfg["deg"],
             "window": cfg.get("window", "mlp"),
             "links": cfg["link_prec"], "filter": "fp32", "rayleigh_ritz": "fp64",
@@ -302,14 +321,14 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    links = generate_links(cfg, seed_offset=rank * 1000)
-    T, L, nev = cfg["T"], cfg["L"], cfg["nev"]
-    solver = make_solver(cfg, local)
+    batch = generate_links(cfg, seed_offset=rank * 1000)
+    T = len(batch)
+    solver = make_solver(cfg, local, batch)
     if cfg.get("window", "mlp") == "mlp":
         from laph_eigsys_b200 import window as lw
         lw.set_model(solver, lw.load_model())
     for i in range(T):
-        solver.set_links(i, links[i])
+        solver.set_links(i, batch[i][2])
     stream = torch.cuda.ExternalStream(solver.stream())
 
     results = None
@@ -348,7 +367,6 @@ def main():
     m = cfg["deg"]
     kb = cfg["block"] or 32
     per_sv, _ = filter_bytes(m, kb, 0)
-    k = -(-(nev + cfg["guard"]) // 32) * 32
     link_b = 112 if cfg["link_prec"] == "bf16" else 216
     sv_iter = fsv / (m - 1)  # site-vectors per filter pass, summed over passes
     site_blocks = sv_iter / kb  # site x column-block pairs per pass
@@ -364,13 +382,16 @@ def main():
     # ---- e2e through the public API with host buffers ----------------------
     e2e = None
     if not args.no_e2e:
-        pin = torch.empty((T,) + links.shape[1:], dtype=torch.complex128, pin_memory=True)
-        pin.numpy()[...] = links
-        hl = pin.numpy()
-        dim = 3 * L ** 3
-        vbuf = torch.empty((nev, dim), dtype=torch.complex128, pin_memory=True).numpy().T  # column-major view
-        ebuf = np.empty(nev)
-        pbuf = np.empty(nev)
+        hl = []
+        for L_, nev_, U_ in batch:
+            pin = torch.empty(U_.shape, dtype=torch.complex128, pin_memory=True)
+            pin.numpy()[...] = U_
+            hl.append(pin.numpy())
+        dmax = max(3 * L_ ** 3 * nev_ for L_, nev_, _ in batch)
+        nmax = max(nev_ for _, nev_, _ in batch)
+        vflat = torch.empty(dmax, dtype=torch.complex128, pin_memory=True).numpy()
+        ebuf = np.empty(nmax)
+        pbuf = np.empty(nmax)
         barrier()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
@@ -379,20 +400,20 @@ def main():
                 solver.set_links(i, hl[i])
             st, _ = solver.run()
             for i in range(T):
-                solver.get_into(i, ebuf, vbuf, pbuf)
+                solver.get_into(i, ebuf, vflat, pbuf)
         f1.record(stream)
         barrier()
         ems = max_over_ranks(f0.elapsed_time(f1))
         e2e = {"value": world * T * args.steps / (ems / 1000.0), "unit": "timeslices/s",
-               "h2d_bytes_per_step": int(T * L ** 3 * 27 * 16),
-               "d2h_bytes_per_step": int(T * (nev * 8 + dim * nev * 16 + nev * 8)),
+               "h2d_bytes_per_step": int(sum(L_ ** 3 * 27 * 16 for L_, _, _ in batch)),
+               "d2h_bytes_per_step": int(sum(nev_ * 16 + 3 * L_ ** 3 * nev_ * 16 for L_, nev_, _ in batch)),
                "ms_per_step": ems / args.steps}
 
     # ---- plain GPU form: MatShell MatMult + Krylov-Schur, one timeslice at a time
     plain = None
     if rank == 0 and world == 1 and not args.no_plain:
         ev0, _, _ = solver.get(0, vectors=False)
-        plain = plain_gpu(cfg, links, float(1.1 * (-ev0)[-1]), args.plain_timeslices, local)
+        plain = plain_gpu(cfg, batch, float(1.1 * (-ev0)[-1]), args.plain_timeslices, local)
         plain["chosen_over_plain"] = value / plain["value"] if plain.get("value") else None
 
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
@@ -402,7 +423,7 @@ def main():
         lam = -ev0
         lam_c = float(1.1 * lam[-1])
         threads = os.cpu_count() or 1
-        dt, info = cpu_reference_step(cfg, links[0], lam_c, 12, threads)
+        dt, info = cpu_reference_step(cfg, batch[0][2], lam_c, 12, threads, batch[0][0], batch[0][1])
         cpu = {"value": 1.0 / dt, "unit": "timeslices/s", "cores": threads, "kind": "port",
                "sample": f"timeslice 0 of the workload: {cfg['smear']} smearing + Krylov-Schur on T_12(B), "
                          f"LAM_L 12, LAM_C {lam_c:.4f} (1.1 x lambda_nev from this run), tol 1e-10",

@@ -251,6 +251,10 @@ int laph_fix_phase_host(int dim, int nev, const double* V, double* Vfix, double*
 /* recover_spectrum (modules/recover_spec.cpp:45-54). */
 int laph_recover_spectrum(int nev, const double* theta, int deg, double lam_l, double lam_c, double* out);
 
+/* Timeslice block of process `rank` among `size` (src/ev_ts.cpp:103-119):
+ * contiguous blocks of LT/size, the first LT % size blocks one longer. */
+int laph_timeslice_split(int LT, int size, int rank, int* t0, int* count);
+
 /* parameters.txt (modules/par_io.cpp:8-136), same key/value rules. */
 typedef struct {
   char config_path[512], result_path[512], in_path[512], phase_path[512];

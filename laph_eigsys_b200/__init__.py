@@ -51,6 +51,13 @@ def spatial_links(conf_ts):
     return np.ascontiguousarray(np.asarray(conf_ts)[:, 1:4])
 
 
+def timeslice_split(LT, size, rank):
+    """(t0, count) of rank's contiguous timeslice block (the reference's MPI split)."""
+    t0, n = ctypes.c_int(), ctypes.c_int()
+    check(lib.laph_timeslice_split(LT, size, rank, ctypes.byref(t0), ctypes.byref(n)), "laph_timeslice_split")
+    return t0.value, n.value
+
+
 def parse_parameters(path):
     cfg = _lib.laph_config()
     check(lib.laph_parse_parameters(str(path).encode(), ctypes.byref(cfg)), "laph_parse_parameters")

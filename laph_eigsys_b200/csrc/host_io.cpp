@@ -434,6 +434,19 @@ int laph_fix_phase_host(int dim, int nev, const double* Vd, double* Vfd, double*
   return LAPH_OK;
 }
 
+int laph_timeslice_split(int LT, int size, int rank, int* t0, int* count) {
+  if (LT < 0 || size < 1 || rank < 0 || rank >= size || !t0 || !count) {
+    set_error("laph_timeslice_split: bad argument");
+    return LAPH_EINVAL;
+  }
+  // rank 0 of the reference fills todos = LT/size, adds one to the first
+  // LT % size, and chains tstart/tend (src/ev_ts.cpp:103-119)
+  const int base = LT / size, extra = LT % size;
+  *count = base + (rank < extra ? 1 : 0);
+  *t0 = rank * base + (rank < extra ? rank : extra);
+  return LAPH_OK;
+}
+
 int laph_recover_spectrum(int nev, const double* theta, int deg, double lam_l, double lam_c, double* out) {
   for (int i = 0; i < nev; ++i) {
     const double b = std::cosh(1.0 / deg * std::acosh(theta[i]));

@@ -39,16 +39,29 @@ int env_int(const char* a, const char* b, int def) {
   return v ? std::atoi(v) : def;
 }
 
-// Contiguous timeslice blocks, first LT % size blocks one longer (src/ev_ts.cpp:103-119).
-void split(int LT, int size, int rank, int* t0, int* n) {
-  const int base = LT / size, extra = LT % size;
-  *n = base + (rank < extra ? 1 : 0);
-  *t0 = rank * base + (rank < extra ? rank : extra);
-}
-
 int die(int st, const char* what) {
   std::fprintf(stderr, "laph_ev_ts: %s: %s (%s)\n", what, laph_strerror(st), laph_last_error());
   return 1;
+}
+
+// The learned-window model shipped next to the executable (data/window_mlp.bin):
+// "LAPHMLP1", int32 nparams, int32 nnorm, float32[nparams + nnorm].
+bool load_window_model(const char* exe, std::vector<float>* model) {
+  std::string dir(exe);
+  const size_t slash = dir.find_last_of('/');
+  dir = slash == std::string::npos ? std::string(".") : dir.substr(0, slash);
+  FILE* f = std::fopen((dir + "/data/window_mlp.bin").c_str(), "rb");
+  if (!f) return false;
+  char magic[8];
+  int sizes[2];
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "LAPHMLP1", 8) == 0 &&
+            std::fread(sizes, sizeof(int), 2, f) == 2 && sizes[0] == laph_mlp_nparams();
+  if (ok) {
+    model->resize(sizes[0] + sizes[1]);
+    ok = std::fread(model->data(), sizeof(float), model->size(), f) == model->size();
+  }
+  std::fclose(f);
+  return ok;
 }
 
 double trace_vdv(int dim, int nev, const double* V) {
@@ -88,7 +101,8 @@ int main(int argc, char** argv) {
   const int V3 = L * L * L, dim = 3 * V3;
   const int size = env_int("LAPH_WORLD_SIZE", "WORLD_SIZE", 1), rank = env_int("LAPH_RANK", "RANK", 0);
   int t0, ntodo;
-  split(LT, size, rank, &t0, &ntodo);
+  st = laph_timeslice_split(LT, size, rank, &t0, &ntodo);
+  if (st != LAPH_OK) return die(st, "timeslice split");
   const int device = env_int("LAPH_DEVICE", "LOCAL_RANK", 0);
   char conf_name[1100];
   std::snprintf(conf_name, sizeof conf_name, "%s/conf.%04d", P.config_path, config);
@@ -180,6 +194,15 @@ int main(int argc, char** argv) {
   laph_solver* s = nullptr;
   st = laph_solver_create(&s, probs.data(), ntodo, &o, device);
   if (st != LAPH_OK) return die(st, "solver");
+  if (o.window == LAPH_WINDOW_MLP) {
+    std::vector<float> model;
+    if (!load_window_model(argv[0], &model)) {
+      std::fprintf(stderr, "laph_ev_ts: window = mlp but data/window_mlp.bin is missing or invalid\n");
+      return 1;
+    }
+    st = laph_solver_set_window_model(s, model.data(), (int)model.size());
+    if (st != LAPH_OK) return die(st, "window model");
+  }
   for (int ts = 0; ts < ntodo; ++ts) {
     st = laph_solver_set_links(s, ts, conf.data() + (size_t)ts * V3 * 72, LAPH_LAYOUT_CONF, 0);
     if (st != LAPH_OK) return die(st, "links");
