@@ -166,8 +166,7 @@ typedef struct {
   int phase_fix;        /* apply fix_phase to the output eigenvectors             */
   uint64_t seed;        /* start block                                            */
   int block;            /* columns per CTA of the filter kernel, 8..64 (0: 32)     */
-  int filter_kernel;    /* 0 auto, 1 register-resident links + L2 bulk prefetch,
-                           2 shared-memory staged rows (even L only)              */
+  int filter_kernel;    /* 0 or 1: register-resident links + L2 bulk prefetch      */
   int jacobi_sweeps;    /* cap on Jacobi sweeps per Rayleigh-Ritz (0: 2); an
                            unfinished sweep set only delays convergence, since
                            residuals are always computed from the new vectors   */

@@ -21,8 +21,6 @@ struct ProbDesc {
   long long tc;    // Chebyshev coefficient table [(mdeg+1)][k]
   int nchunk;      // row chunks of the Gram reduction
   int nrt;         // row tiles of the rotation
-  int zr;          // z-rows per CTA of the staged filter (zr | L, zr*L <= 128)
-  int pad_;
 };
 
 // Window/state per problem, written by the device.

@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(128) k_residual64(const ProbDesc* __restrict__
       const double2 xs = __ldg(x + 3 * (size_t)s + a);
       const double2 r = make_double2((6.0 - th) * xs.x - acc[a].x, (6.0 - th) * xs.y - acc[a].y);
       rr += r.x * r.x + r.y * r.y;
-      Sp[col + 3 * (size_t)s + a] = make_float2((float)(sc * r.x), (float)(sc * r.y));
+      Sp[col + (size_t)a * d.V3 + s] = make_float2((float)(sc * r.x), (float)(sc * r.y));  // colour-major
     }
   }
   // block reduction (fixed order)

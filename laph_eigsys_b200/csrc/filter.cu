@@ -9,7 +9,10 @@
 // walks kb columns, so the 6 links a site needs (its 3 forward links and the
 // 3 backward links U_mu(x-mu)) are read from HBM once per kb vectors and held
 // in 108 registers; the vector reads of consecutive threads are consecutive
-// 24-byte site vectors (fully coalesced), neighbour reuse comes from L1/L2.
+// site values (fully coalesced), neighbour reuse comes from L1/L2.  Inside
+// each column the FP32 buffers (S and the E ring) are colour-major,
+// element (site, c) at c*V3 + site, so every warp load is one dense 256-byte
+// access; the FP64 blocks keep the reference's 3*site + colour order.
 // Per-column coefficients (a_j, z_j, g_j) come from a device table written by
 // the Rayleigh-Ritz step, so every launch of an iteration is identical.
 // Algorithmic bytes per site and vector: 24 (X) + 24 (S) + 24 (Z) + 24 (Y)
@@ -127,12 +130,15 @@ __global__ void __launch_bounds__(128, 3)
   const bool pf = threadIdx.x == 0 && (nsite % 2 == 0) && (d.dim % 2 == 0);
   auto prefetch = [&](int j) {
     if (!pf || j >= j1) return;
-    const size_t col = base + (size_t)j * d.dim + 3 * (size_t)s0;
-    const unsigned bytes = 24u * nsite;
-    l2_prefetch(Xp + col, bytes);
-    l2_prefetch(Sp + col, bytes);
-    if (HAS_Z) l2_prefetch(Zp + col, bytes);
-    if (FINAL) l2_prefetch(Vp + col, 2 * bytes);
+    const size_t col = base + (size_t)j * d.dim;
+    const unsigned bytes = 8u * nsite;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      l2_prefetch(Xp + col + (size_t)c * d.V3 + s0, bytes);
+      l2_prefetch(Sp + col + (size_t)c * d.V3 + s0, bytes);
+      if (HAS_Z) l2_prefetch(Zp + col + (size_t)c * d.V3 + s0, bytes);
+    }
+    if (FINAL) l2_prefetch(Vp + col + 3 * (size_t)s0, 6 * bytes);
   };
 #pragma unroll 1
   for (int j = j0; j < min(j1, j0 + kPrefetch); ++j) prefetch(j);
@@ -147,8 +153,8 @@ __global__ void __launch_bounds__(128, 3)
       float2 xu[3], xd[3];
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        xu[b] = __ldg(x + 3 * (size_t)up[mu] + b);
-        xd[b] = __ldg(x + 3 * (size_t)dn[mu] + b);
+        xu[b] = __ldg(x + (size_t)b * d.V3 + up[mu]);
+        xd[b] = __ldg(x + (size_t)b * d.V3 + dn[mu]);
       }
 #pragma unroll
       for (int a = 0; a < 3; ++a)
@@ -164,8 +170,8 @@ __global__ void __launch_bounds__(128, 3)
     const float gj = (float)__ldg(tc + 2 * d.k + j);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const size_t i = col + 3 * (size_t)s + a;
-      const float2 xs = __ldg(x + 3 * (size_t)s + a);
+      const size_t i = col + (size_t)a * d.V3 + s;  // colour-major FP32 buffers
+      const float2 xs = __ldg(x + (size_t)a * d.V3 + s);
       const float2 ss = __ldg(Sp + i);
       float2 r;
       r.x = fmaf(a_h, acc[a].x, fmaf(a_d, xs.x, gj * ss.x));
@@ -176,178 +182,16 @@ __global__ void __launch_bounds__(128, 3)
         r.y = fmaf(zc, zz.y, r.y);
       }
       if (FINAL) {
-        // W = T_m(theta_B) V + E_m in FP64
+        // W = T_m(theta_B) V + E_m in FP64 (FP64 blocks keep the 3*site + colour order)
         const double tm = __ldg(tc + (size_t)3 * d.k + j);
-        const double2 v = __ldg(Vp + i);
-        Wp[i] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
+        const size_t iv = col + 3 * (size_t)s + a;
+        const double2 v = __ldg(Vp + iv);
+        Wp[iv] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
       } else {
         Yp[i] = r;
       }
     }
   }
-}
-
-// ------------------------------------------- the filter, smem-staged -----
-// Same arithmetic as k_cheb_mrhs for even L.  A CTA owns zr consecutive
-// z-rows (x0, y0..y0+zr-1), one thread per site, and walks its kb columns.
-// For every column the rows it needs -- its own rows of X, S and Z, the two
-// y-halo rows and the 2*zr rows of the x-1 / x+1 planes of X -- are copied
-// global -> shared with 16-byte cp.async into a 3-stage ring, two columns
-// ahead of the one being computed, so DRAM latency overlaps the stencil math
-// instead of stalling it.  Each z-row of a column is 24*L contiguous bytes
-// (16-byte aligned for even L).  Slots of the X tile: [0, zr) own rows,
-// zr: row y0-1, zr+1: row y0+zr, zr+2+i: (x0+1, y0+i), 2zr+2+i: (x0-1, y0+i).
-constexpr int kStages = 3;
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-template <typename LT, bool HAS_Z, bool FINAL>
-__global__ void __launch_bounds__(128, 3)
-    k_cheb_tile(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, const int* __restrict__ start, int np,
-                int kb, int stage_f2, const LT* __restrict__ links, const float* __restrict__ scale,
-                const float2* __restrict__ Xp, const float2* __restrict__ Zp, const float2* __restrict__ Sp,
-                float2* __restrict__ Yp, const double2* __restrict__ Vp, double2* __restrict__ Wp,
-                const double* __restrict__ tcoef, int step) {
-  extern __shared__ float4 smem_raw[];
-  float2* smem = reinterpret_cast<float2*>(smem_raw);
-  const int p = find_prob(start, np, blockIdx.x);
-  if (!ps[p].active) return;
-  const ProbDesc d = pd[p];
-  const int L = d.L, zr = d.zr, row3 = 3 * L;
-  const int ntile = (L * L) / zr;
-  const int t = blockIdx.x - start[p];
-  const int tile = t % ntile, cb = t / ntile;
-  const int x0 = (tile * zr) / L, y0 = (tile * zr) % L;
-  const int j0 = cb * kb, j1 = min(j0 + kb, d.k), nc = j1 - j0;
-  const int nthr = zr * L;
-  const int tid = threadIdx.x;
-  const bool worker = tid < nthr;
-  const int ri = worker ? tid / L : 0, z = worker ? tid % L : 0;
-  const Lat g{L, L * L, d.V3};
-  const int s = x0 * g.L2 + (y0 + ri) * L + z;
-  // X-tile slot of each row and its global row index (x*L + y)
-  const int nx = 3 * zr + 2, ns = zr, nz = HAS_Z ? zr : 0;
-  const int nrows = nx + ns + nz;
-  auto row_of = [&](int r) -> int {  // global (x*L + y) of stage row r
-    int q = r;
-    if (q >= nx) q = (q - nx) % zr;  // S / Z rows: own rows
-    if (q < zr) return x0 * L + y0 + q;
-    if (q == zr) return x0 * L + (y0 + L - 1) % L;
-    if (q == zr + 1) return x0 * L + (y0 + zr) % L;
-    if (q < 2 * zr + 2) return ((x0 + 1) % L) * L + y0 + (q - zr - 2);
-    return ((x0 + L - 1) % L) * L + y0 + (q - 2 * zr - 2);
-  };
-  const size_t base = (size_t)d.blk;
-  const int chunks_per_row = (row3 * 8) / 16;
-  auto issue = [&](int c) {
-    if (c < nc) {
-      const size_t col = base + (size_t)(j0 + c) * d.dim;
-      float2* buf = smem + (size_t)(c % kStages) * stage_f2;
-      const int tot = nrows * chunks_per_row;
-      for (int q = tid; q < tot; q += blockDim.x) {
-        const int r = q / chunks_per_row, ch = q - r * chunks_per_row;
-        const float2* src = (r < nx ? Xp : (r < nx + ns ? Sp : Zp)) + col + (size_t)row_of(r) * row3 + 2 * ch;
-        cp_async16(buf + (size_t)r * row3 + 2 * ch, src);
-      }
-    }
-    cp_async_commit();
-  };
-  // links of this site into registers (once per kb columns)
-  int dn[3];
-  {
-    int sx, sy, sz;
-    site_xyz(g, s, sx, sy, sz);
-#pragma unroll
-    for (int mu = 0; mu < 3; ++mu) dn[mu] = nb_dn(g, sx, sy, sz, mu);
-  }
-  const LT* U = links + d.uf;
-  const float* scl = scale + d.sc;
-  float2 uf[3][9], ub[3][9];
-  if (worker) {
-#pragma unroll
-    for (int mu = 0; mu < 3; ++mu)
-#pragma unroll
-      for (int e = 0; e < 9; ++e) {
-        uf[mu][e] = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + s, s);
-        ub[mu][e] = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + dn[mu], dn[mu]);
-      }
-  }
-  const double c_hop = ps[p].c_hop, c_diag = ps[p].c_diag;
-  const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
-  // neighbour slots/columns inside the X tile
-  const int zp = (z + 1 == L) ? 0 : z + 1, zm = (z == 0) ? L - 1 : z - 1;
-  const int yp_slot = (ri + 1 < zr) ? ri + 1 : zr + 1, ym_slot = (ri >= 1) ? ri - 1 : zr;
-  const int xp_slot = zr + 2 + ri, xm_slot = 2 * zr + 2 + ri;
-  const int up_off[3] = {xp_slot * row3 + 3 * z, yp_slot * row3 + 3 * z, ri * row3 + 3 * zp};
-  const int dn_off[3] = {xm_slot * row3 + 3 * z, ym_slot * row3 + 3 * z, ri * row3 + 3 * zm};
-  const int self_off = ri * row3 + 3 * z;
-  const int s_off = nx * row3 + self_off, z_off = (nx + ns) * row3 + self_off;
-
-#pragma unroll
-  for (int c = 0; c < kStages - 1; ++c) issue(c);
-#pragma unroll 1
-  for (int c = 0; c < nc; ++c) {
-    issue(c + kStages - 1);
-    cp_async_wait<kStages - 1>();
-    __syncthreads();
-    const float2* buf = smem + (size_t)(c % kStages) * stage_f2;
-    if (worker) {
-      const int j = j0 + c;
-      float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-#pragma unroll
-      for (int mu = 0; mu < 3; ++mu) {
-        float2 xu[3], xd[3];
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          xu[b] = buf[up_off[mu] + b];
-          xd[b] = buf[dn_off[mu] + b];
-        }
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            cfmaf(acc[a], uf[mu][3 * a + b], xu[b]);
-            cfmacf(acc[a], ub[mu][3 * b + a], xd[b]);
-          }
-      }
-      const double aj = __ldg(tc + j);
-      const float a_h = (float)(aj * c_hop), a_d = (float)(aj * c_diag);
-      const float zc = (float)__ldg(tc + d.k + j);
-      const float gj = (float)__ldg(tc + 2 * d.k + j);
-      const size_t col = base + (size_t)j * d.dim;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float2 xs = buf[self_off + a];
-        const float2 ss = buf[s_off + a];
-        float2 r;
-        r.x = fmaf(a_h, acc[a].x, fmaf(a_d, xs.x, gj * ss.x));
-        r.y = fmaf(a_h, acc[a].y, fmaf(a_d, xs.y, gj * ss.y));
-        if (HAS_Z) {
-          const float2 zz = buf[z_off + a];
-          r.x = fmaf(zc, zz.x, r.x);
-          r.y = fmaf(zc, zz.y, r.y);
-        }
-        const size_t i = col + 3 * (size_t)s + a;
-        if (FINAL) {
-          const double tm = __ldg(tc + (size_t)3 * d.k + j);
-          const double2 v = __ldg(Vp + i);
-          Wp[i] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
-        } else {
-          Yp[i] = r;
-        }
-      }
-    }
-    __syncthreads();
-  }
-  cp_async_wait<0>();
 }
 
 // ------------------------------------------------ FP64 block stencil: A W --
@@ -421,42 +265,6 @@ __global__ void k_random_block(const ProbDesc* __restrict__ pd, const int* __res
 int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const double2* U64, float2* Uf32, void* Ubf,
                float* scale, int bf16, cudaStream_t st) {
   k_pack_links<<<nblk, 128, 0, st>>>(pd, start, np, U64, Uf32, reinterpret_cast<__nv_bfloat162*>(Ubf), scale, bf16);
-  LAPH_CUDA_TRY(cudaGetLastError());
-  return LAPH_OK;
-}
-
-int cheb_step_tiled(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb,
-                    int stage_f2, int bf16, const void* links, const float* scale, const float2* X, const float2* Z,
-                    const float2* S, float2* Y, const double2* V, double2* W, const double* tcoef, int step,
-                    bool final_step, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * (size_t)stage_f2 * kStages;
-#define LAPH_CHEBT(LT, HZ, FIN)                                                                                  \
-  do {                                                                                                           \
-    static int attr_dev = -1;                                                                                    \
-    int cur_dev = 0;                                                                                             \
-    cudaGetDevice(&cur_dev);                                                                                     \
-    if (attr_dev != cur_dev) {                                                                                   \
-      LAPH_CUDA_TRY(cudaFuncSetAttribute(k_cheb_tile<LT, HZ, FIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                         100 * 1024));                                                           \
-      attr_dev = cur_dev;                                                                                        \
-    }                                                                                                            \
-    k_cheb_tile<LT, HZ, FIN><<<nblk, 128, smem, st>>>(pd, ps, start, np, kb, stage_f2,                           \
-                                                      reinterpret_cast<const LT*>(links), scale, X, Z, S, Y, V, W, \
-                                                      tcoef, step);                                              \
-  } while (0)
-  const bool hz = Z != nullptr;
-  if (bf16) {
-    if (hz && final_step) LAPH_CHEBT(__nv_bfloat162, true, true);
-    else if (hz) LAPH_CHEBT(__nv_bfloat162, true, false);
-    else if (final_step) LAPH_CHEBT(__nv_bfloat162, false, true);
-    else LAPH_CHEBT(__nv_bfloat162, false, false);
-  } else {
-    if (hz && final_step) LAPH_CHEBT(float2, true, true);
-    else if (hz) LAPH_CHEBT(float2, true, false);
-    else if (final_step) LAPH_CHEBT(float2, false, true);
-    else LAPH_CHEBT(float2, false, false);
-  }
-#undef LAPH_CHEBT
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

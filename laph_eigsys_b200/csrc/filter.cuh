@@ -12,12 +12,6 @@ int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const dou
 int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
               const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
               const double2* V, double2* W, const double* tcoef, int step, bool final_step, cudaStream_t st);
-// Same step through the shared-memory staged kernel (all L even); stage_f2 =
-// float2 elements of one pipeline stage (max over problems of (5 zr + 2) * 3 L).
-int cheb_step_tiled(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb,
-                    int stage_f2, int bf16, const void* links, const float* scale, const float2* X, const float2* Z,
-                    const float2* S, float2* Y, const double2* V, double2* W, const double* tcoef, int step,
-                    bool final_step, cudaStream_t st);
 // Y = (-Delta) W for every column, FP64.
 int neglap64_batch(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
                    const double2* W, double2* Y, cudaStream_t st);

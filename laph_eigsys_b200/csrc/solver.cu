@@ -47,9 +47,8 @@ struct laph_solver {
   ProbState* d_ps = nullptr;
   std::vector<ProbState> hps;
   // CTA -> problem prefix tables
-  int *st_tile = nullptr, *st_site = nullptr, *st_filt = nullptr, *st_nl = nullptr, *st_gram = nullptr, *st_gred = nullptr,
+  int *st_site = nullptr, *st_filt = nullptr, *st_nl = nullptr, *st_gram = nullptr, *st_gred = nullptr,
       *st_rot = nullptr, *st_rand = nullptr, *st_col = nullptr;
-  int nb_tile = 0, stage_f2 = 0, all_even = 1;
   int nb_site = 0, nb_filt = 0, nb_nl = 0, nb_gram = 0, nb_gred = 0, nb_rot = 0, nb_rand = 0, nb_col = 0;
   // pools
   double2 *U64raw = nullptr, *U64 = nullptr, *Utmp = nullptr, *dec = nullptr, *stage = nullptr;
@@ -129,7 +128,7 @@ int laph_solver_destroy(laph_solver* s) {
   if (!s) return LAPH_OK;
   cudaSetDevice(s->dev);
   if (s->st) cudaStreamSynchronize(s->st);
-  void* ptrs[] = {s->d_pd, s->d_ps, s->st_tile, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
+  void* ptrs[] = {s->d_pd, s->d_ps, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
                   s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
                   s->phases, s->norms, s->d_nactive, s->model, s->feats, s->mwork, s->bound, s->plaq, s->wdeg};
@@ -159,9 +158,9 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     return LAPH_ENODEV;
   }
   if (opts->deg < 2 || opts->deg > 64 || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1 ||
-      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 2) {
+      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 1) {
     set_error("laph_solver_create: need 2 <= deg <= 64, guard >= 0, tol > 0, max_it >= 1, 0 <= block <= 512, "
-              "filter_kernel in {0, 1, 2}");
+              "filter_kernel in {0, 1}");
     return LAPH_EINVAL;
   }
   for (int i = 0; i < n; ++i) {
@@ -190,7 +189,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   // descriptors and pool offsets
   long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
   size_t max_run = 0, max_v3 = 0;
-  std::vector<int> per_tile, per_site, per_filt, per_nl, per_gram, per_gred, per_rot, per_rand, per_col;
+  std::vector<int> per_site, per_filt, per_nl, per_gram, per_gred, per_rot, per_rand, per_col;
   for (int i = 0; i < n; ++i) {
     ProbDesc d{};
     d.L = probs[i].L;
@@ -211,11 +210,6 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     const int chunk_rows = 8192;
     d.nchunk = (d.dim + chunk_rows - 1) / chunk_rows;
     d.nrt = (d.V3 + 127) / 128;  // site tiles of the residual kernel
-    d.zr = 1;
-    for (int r = 1; r <= d.L; ++r)
-      if (d.L % r == 0 && r * d.L <= 128) d.zr = r;
-    if (d.L % 2) s->all_even = 0;
-    s->stage_f2 = std::max(s->stage_f2, (5 * d.zr + 2) * 3 * d.L);
     const int T = d.k / kGramTile, npair = T * (T + 1) / 2;
     o_u64 += 27LL * d.V3;
     o_uf += 27LL * d.V3;
@@ -231,7 +225,6 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     const int nst = (d.V3 + 127) / 128;
     per_site.push_back(nst);
     per_filt.push_back(nst * ((d.k + s->kb - 1) / s->kb));
-    per_tile.push_back((d.L * d.L / d.zr) * ((d.k + s->kb - 1) / s->kb));
     per_nl.push_back(nst * d.k);
     per_gram.push_back(d.nchunk * npair);
     per_gred.push_back((2 * npair * kGramTile * kGramTile + 255) / 256);
@@ -269,7 +262,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     cudaGetLastError();
     return fail(LAPH_ENOMEM);
   }
-  if ((rc = upload_prefix(per_tile, &s->st_tile, &s->nb_tile)) || (rc = upload_prefix(per_site, &s->st_site, &s->nb_site)) || (rc = upload_prefix(per_filt, &s->st_filt, &s->nb_filt)) ||
+  if ((rc = upload_prefix(per_site, &s->st_site, &s->nb_site)) || (rc = upload_prefix(per_filt, &s->st_filt, &s->nb_filt)) ||
       (rc = upload_prefix(per_nl, &s->st_nl, &s->nb_nl)) || (rc = upload_prefix(per_gram, &s->st_gram, &s->nb_gram)) ||
       (rc = upload_prefix(per_gred, &s->st_gred, &s->nb_gred)) || (rc = upload_prefix(per_rot, &s->st_rot, &s->nb_rot)) ||
       (rc = upload_prefix(per_rand, &s->st_rand, &s->nb_rand)) || (rc = upload_prefix(per_col, &s->st_col, &s->nb_col)))
@@ -341,12 +334,8 @@ static int filter(laph_solver* s, int m) {
     const float2* X = (n == 1) ? s->S : s->E[(n - 2) % 3];
     const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
     float2* Yo = s->E[(n - 1) % 3];
-    if (s->all_even && s->o.filter_kernel == 2)
-      LAPH_TRY(cheb_step_tiled(s->d_pd, s->d_ps, s->st_tile, s->np, s->nb_tile, s->kb, s->stage_f2, bf, links, s->scale,
-                               X, Z, s->S, Yo, s->V, s->W, s->tcoef, n, fin, s->st));
-    else
-      LAPH_TRY(cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo,
-                         s->V, s->W, s->tcoef, n, fin, s->st));
+    LAPH_TRY(cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo,
+                       s->V, s->W, s->tcoef, n, fin, s->st));
   }
   return LAPH_OK;
 }
