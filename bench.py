@@ -38,9 +38,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
-    # 32^3 x 64, eps 0.3, stout 5 x 0.1, nev 120 (+16 guard), BF16 links
+    # 32^3 x 64, eps 0.3, stout 5 x 0.1, nev 120 (+16 guard), FP32 filter links
     "c3": dict(L=32, T=64, eps=0.3, seed=1229, smear="stout", p1=0.1, p2=0.0, iters=5, compat=1, nev=120,
-               guard=16, link_prec="bf16", tol=1e-9, deg=48),
+               guard=16, link_prec="fp32", tol=1e-9, deg=48),
     # 24^3 x 48, eps 0.3, HYP 0.62/0.62 x 1, nev 120
     "c2": dict(L=24, T=48, eps=0.3, seed=1228, smear="hyp", p1=0.62, p2=0.62, iters=1, compat=0, nev=120,
                guard=16, link_prec="fp32", tol=1e-9, deg=12),
@@ -49,10 +49,10 @@ CONFIGS = {
                guard=16, link_prec="fp32", tol=1e-9, deg=8),
     # one launch mixing 16^3 x 32 (nev 60), 24^3 x 48 (nev 120), 32^3 x 64 (nev 180), APE 0.5 x 10
     "c4": dict(mixed=[(16, 32, 60, 1230), (24, 48, 120, 1231), (32, 64, 180, 1232)], eps=0.3, smear="ape", p1=0.5,
-               p2=0.0, iters=10, compat=1, guard=16, link_prec="bf16", tol=1e-9, deg=48, L=32, T=144, nev=180),
+               p2=0.0, iters=10, compat=1, guard=16, link_prec="fp32", tol=1e-9, deg=48, L=32, T=144, nev=180),
     # 48^3 x 96, eps 0.25, stout 6 x 0.1, nev 220, solved in memory-bounded waves
     "c5": dict(L=48, T=96, eps=0.25, seed=1233, smear="stout", p1=0.1, p2=0.0, iters=6, compat=1, nev=220,
-               guard=16, link_prec="bf16", tol=1e-9, deg=48, wave=16),
+               guard=16, link_prec="fp32", tol=1e-9, deg=48, wave=16),
 }
 HBM_FALLBACK = 6650.0
 
@@ -154,7 +154,7 @@ def make_solver(cfg, device, batch):
                      smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
                      link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
                      max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
-                     filter_kernel=cfg.get("filter_kernel", 0), jacobi_sweeps=cfg.get("sweeps", 0),
+                     filter_kernel=cfg.get("filter_kernel", 1), jacobi_sweeps=cfg.get("sweeps", 0),
                      lam_cut=cfg.get("lam_cut0", 0.0),
                      window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
                          cfg.get("window", "mlp")])
@@ -269,7 +269,7 @@ def main():
     ap.add_argument("--link-prec", default=None, choices=["bf16", "fp32"])
     ap.add_argument("--timeslices", type=int, default=None)
     ap.add_argument("--block", type=int, default=0)
-    ap.add_argument("--filter-kernel", type=int, default=0)
+    ap.add_argument("--filter-kernel", type=int, default=1, choices=[0, 1])
     ap.add_argument("--guard", type=int, default=None)
     ap.add_argument("--sweeps", type=int, default=0)
     ap.add_argument("--lam-cut0", type=float, default=0.0)

@@ -155,7 +155,8 @@ typedef struct {
   double smear_p1, smear_p2;
   int smear_iters;
   int smear_compat;
-  int guard;            /* block vectors beyond nev (>= 0; rounded up to a multiple of 8) */
+  int guard;            /* block vectors beyond nev (>= 0); the block width
+                           nev + guard is rounded up to a multiple of 32         */
   int link_prec;        /* LAPH_LINKS_FP32 / LAPH_LINKS_BF16                      */
   double tol;           /* target ||(-Delta)v - lambda v|| / (||v|| lambda_max)   */
   int max_it;           /* outer iterations                                       */
@@ -166,7 +167,9 @@ typedef struct {
   int phase_fix;        /* apply fix_phase to the output eigenvectors             */
   uint64_t seed;        /* start block                                            */
   int block;            /* columns per CTA of the filter kernel, 8..64 (0: 32)     */
-  int filter_kernel;    /* 0 or 1: register-resident links + L2 bulk prefetch      */
+  int filter_kernel;    /* filter variant, both with register-resident links and L2
+                           bulk prefetch: 0 FP64 coefficients per thread; 1 FP32
+                           coefficients staged per CTA (default; block <= 64)    */
   int jacobi_sweeps;    /* cap on Jacobi sweeps per Rayleigh-Ritz (0: 2); an
                            unfinished sweep set only delays convergence, since
                            residuals are always computed from the new vectors   */

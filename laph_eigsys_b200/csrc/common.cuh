@@ -68,6 +68,19 @@ __host__ __device__ __forceinline__ void cfmacf(float2& acc, float2 a, float2 b)
   acc.y = fmaf(-a.y, b.x, acc.y);
 }
 
+// ------------------------------------------------------------- cp.async ---
+// 16-byte global -> shared copy that bypasses L1; ok == false writes zeros and
+// reads nothing (src-size 0), src must still be a mapped address.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool ok) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(ok ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ------------------------------------------------------------ lattice idx ---
 // site = x*L*L + y*L + z, periodic (modules/navigation.cpp:27-88).
 struct Lat {

@@ -19,8 +19,11 @@ namespace laph {
 // ------------------------------------------------------------------ Gram ---
 // CTA: 64 threads, output tiles G[ti,tj] = W_ti^H W_tj and H[ti,tj] = W_ti^H Y_tj
 // (32 x 32 each, thread 4x4 complex of both), over the rows of one chunk;
-// the W_ti tile is staged once for both products.
-constexpr int GT = 32, GK = 16;
+// the W_ti tile is staged once for both products.  Rows arrive through a
+// two-stage cp.async ring (dynamic shared memory [stage][A|W|Y][col][GP]),
+// so the next 16 rows load while the current 16 are multiplied.
+constexpr int GT = 32, GK = 16, GP = GK + 1;
+constexpr int kGramSmem = 2 * 3 * GT * GP * (int)sizeof(double2);
 
 __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
                                              const int* __restrict__ start, int np, int chunk_rows,
@@ -44,34 +47,52 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
   const double2* BW = W + d.blk + (size_t)(tj * GT) * d.dim;
   const double2* BY = Y + d.blk + (size_t)(tj * GT) * d.dim;
   const int r0 = chunk * chunk_rows, r1 = min(d.dim, r0 + chunk_rows);
-  __shared__ double2 sA[GK][GT + 1], sW[GK][GT + 1], sY[GK][GT + 1];
+  extern __shared__ double2 gsm[];
   const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
-  double2 ag[4][4], ah[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) ag[a][b] = ah[a][b] = make_double2(0.0, 0.0);
-  for (int r = r0; r < r1; r += GK) {
+  // thread -> (column c, row q) of each staged 32 x 16 slab: 16 threads per column, 256 B contiguous
+  auto load = [&](int r, int b) {
+    double2* s = gsm + b * 3 * GT * GP;
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const int idx = threadIdx.x + 64 * e;
       const int c = idx >> 4, q = idx & 15;
       const int row = r + q;
       const bool ok = row < r1;
-      sA[q][c] = ok ? __ldg(A + (size_t)c * d.dim + row) : make_double2(0.0, 0.0);
-      sW[q][c] = ok ? __ldg(BW + (size_t)c * d.dim + row) : make_double2(0.0, 0.0);
-      sY[q][c] = ok ? __ldg(BY + (size_t)c * d.dim + row) : make_double2(0.0, 0.0);
+      const size_t off = (size_t)c * d.dim + (ok ? row : 0);
+      cp_async16(s + c * GP + q, A + off, ok);
+      cp_async16(s + (GT + c) * GP + q, BW + off, ok);
+      cp_async16(s + (2 * GT + c) * GP + q, BY + off, ok);
+    }
+    cp_async_commit();
+  };
+  double2 ag[4][4], ah[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) ag[a][b] = ah[a][b] = make_double2(0.0, 0.0);
+  const int nstep = (r1 - r0 + GK - 1) / GK;
+  load(r0, 0);
+  for (int it = 0; it < nstep; ++it) {
+    const int b = it & 1;
+    if (it + 1 < nstep) {
+      load(r0 + (it + 1) * GK, b ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const double2* sA = gsm + b * 3 * GT * GP;
+    const double2* sW = sA + GT * GP;
+    const double2* sY = sW + GT * GP;
 #pragma unroll
     for (int q = 0; q < GK; ++q) {
       double2 a[4], bw[4], by[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = sA[q][ty + 8 * i];
+      for (int i = 0; i < 4; ++i) a[i] = sA[(ty + 8 * i) * GP + q];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        bw[j] = sW[q][tx + 8 * j];
-        by[j] = sY[q][tx + 8 * j];
+        bw[j] = sW[(tx + 8 * j) * GP + q];
+        by[j] = sY[(tx + 8 * j) * GP + q];
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
@@ -140,9 +161,18 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
                                                 double2* __restrict__ KK, double* __restrict__ theta,
                                                 double* __restrict__ tcoef, double* __restrict__ scol,
                                                 double* __restrict__ dwork, int first_iter, int fixed_cut,
-                                                int max_sweeps) {
+                                                int max_sweeps, unsigned long long* __restrict__ tstamp) {
   const int p = blockIdx.x;
   if (!ps[p].active) return;
+  // phase boundaries (global timer, ns) for the solver's trace: [p][0..6]
+  auto stamp = [&](int ph) {
+    if (threadIdx.x == 0) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      tstamp[p * kSmallPhases + ph] = t;
+    }
+  };
+  stamp(0);
   const ProbDesc d = pd[p];
   const int k = d.k, tid = threadIdx.x, nt = blockDim.x;
   const size_t kk2 = (size_t)k * k;
@@ -197,6 +227,7 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     }
     __syncthreads();
   }
+  stamp(1);
   // (c) Minv = D^{-1} R^{-1} (upper triangular), column by column
   for (size_t e = tid; e < kk2; e += nt) Mi[e] = make_double2(0.0, 0.0);
   __syncthreads();
@@ -219,6 +250,7 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     Mi[e] = cscal(Mi[e], dinv[i]);
   }
   __syncthreads();
+  stamp(2);
   // (d) T1 = H Minv ; Ht = Minv^H T1 (Hermitian part)
   for (size_t e = tid; e < kk2; e += nt) {
     const int i = (int)(e % k), j = (int)(e / k);
@@ -247,20 +279,32 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     Q[e] = make_double2(i == j ? 1.0 : 0.0, 0.0);
   }
   __syncthreads();
-  // (e) cyclic Jacobi, round-robin ordering of k/2 disjoint pairs per step
-  __shared__ double s_c[512], s_s[512];
-  __shared__ double2 s_e[512];
-  __shared__ int s_p[512], s_q[512];
+  stamp(3);
+  // (e) cyclic Jacobi in "position order": in every step position i is paired
+  // with its mirror k-1-i, and after the rotations positions 1..k-1 shift by
+  // one (round-robin tournament: every pair meets once in k-1 steps).  The
+  // shift is folded into the update, which writes the rotated 2x2 blocks of
+  // Ht (and the rotated column pairs of Q) to their new positions in a second
+  // buffer, so each step is one read and one write of both matrices with
+  // unit-stride warp accesses.  Ht ping-pongs with the H storage, Q with the
+  // G storage; Q's rows stay in the original basis order and its columns
+  // follow Ht's diagonal, which is all the sort below needs.
+  __shared__ double s_c[256], s_s[256];
+  __shared__ double2 s_e[256];
   const int half = k / 2;
+  double2* hc = Ht;  // current Ht
+  double2* hn = H;   // next Ht
+  double2* qc = Q;
+  double2* qn = G;
+  auto shift = [&](int pos) { return pos == 0 ? 0 : (pos == k - 1 ? 1 : pos + 1); };
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     double off = 0.0, dia = 0.0;
     for (size_t e = tid; e < kk2; e += nt) {
       const int i = (int)(e % k), j = (int)(e / k);
-      const double2 v = Ht[e];
+      const double2 v = hc[e];
       if (i != j) off += v.x * v.x + v.y * v.y;
       else dia += v.x * v.x;
     }
-    // block reduce off and dia
     for (int o = 16; o > 0; o >>= 1) {
       off += __shfl_xor_sync(0xffffffffu, off, o);
       dia += __shfl_xor_sync(0xffffffffu, dia, o);
@@ -285,73 +329,87 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     // leaves eigenvector errors below 1e-10, far under the residual target
     if (s_red[0] <= 1e-27 * s_red[1]) break;
     for (int step = 0; step < k - 1; ++step) {
+      // rotation of pair r = (r, k-1-r): J (p,p)=c (p,q)=s (q,p)=-s e (q,q)=c e, e = e^{-i phi}
       for (int r = tid; r < half; r += nt) {
-        auto rot = [&](int pos) { return ((pos - 1 + step) % (k - 1)) + 1; };
-        const int pp = (r == 0) ? 0 : rot(r);
-        const int qq = rot(k - 1 - r);
-        const int pa = min(pp, qq), qb = max(pp, qq);
-        const double2 g = at(Ht, k, pa, qb);
+        const int pa = r, qb = k - 1 - r;
+        const double2 g = at(hc, k, pa, qb);
         const double rr = hypot(g.x, g.y);
-        const double app = at(Ht, k, pa, pa).x, aqq = at(Ht, k, qb, qb).x;
+        const double app = at(hc, k, pa, pa).x, aqq = at(hc, k, qb, qb).x;
         double c = 1.0, s = 0.0;
         double2 em = make_double2(1.0, 0.0);
         if (rr > 1e-300 && rr > 1e-18 * sqrt(fabs(app * aqq))) {
-          em = make_double2(g.x / rr, -g.y / rr);  // e^{-i phi}
+          em = make_double2(g.x / rr, -g.y / rr);
           const double tau = (aqq - app) / (2.0 * rr);
           const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
           c = 1.0 / sqrt(1.0 + tt * tt);
           s = tt * c;
         }
-        s_p[r] = pa;
-        s_q[r] = qb;
         s_c[r] = c;
         s_s[r] = s;
         s_e[r] = em;
       }
       __syncthreads();
-      // columns: H <- H J ; Q <- Q J.  J: (p,p)=c (p,q)=s (q,p)=-s e (q,q)=c e, e = e^{-i phi}
+      // Ht <- J^H Ht J on every 2x2 block (rows r', k-1-r'; columns r, k-1-r), shifted
+      for (int e = tid; e < half * half; e += nt) {
+        const int r = e / half, rp = e - r * half;
+        const int p = r, q = k - 1 - r, pp = rp, qq = k - 1 - rp;
+        const double c = s_c[r], s = s_s[r];
+        const double2 em = s_e[r];
+        const double c2 = s_c[rp], s2 = s_s[rp];
+        const double2 ep = cconj(s_e[rp]);
+        const double2 a_pp = at(hc, k, pp, p), a_qp = at(hc, k, qq, p);
+        const double2 a_pq = at(hc, k, pp, q), a_qq = at(hc, k, qq, q);
+        // columns: X = A J
+        const double2 t1 = cmul(a_pq, em), t2 = cmul(a_qq, em);
+        const double2 x_pp = make_double2(c * a_pp.x - s * t1.x, c * a_pp.y - s * t1.y);
+        const double2 x_qp = make_double2(c * a_qp.x - s * t2.x, c * a_qp.y - s * t2.y);
+        const double2 x_pq = make_double2(s * a_pp.x + c * t1.x, s * a_pp.y + c * t1.y);
+        const double2 x_qq = make_double2(s * a_qp.x + c * t2.x, s * a_qp.y + c * t2.y);
+        // rows: B = J'^H X, J'^H (p',p')=c' (p',q')=-s' conj(e') (q',p')=s' (q',q')=c' conj(e')
+        const double2 u1 = cmul(x_qp, ep), u2 = cmul(x_qq, ep);
+        double2 b_pp = make_double2(c2 * x_pp.x - s2 * u1.x, c2 * x_pp.y - s2 * u1.y);
+        double2 b_qp = make_double2(s2 * x_pp.x + c2 * u1.x, s2 * x_pp.y + c2 * u1.y);
+        double2 b_pq = make_double2(c2 * x_pq.x - s2 * u2.x, c2 * x_pq.y - s2 * u2.y);
+        double2 b_qq = make_double2(s2 * x_pq.x + c2 * u2.x, s2 * x_pq.y + c2 * u2.y);
+        if (rp == r) {
+          // diagonal block: the rotated pair is decoupled exactly
+          if (s != 0.0) b_pq = b_qp = make_double2(0.0, 0.0);
+          b_pp.y = 0.0;
+          b_qq.y = 0.0;
+        }
+        const int np_ = shift(p), nq_ = shift(q), npp = shift(pp), nqq = shift(qq);
+        at(hn, k, npp, np_) = b_pp;
+        at(hn, k, nqq, np_) = b_qp;
+        at(hn, k, npp, nq_) = b_pq;
+        at(hn, k, nqq, nq_) = b_qq;
+      }
+      // Q <- Q J, columns shifted
       for (int e = tid; e < half * k; e += nt) {
         const int r = e / k, i = e - r * k;
-        const int pa = s_p[r], qb = s_q[r];
+        const int p = r, q = k - 1 - r;
         const double c = s_c[r], s = s_s[r];
-        if (s == 0.0) continue;
         const double2 em = s_e[r];
-        const double2 hp = at(Ht, k, i, pa), hq = at(Ht, k, i, qb);
-        const double2 hqe = cmul(hq, em);
-        at(Ht, k, i, pa) = make_double2(c * hp.x - s * hqe.x, c * hp.y - s * hqe.y);
-        at(Ht, k, i, qb) = make_double2(s * hp.x + c * hqe.x, s * hp.y + c * hqe.y);
-        const double2 qp = at(Q, k, i, pa), qq = at(Q, k, i, qb);
-        const double2 qqe = cmul(qq, em);
-        at(Q, k, i, pa) = make_double2(c * qp.x - s * qqe.x, c * qp.y - s * qqe.y);
-        at(Q, k, i, qb) = make_double2(s * qp.x + c * qqe.x, s * qp.y + c * qqe.y);
+        const double2 qp = at(qc, k, i, p), qq = cmul(at(qc, k, i, q), em);
+        at(qn, k, i, shift(p)) = make_double2(c * qp.x - s * qq.x, c * qp.y - s * qq.y);
+        at(qn, k, i, shift(q)) = make_double2(s * qp.x + c * qq.x, s * qp.y + c * qq.y);
       }
       __syncthreads();
-      // rows: H <- J^H H.  J^H: (p,p)=c (p,q)=-s conj(e) (q,p)=s (q,q)=c conj(e)
-      for (int e = tid; e < half * k; e += nt) {
-        const int r = e / k, j = e - r * k;
-        const int pa = s_p[r], qb = s_q[r];
-        const double c = s_c[r], s = s_s[r];
-        if (s == 0.0) continue;
-        const double2 ep = cconj(s_e[r]);
-        const double2 hp = at(Ht, k, pa, j), hq = at(Ht, k, qb, j);
-        const double2 hqe = cmul(hq, ep);
-        at(Ht, k, pa, j) = make_double2(c * hp.x - s * hqe.x, c * hp.y - s * hqe.y);
-        at(Ht, k, qb, j) = make_double2(s * hp.x + c * hqe.x, s * hp.y + c * hqe.y);
-      }
-      __syncthreads();
-      for (int r = tid; r < half; r += nt) {
-        if (s_s[r] == 0.0) continue;
-        const int pa = s_p[r], qb = s_q[r];
-        at(Ht, k, pa, qb) = make_double2(0.0, 0.0);
-        at(Ht, k, qb, pa) = make_double2(0.0, 0.0);
-        at(Ht, k, pa, pa).y = 0.0;
-        at(Ht, k, qb, qb).y = 0.0;
-      }
-      __syncthreads();
+      double2* t = hc;
+      hc = hn;
+      hn = t;
+      t = qc;
+      qc = qn;
+      qn = t;
     }
   }
+  if (qc != Q) {
+    // C below is written to the G storage: bring Q home first
+    for (size_t e = tid; e < kk2; e += nt) Q[e] = qc[e];
+    __syncthreads();
+  }
+  stamp(4);
   // (f) sort ascending (rank sort, ties by index)
-  for (int i = tid; i < k; i += nt) lam[i] = at(Ht, k, i, i).x;
+  for (int i = tid; i < k; i += nt) lam[i] = at(hc, k, i, i).x;
   __syncthreads();
   for (int i = tid; i < k; i += nt) {
     const double li = lam[i];
@@ -374,6 +432,7 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     G[e] = s;
   }
   __syncthreads();
+  stamp(5);
   // (h) next window [lam_cut, lam_max] and Chebyshev coefficients
   if (tid == 0) {
     ProbState& S = ps[p];
@@ -388,6 +447,7 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     S.chol_fail = s_flag;
     S.theta_min = th[0];
   }
+  stamp(6);
 }
 
 // ------------------------------------------------- Chebyshev coefficients --
@@ -443,9 +503,11 @@ __global__ void k_coef(const ProbDesc* __restrict__ pd, const ProbState* __restr
 
 // ---------------------------------------------------------------- rotate ---
 // V = W C.  CTA: 128 threads, tile 128 rows x 32 columns; thread: rows ty+16i
-// (i < 8), columns tx+8j (j < 4); W and C staged through shared memory, two
-// stages.
-constexpr int RR = 128, RC = 32, RK = 8;
+// (i < 8), columns tx+8j (j < 4); W and C slabs of RK columns/rows arrive
+// through a three-stage cp.async ring (dynamic shared memory).
+constexpr int RR = 128, RC = 32, RK = 8, RS = 3;
+constexpr int kRotStage = RK * RR + RK * RC;  // double2 per stage
+constexpr int kRotSmem = RS * kRotStage * (int)sizeof(double2);
 
 __global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
                                                 const int* __restrict__ start, int np, const double2* __restrict__ Wp,
@@ -460,46 +522,61 @@ __global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd,
   const int k = d.k;
   const double2* C = KK + d.kk;  // C in G storage, column-major k x k
   const double2* Wb = Wp + d.blk;
-  __shared__ double2 sW[2][RK][RR], sC[2][RK][RC];
+  extern __shared__ double2 rsm[];
   const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
   double2 av[8][4];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) av[i][j] = make_double2(0.0, 0.0);
+  // stage layout: sW[RK][RR] then sC[RK][RC]
   auto load = [&](int q0, int b) {
+    double2* sW = rsm + b * kRotStage;
+    double2* sC = sW + RK * RR;
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const int idx = threadIdx.x + 128 * e;
       const int c = idx >> 7, r = idx & 127;
       const int row = row0 + r;
-      sW[b][c][r] = row < d.dim ? __ldg(Wb + (size_t)(q0 + c) * d.dim + row) : make_double2(0.0, 0.0);
+      const bool ok = row < d.dim;
+      cp_async16(sW + c * RR + r, Wb + (size_t)(q0 + c) * d.dim + (ok ? row : 0), ok);
     }
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const int idx = threadIdx.x + 128 * e;
       const int c = idx & 31, r = idx >> 5;
-      sC[b][r][c] = __ldg(C + (size_t)(col0 + c) * k + q0 + r);
+      cp_async16(sC + r * RC + c, C + (size_t)(col0 + c) * k + q0 + r, true);
     }
+    cp_async_commit();
   };
-  load(0, 0);
-  __syncthreads();
-  for (int q0 = 0, b = 0; q0 < k; q0 += RK, b ^= 1) {
-    if (q0 + RK < k) load(q0 + RK, b ^ 1);
+  const int nstep = k / RK;
+#pragma unroll
+  for (int s = 0; s < RS - 1; ++s) {
+    if (s < nstep) load(s * RK, s);
+    else cp_async_commit();  // keep the group count uniform
+  }
+  for (int it = 0; it < nstep; ++it) {
+    cp_async_wait<RS - 2>();
+    __syncthreads();
+    // refill the slot consumed in the previous step (all threads are past it)
+    if (it + RS - 1 < nstep) load((it + RS - 1) * RK, (it + RS - 1) % RS);
+    else cp_async_commit();
+    const double2* sW = rsm + (it % RS) * kRotStage;
+    const double2* sC = sW + RK * RR;
 #pragma unroll
     for (int q = 0; q < RK; ++q) {
       double2 w[8], c[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) w[i] = sW[b][q][ty + 16 * i];
+      for (int i = 0; i < 8; ++i) w[i] = sW[q * RR + ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) c[j] = sC[b][q][tx + 8 * j];
+      for (int j = 0; j < 4; ++j) c[j] = sC[q * RC + tx + 8 * j];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) cfma(av[i][j], w[i], c[j]);
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int col = col0 + tx + 8 * j;
@@ -659,9 +736,14 @@ __global__ void k_phase_fix(const ProbDesc* __restrict__ pd, const int* __restri
 }
 
 // ------------------------------------------------------------- launchers ---
+int dense_init() {
+  LAPH_CUDA_TRY(cudaFuncSetAttribute(k_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, kGramSmem));
+  LAPH_CUDA_TRY(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, kRotSmem));
+  return LAPH_OK;
+}
 int gram(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int chunk_rows,
          const double2* W, const double2* Y, double2* gpart, cudaStream_t st) {
-  k_gram<<<nblk, 64, 0, st>>>(pd, ps, start, np, chunk_rows, W, Y, gpart);
+  k_gram<<<nblk, 64, kGramSmem, st>>>(pd, ps, start, np, chunk_rows, W, Y, gpart);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }
@@ -672,8 +754,9 @@ int gram_reduce(const ProbDesc* pd, const ProbState* ps, const int* start, int n
   return LAPH_OK;
 }
 int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* theta, double* tcoef, double* scol,
-                double* dwork, int first_iter, int fixed_cut, int max_sweeps, cudaStream_t st) {
-  k_small<<<np, 1024, 0, st>>>(pd, ps, KK, theta, tcoef, scol, dwork, first_iter, fixed_cut, max_sweeps);
+                double* dwork, int first_iter, int fixed_cut, int max_sweeps, unsigned long long* tstamp,
+                cudaStream_t st) {
+  k_small<<<np, 1024, 0, st>>>(pd, ps, KK, theta, tcoef, scol, dwork, first_iter, fixed_cut, max_sweeps, tstamp);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }
@@ -685,7 +768,7 @@ int coef(const ProbDesc* pd, const ProbState* ps, int np, const double* theta, d
 }
 int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* W,
            const double2* KK, double2* V, cudaStream_t st) {
-  k_rotate<<<nblk, 128, 0, st>>>(pd, ps, start, np, W, KK, V);
+  k_rotate<<<nblk, 128, kRotSmem, st>>>(pd, ps, start, np, W, KK, V);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

@@ -5,12 +5,18 @@
 namespace laph {
 constexpr int kGramTile = 32;   // block widths k are multiples of this
 constexpr int kRotRows = 128;   // rows per rotation tile
+// Opt the dense kernels into their dynamic shared memory on the current device.
+int dense_init();
 int gram(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int chunk_rows,
          const double2* W, const double2* Y, double2* gpart, cudaStream_t st);
 int gram_reduce(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* gpart,
                 double2* KK, cudaStream_t st);
+// Per problem: scaling, Cholesky, inverse, projected matrix, Jacobi, sort, C, next window.
+// tstamp[p][0..kSmallPhases-1] receives the global timer (ns) at the phase boundaries.
+constexpr int kSmallPhases = 7;
 int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* theta, double* tcoef, double* scol,
-                double* dwork, int first_iter, int fixed_cut, int max_sweeps, cudaStream_t st);
+                double* dwork, int first_iter, int fixed_cut, int max_sweeps, unsigned long long* tstamp,
+                cudaStream_t st);
 // Chebyshev coefficient table and S scaling for a filter of degree m.
 int coef(const ProbDesc* pd, const ProbState* ps, int np, const double* theta, double* tcoef, double* scol, int m,
          cudaStream_t st);

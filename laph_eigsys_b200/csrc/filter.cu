@@ -194,6 +194,151 @@ __global__ void __launch_bounds__(128, 3)
   }
 }
 
+// Variant of the same step for column blocks kb <= kCoefMax (the default): the
+// CTA first converts this step's coefficients of its columns to FP32
+// (a c_hop, a c_diag, z, g) in shared memory, so the column loop reads one
+// broadcast float4 instead of three FP64 loads and four conversions per
+// thread.  (Software-pipelining the loop over column pairs, with the 27
+// vector values of column j+1 in flight while column j is computed, needs
+// ~250 registers, halves residency to 2 CTAs per SM and measured no faster.)
+constexpr int kCoefMax = 64;
+struct ChebCol {
+  float2 xu[3][3], xd[3][3], xs[3], ss[3], zz[3];
+};
+
+template <typename LT, bool HAS_Z, bool FINAL>
+__global__ void __launch_bounds__(128, 3)
+    k_cheb_mrhs2(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, const int* __restrict__ start,
+                 int np, int kb, const LT* __restrict__ links, const float* __restrict__ scale,
+                 const float2* __restrict__ Xp, const float2* __restrict__ Zp, const float2* __restrict__ Sp,
+                 float2* __restrict__ Yp, const double2* __restrict__ Vp, double2* __restrict__ Wp,
+                 const double* __restrict__ tcoef, int step) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int nst = (d.V3 + 127) >> 7;
+  const int t = blockIdx.x - start[p];
+  const int st = t % nst, cb = t / nst;
+  const int s = st * 128 + threadIdx.x;
+  const bool valid = s < d.V3;
+  const int j1 = min(cb * kb + kb, d.k);
+  const int nlock = ps[p].nlock;
+  if (FINAL && valid) {
+    for (int j = cb * kb; j < min(j1, nlock); ++j) {
+      const size_t i = (size_t)d.blk + (size_t)j * d.dim + 3 * (size_t)s;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) Wp[i + a] = __ldg(Vp + i + a);
+    }
+  }
+  const int j0 = max(cb * kb, nlock);
+  if (j0 >= j1) return;  // uniform over the CTA
+  __shared__ float4 cf[kCoefMax];
+  __shared__ double ctm[kCoefMax];
+  {
+    const double c_hop = ps[p].c_hop, c_diag = ps[p].c_diag;
+    const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
+    for (int j = j0 + (int)threadIdx.x; j < j1; j += 128) {
+      const double a = tc[j];
+      cf[j - j0] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
+      if (FINAL) ctm[j - j0] = tc[(size_t)3 * d.k + j];
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+  const Lat g{d.L, d.L * d.L, d.V3};
+  int sx, sy, sz;
+  site_xyz(g, s, sx, sy, sz);
+  int up[3], dn[3];
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu) {
+    up[mu] = nb_up(g, sx, sy, sz, mu);
+    dn[mu] = nb_dn(g, sx, sy, sz, mu);
+  }
+  const LT* U = links + d.uf;
+  const float* scl = scale + d.sc;
+  float2 uf[3][9], ub[3][9];
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu)
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      uf[mu][e] = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + s, s);
+      ub[mu][e] = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + dn[mu], dn[mu]);
+    }
+  const size_t base = (size_t)d.blk;
+  const int s0 = st * 128, nsite = min(128, d.V3 - s0);
+  const bool pf = threadIdx.x == 0 && (nsite % 2 == 0) && (d.dim % 2 == 0);
+  auto prefetch = [&](int j) {
+    if (!pf || j >= j1) return;
+    const size_t col = base + (size_t)j * d.dim;
+    const unsigned bytes = 8u * nsite;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      l2_prefetch(Xp + col + (size_t)c * d.V3 + s0, bytes);
+      l2_prefetch(Sp + col + (size_t)c * d.V3 + s0, bytes);
+      if (HAS_Z) l2_prefetch(Zp + col + (size_t)c * d.V3 + s0, bytes);
+    }
+    if (FINAL) l2_prefetch(Vp + col + 3 * (size_t)s0, 6 * bytes);
+  };
+  auto fetch = [&](int j, ChebCol& c) {
+    const size_t col = base + (size_t)j * d.dim;
+    const float2* x = Xp + col;
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        c.xu[mu][b] = __ldg(x + (size_t)b * d.V3 + up[mu]);
+        c.xd[mu][b] = __ldg(x + (size_t)b * d.V3 + dn[mu]);
+      }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      c.xs[a] = __ldg(x + (size_t)a * d.V3 + s);
+      c.ss[a] = __ldg(Sp + col + (size_t)a * d.V3 + s);
+      if (HAS_Z) c.zz[a] = __ldg(Zp + col + (size_t)a * d.V3 + s);
+    }
+  };
+  auto compute = [&](int j, const ChebCol& c) {
+    float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu)
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          cfmaf(acc[a], uf[mu][3 * a + b], c.xu[mu][b]);
+          cfmacf(acc[a], ub[mu][3 * b + a], c.xd[mu][b]);
+        }
+    const float4 q = cf[j - j0];  // (a c_hop, a c_diag, z, g)
+    const size_t col = base + (size_t)j * d.dim;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float2 r;
+      r.x = fmaf(q.x, acc[a].x, fmaf(q.y, c.xs[a].x, q.w * c.ss[a].x));
+      r.y = fmaf(q.x, acc[a].y, fmaf(q.y, c.xs[a].y, q.w * c.ss[a].y));
+      if (HAS_Z) {
+        r.x = fmaf(q.z, c.zz[a].x, r.x);
+        r.y = fmaf(q.z, c.zz[a].y, r.y);
+      }
+      if (FINAL) {
+        const size_t iv = col + 3 * (size_t)s + a;
+        const double2 v = __ldg(Vp + iv);
+        const double tm = ctm[j - j0];
+        Wp[iv] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
+      } else {
+        Yp[col + (size_t)a * d.V3 + s] = r;
+      }
+    }
+  };
+#pragma unroll 1
+  for (int j = j0; j < min(j1, j0 + kPrefetch); ++j) prefetch(j);
+  ChebCol A;
+#pragma unroll 1
+  for (int j = j0; j < j1; ++j) {
+    prefetch(j + kPrefetch);
+    fetch(j, A);
+    compute(j, A);
+  }
+}
+
 // ------------------------------------------------ FP64 block stencil: A W --
 // Y_j = (-Delta) W_j = 6 W_j - hop(W_j), FP64, one thread per (site, column).
 __global__ void __launch_bounds__(128) k_neglap64_batch(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
@@ -271,11 +416,31 @@ int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const dou
 
 int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
               const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
-              const double2* V, double2* W, const double* tcoef, int step, bool final_step, cudaStream_t st) {
+              const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant,
+              cudaStream_t st) {
+  const bool hz = Z != nullptr;
+  if (variant == 1 && kb <= kCoefMax) {
+#define LAPH_CHEB2(LT, HZ, FIN)                                                                             \
+  k_cheb_mrhs2<LT, HZ, FIN><<<nblk, 128, 0, st>>>(pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), \
+                                                  scale, X, Z, S, Y, V, W, tcoef, step)
+    if (bf16) {
+      if (hz && final_step) LAPH_CHEB2(__nv_bfloat162, true, true);
+      else if (hz) LAPH_CHEB2(__nv_bfloat162, true, false);
+      else if (final_step) LAPH_CHEB2(__nv_bfloat162, false, true);
+      else LAPH_CHEB2(__nv_bfloat162, false, false);
+    } else {
+      if (hz && final_step) LAPH_CHEB2(float2, true, true);
+      else if (hz) LAPH_CHEB2(float2, true, false);
+      else if (final_step) LAPH_CHEB2(float2, false, true);
+      else LAPH_CHEB2(float2, false, false);
+    }
+#undef LAPH_CHEB2
+    LAPH_CUDA_TRY(cudaGetLastError());
+    return LAPH_OK;
+  }
 #define LAPH_CHEB(LT, HZ, FIN)                                                                                  \
   k_cheb_mrhs<LT, HZ, FIN><<<nblk, 128, 0, st>>>(pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), scale, \
                                                  X, Z, S, Y, V, W, tcoef, step)
-  const bool hz = Z != nullptr;
   if (bf16) {
     if (hz && final_step) LAPH_CHEB(__nv_bfloat162, true, true);
     else if (hz) LAPH_CHEB(__nv_bfloat162, true, false);

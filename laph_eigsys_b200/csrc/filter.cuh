@@ -8,10 +8,12 @@ int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const dou
                float* scale, int bf16, cudaStream_t st);
 // One Chebyshev step Y_j = a_j (c_hop hop(X_j) + c_diag X_j) + z_j Z_j + g_j S_j (FP32)
 // with (a, z, g) = tcoef[step][0..2][j]; final_step writes W_j = tcoef[step+1][0][j] V_j + Y_j
-// in FP64 instead of Y.
+// in FP64 instead of Y.  variant 0: per-thread FP64 coefficients; 1: FP32 coefficients
+// staged in shared memory (kb <= 64; larger blocks take variant 0).
 int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
               const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
-              const double2* V, double2* W, const double* tcoef, int step, bool final_step, cudaStream_t st);
+              const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant,
+              cudaStream_t st);
 // Y = (-Delta) W for every column, FP64.
 int neglap64_batch(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
                    const double2* W, double2* Y, cudaStream_t st);

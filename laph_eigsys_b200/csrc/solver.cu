@@ -24,6 +24,8 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -62,6 +64,7 @@ struct laph_solver {
          *phases = nullptr, *norms = nullptr;
   int* d_nactive = nullptr;
   int* h_nactive = nullptr;
+  unsigned long long* tstamp = nullptr;  // [np][kSmallPhases] phase boundaries of the small dense step
   size_t blk_total = 0;
   std::vector<int> links_set;
   std::vector<int> degs;  // filter degree of each pass of the last run
@@ -115,13 +118,14 @@ void laph_solve_opts_default(laph_solve_opts* o) {
   std::memset(o, 0, sizeof *o);
   o->smear_kind = LAPH_SMEAR_NONE;
   o->guard = 16;
-  o->link_prec = LAPH_LINKS_BF16;
+  o->link_prec = LAPH_LINKS_FP32;
   o->tol = 1e-9;
   o->max_it = 200;
   o->window = LAPH_WINDOW_LANCZOS;
   o->deg = 16;
   o->phase_fix = 1;
   o->seed = 1227;
+  o->filter_kernel = 1;
 }
 
 int laph_solver_destroy(laph_solver* s) {
@@ -131,7 +135,8 @@ int laph_solver_destroy(laph_solver* s) {
   void* ptrs[] = {s->d_pd, s->d_ps, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
                   s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
-                  s->phases, s->norms, s->d_nactive, s->model, s->feats, s->mwork, s->bound, s->plaq, s->wdeg};
+                  s->phases, s->norms, s->d_nactive, s->model, s->feats, s->mwork, s->bound, s->plaq, s->wdeg,
+                  s->tstamp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->h_nactive) cudaFreeHost(s->h_nactive);
@@ -186,6 +191,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     set_error("laph_solver_create: cannot use device %d", device);
     return fail(LAPH_ECUDA);
   }
+  if (int e = dense_init()) return fail(e);
   // descriptors and pool offsets
   long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
   size_t max_run = 0, max_v3 = 0;
@@ -251,7 +257,8 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
       (rc = dalloc(&s->resid, o_kv)) || (rc = dalloc(&s->phases, o_kv)) || (rc = dalloc(&s->norms, o_kv)) ||
       (rc = dalloc(&s->d_nactive, 1)) || (rc = dalloc(&s->model, kMlpParams + kMlpNorm)) ||
       (rc = dalloc(&s->feats, (size_t)n * kMlpIn)) || (rc = dalloc(&s->mwork, (size_t)n * (kMlpIn + kMlpOut))) ||
-      (rc = dalloc(&s->bound, n)) || (rc = dalloc(&s->plaq, 4 * (size_t)n)) || (rc = dalloc(&s->wdeg, n)))
+      (rc = dalloc(&s->bound, n)) || (rc = dalloc(&s->plaq, 4 * (size_t)n)) || (rc = dalloc(&s->wdeg, n)) ||
+      (rc = dalloc(&s->tstamp, (size_t)n * kSmallPhases)))
     return fail(rc);
   if (opts->link_prec == LAPH_LINKS_BF16) {
     if ((rc = dalloc(reinterpret_cast<float2**>(&s->Ubf), (size_t)o_uf))) return fail(rc);  // 4 B per element
@@ -317,7 +324,7 @@ static int iteration_rr(laph_solver* s, int first_iter) {
   LAPH_TRY(gram(s->d_pd, s->d_ps, s->st_gram, s->np, s->nb_gram, 8192, s->W, s->Y, s->gpart, s->st));
   LAPH_TRY(gram_reduce(s->d_pd, s->d_ps, s->st_gred, s->np, s->nb_gred, s->gpart, s->KK, s->st));
   LAPH_TRY(small_dense(s->d_pd, s->d_ps, s->np, s->KK, s->theta, s->tcoef, s->scol, s->dwork, first_iter, fixed ? 1 : 0,
-                       s->o.jacobi_sweeps > 0 ? s->o.jacobi_sweeps : 2, s->st));
+                       s->o.jacobi_sweeps > 0 ? s->o.jacobi_sweeps : 2, s->tstamp, s->st));
   LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->KK, s->V, s->st));
   LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
   LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
@@ -335,7 +342,7 @@ static int filter(laph_solver* s, int m) {
     const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
     float2* Yo = s->E[(n - 1) % 3];
     LAPH_TRY(cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo,
-                       s->V, s->W, s->tcoef, n, fin, s->st));
+                       s->V, s->W, s->tcoef, n, fin, s->o.filter_kernel, s->st));
   }
   return LAPH_OK;
 }
@@ -458,11 +465,46 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     cudaEventCreate(&s->evf[0]);
     cudaEventCreate(&s->evf[1]);
   }
+  const char* tr_env = std::getenv("LAPH_TRACE");
+  const bool trace = tr_env && *tr_env && *tr_env != '0';
+  if (trace) LAPH_CUDA_TRY(cudaMemsetAsync(s->tstamp, 0, (size_t)s->np * kSmallPhases * sizeof(unsigned long long), s->st));
   int it = 1;
   for (; it < o.max_it; ++it) {
     LAPH_CUDA_TRY(cudaMemcpyAsync(s->h_nactive, s->d_nactive, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     LAPH_CUDA_TRY(cudaMemcpyAsync(s->hps.data(), s->d_ps, s->np * sizeof(ProbState), cudaMemcpyDeviceToHost, s->st));
     LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+    if (trace) {
+      // LAPH_TRACE=1: one line per outer iteration with the batch's state after the last Rayleigh-Ritz
+      long long nl = 0, nk = 0, nc = 0, nv = 0;
+      double mr = 0.0;
+      for (int i = 0; i < s->np; ++i) {
+        nl += s->hps[i].nlock;
+        nk += s->hd[i].k;
+        nc += s->hps[i].nconv;
+        nv += s->hd[i].nev;
+        if (s->hps[i].active) mr = std::max(mr, s->hps[i].max_resid);
+      }
+      std::fprintf(stderr, "laph_trace it %d active %d locked %lld/%lld converged %lld/%lld max_resid %.3e\n", it,
+                   *s->h_nactive, nl, nk, nc, nv, mr);
+      // mean duration of the phases of the last small dense step over the problems that ran it
+      std::vector<unsigned long long> ts((size_t)s->np * kSmallPhases);
+      if (cudaMemcpy(ts.data(), s->tstamp, ts.size() * sizeof(ts[0]), cudaMemcpyDeviceToHost) == cudaSuccess) {
+        double ph[kSmallPhases - 1] = {0};
+        int cnt = 0;
+        for (int i = 0; i < s->np; ++i) {
+          const unsigned long long* t = &ts[(size_t)i * kSmallPhases];
+          if (t[0] == 0 || t[kSmallPhases - 1] < t[0]) continue;
+          ++cnt;
+          for (int q = 0; q + 1 < kSmallPhases; ++q) ph[q] += 1e-3 * (double)(t[q + 1] - t[q]);
+        }
+        cudaMemset(s->tstamp, 0, ts.size() * sizeof(ts[0]));
+        if (cnt)
+          std::fprintf(stderr,
+                       "laph_trace it %d small dense us: cholesky %.0f inverse %.0f project %.0f jacobi %.0f "
+                       "sort+C %.0f window %.0f\n",
+                       it, ph[0] / cnt, ph[1] / cnt, ph[2] / cnt, ph[3] / cnt, ph[4] / cnt, ph[5] / cnt);
+      }
+    }
     if (*s->h_nactive == 0) break;
     // Degree of this pass.  While the Ritz vectors are still poor (largest
     // wanted residual > 1e-2) the amplification of the filter is capped at
@@ -483,6 +525,7 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
       if (s->hps[i].active) s->cnt[0] += (long long)s->hd[i].V3 * (s->hd[i].k - s->hps[i].nlock) * (m - 1);
     s->cnt[1] += m - 1;
     s->degs.push_back(m);
+    if (trace) std::fprintf(stderr, "laph_trace it %d filter degree %d\n", it, m);
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[0], s->st));
     LAPH_TRY(filter_graph(s, m));
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[1], s->st));

@@ -103,3 +103,21 @@ def test_same_solver_runs_twice(gpu):
     b = s.get(0)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     s.close()
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("L,nev,prec", [(6, 20, "fp32"), (8, 40, "bf16")])
+def test_filter_variants_match_dense(gpu, orc, variant, L, nev, prec):
+    """Both filter variants (per-thread FP64 coefficients, FP32 coefficients staged per CTA) converge to
+    the dense eigenpairs; L = 6 leaves the last site tile partly empty."""
+    U = random_links(L, 0.4, 4000 + L)
+    tol = 1e-10
+    s = gpu.Solver([(L, nev)], guard=16, tol=tol, deg=10, max_it=300, filter_kernel=variant,
+                   link_prec=gpu.LINKS_BF16 if prec == "bf16" else gpu.LINKS_FP32)
+    s.set_links(0, U)
+    st, res = s.run()
+    assert st == 0, res
+    ev, V, ph = s.get(0)
+    A, w, X = dense_ref(orc, U, L)
+    check_solution(A, w, X, ev, V, ph, nev, tol)
+    s.close()
