@@ -262,6 +262,56 @@ def workload_config(cfg):
             "l2": "inputs larger than L2 (each 64-timeslice block of vectors is 8 GB)"}
 
 
+def sourceshape_flops(L, nev):
+    """FP64 flops of the source-shape kernel: per parity class the upper 32-site tile pairs of V_c V_c^dag,
+    9 nev complex FMAs per site pair."""
+    nc = (L // 2) ** 3
+    t = (nc + 31) // 32
+    return 8 * (t * (t + 1) // 2) * 32 * 32 * 9 * nev * 8.0
+
+
+def measure_sourceshape(solver, stream, batch, no_cpu, reps=4):
+    """psi(r) of the first solved timeslices in place on the device (CUDA events on the solver's stream), and the
+    oracle's restatement on one 16^3 eigensystem beside the device kernel on the same input."""
+    import torch
+    import laph_eigsys_b200 as lb
+    L, nev, _ = batch[0]
+    n = min(reps, len(batch))
+    solver.sourceshape(0)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(n):
+        solver.sourceshape(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    fl = sourceshape_flops(L, nev)
+    out = {"workload": f"psi(r) of {L}^3 x nev {nev}, (L/2)^3 = {(L // 2) ** 3} displacements, FP64",
+           "ms_per_timeslice": ms, "tflops": fl / (ms / 1e3) / 1e12, "bound": "fp64",
+           "fp64_peak_tflops": 33.5, "peak_source": "FP64 FMA loop measured on this pool's B200",
+           "frac": fl / (ms / 1e3) / 1e12 / 33.5, "timeslices": n}
+    if not no_cpu:
+        import oracle as orc
+        Ls, nevs = 16, min(nev, 120)
+        rng = np.random.default_rng(16)
+        V, _ = np.linalg.qr(rng.normal(size=(3 * Ls ** 3, nevs)) + 1j * rng.normal(size=(3 * Ls ** 3, nevs)))
+        V = np.asfortranarray(V)
+        orc.set_threads(os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        ref = orc.sourceshape(V, Ls)
+        cpu_s = time.perf_counter() - t0
+        lb.sourceshape(V, Ls)
+        t1 = time.perf_counter()
+        got = lb.sourceshape(V, Ls)
+        gpu_s = time.perf_counter() - t1
+        out["cpu_sample"] = {"workload": f"16^3 x nev {nevs} (random orthonormal block)", "cpu_seconds": cpu_s,
+                             "cores": os.cpu_count() or 1, "kind": "port",
+                             "gpu_seconds_host_api": gpu_s,
+                             "max_rel_diff": float(np.abs(got - ref).max() / np.abs(ref).max())}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -281,6 +331,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-shape", action="store_true")
     ap.add_argument("--plain-timeslices", type=int, default=2)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -423,6 +474,11 @@ def main():
         plain = plain_gpu(cfg, batch, float(1.1 * (-ev0)[-1]), args.plain_timeslices, local)
         plain["chosen_over_plain"] = value / plain["value"] if plain.get("value") else None
 
+    # ---- source shape of the solved eigenvectors (next row of the path) ------
+    shape = None
+    if rank == 0 and world == 1 and not args.no_shape and all(L_ % 2 == 0 for L_, _, _ in batch):
+        shape = measure_sourceshape(solver, stream, batch, args.no_cpu)
+
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -442,6 +498,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
                 "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "sourceshape": shape,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid, "filter_ms_per_step": filt_ms / args.steps,
                            "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
                                                        solver.timings()))}}

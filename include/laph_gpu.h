@@ -229,6 +229,29 @@ int laph_solver_features(laph_solver* s, float* feats, double* bound);
 /* All k Ritz values of problem i after the last run (k returned). */
 int laph_solver_ritz(laph_solver* s, int i, double* theta, int* k);
 
+/* ---- source shape (the reference's sourceshape program) ------------------
+ * psi(r) = sum_x || V_{x+r} V_x^dag ||_F over the grid r_i = 0, 2, ..., L-2,
+ * V_y the 3 x nev block of rows 3y .. 3y+2 of the eigensystem: replaces
+ * source_shape_complete / dll_op (modules/sourceshape_funcs.cpp:30-81).
+ * psi[(L/2)^3] (host) in the reference's order (r1 = x outer, r3 = z inner).
+ * FP64 on the device; even L only.  evals (may be NULL): weight column n by
+ * sqrt|evals[n]| first (weight_eigenvectors, sourceshape_funcs.cpp:85-96).
+ * laph_sourceshape takes a column-major complex128 eigensystem [3 V3][nev]
+ * in host (on_device = 0) or device memory; laph_solver_sourceshape works on
+ * problem i of a solver that has run, in place on the device (weighted != 0:
+ * by sqrt of its eigenvalues). */
+int laph_sourceshape(const double* V, int L, int nev, const double* evals, int on_device, double* psi, int device);
+int laph_solver_sourceshape(laph_solver* s, int i, int weighted, double* psi);
+/* avg_radii (sourceshape_funcs.cpp:100-135): psi averaged over grid points of
+ * equal |r| (to 1e-11), radii in order of first appearance; r_out / psi_out
+ * hold up to (L/2)^3 entries, *n_out gets the count. */
+int laph_sourceshape_avg(int L, const double* psi, double* r_out, double* psi_out, int* n_out);
+/* write_sourceshape_ascii / _bin (modules/read_write.cpp:205-234):
+ * "<dir>/sourceshape_nev<nev>.<config>.<t>" ("#r\tpsi(r)" then "r psi" with 12
+ * significant digits) and "<dir>/sourceshape_nev<nev>.%04d.%03d.bin" ((r, psi)
+ * double pairs); dir NULL or "" is the working directory, as in the reference. */
+int laph_write_sourceshape(const char* dir, int config, int t, int nev, int n, const double* r, const double* psi);
+
 /* ---- host-side utilities (no device needed) ------------------------------ */
 /* Seeded synthetic gauge field U = exp(i eps H), H = sum_a c_a lambda_a with
  * c_a ~ N(0,1) i.i.d. (Gell-Mann basis), for all 4 directions; output in the
@@ -239,6 +262,17 @@ int laph_gauge_random(double* conf, int L, int nt, double eps, uint64_t seed);
  * The writer emits ildg-format + ildg-binary-data records (big-endian FP64). */
 int laph_lime_write_gauge(const char* path, const double* conf, int L, int T);
 int laph_lime_read_gauge(const char* path, int T, int L, int t_i, int t_f, double* conf);
+/* Beyond the reference, whose reader stops at single-precision files
+ * (modules/io.cpp:72-79): laph_lime_read_gauge_any reads FP64 or FP32 ILDG
+ * binary data (FP32 widened to FP64), telling them apart by the record size
+ * and, when an ildg-format record precedes the data, checking its <precision>
+ * (LAPH_ESIZE on a mismatch); *precision (may be NULL) receives 32 or 64.
+ * laph_lime_info parses the ildg-format XML record (lx, ly, lz, lt,
+ * precision) and checks it against the size of the binary record.
+ * laph_lime_write_gauge_prec writes either precision (the plain writer is 64). */
+int laph_lime_read_gauge_any(const char* path, int T, int L, int t_i, int t_f, double* conf, int* precision);
+int laph_lime_info(const char* path, int* lx, int* ly, int* lz, int* lt, int* precision);
+int laph_lime_write_gauge_prec(const char* path, const double* conf, int L, int T, int precision);
 /* write_eig_sys_bin / write_eigenvalues_bin (modules/read_write.cpp:176-250):
  * "<dir>/<prefix>.%04d.%03d".  The eigenvector writer runs check_trace first
  * and returns LAPH_ETRACE (nothing written) where the reference exits. */

@@ -15,7 +15,7 @@ from ._lib import (LAYOUT_CONF, LAYOUT_EIGEN, LAYOUT_ROWMAJOR, LINKS_BF16, LINKS
                    SMEAR_NONE, SMEAR_STOUT, WINDOW_FIXED, WINDOW_LANCZOS, WINDOW_MLP, LaphError, check, lib)
 
 __all__ = ["Context", "Solver", "gauge_random", "lime_write_gauge", "lime_read_gauge", "parse_parameters",
-           "check_trace", "fix_phase", "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin",
+           "lime_read_gauge_any", "lime_info", "sourceshape", "sourceshape_avg", "write_sourceshape", "check_trace", "fix_phase", "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin",
            "read_eigsys_bin", "read_eigenvalues_bin", "LaphError", "lib"]
 
 
@@ -35,15 +35,59 @@ def gauge_random(L, nt, eps, seed):
     return conf
 
 
-def lime_write_gauge(path, conf, L, T):
+def lime_write_gauge(path, conf, L, T, precision=64):
     conf = _c128(conf)
-    check(lib.laph_lime_write_gauge(str(path).encode(), _ptr(conf), L, T), "laph_lime_write_gauge")
+    check(lib.laph_lime_write_gauge_prec(str(path).encode(), _ptr(conf), L, T, precision),
+          "laph_lime_write_gauge_prec")
 
 
 def lime_read_gauge(path, T, L, t_i, t_f):
     conf = np.empty((t_f - t_i + 1, L ** 3, 4, 3, 3), dtype=np.complex128)
     check(lib.laph_lime_read_gauge(str(path).encode(), T, L, t_i, t_f, _ptr(conf)), "laph_lime_read_gauge")
     return conf
+
+
+def lime_read_gauge_any(path, T, L, t_i, t_f):
+    """FP64 or FP32 ILDG links (FP32 widened); returns (conf, precision)."""
+    conf = np.empty((t_f - t_i + 1, L ** 3, 4, 3, 3), dtype=np.complex128)
+    prec = ctypes.c_int()
+    check(lib.laph_lime_read_gauge_any(str(path).encode(), T, L, t_i, t_f, _ptr(conf), ctypes.byref(prec)),
+          "laph_lime_read_gauge_any")
+    return conf, prec.value
+
+
+def lime_info(path):
+    """(lx, ly, lz, lt, precision) from the ildg-format record."""
+    v = [ctypes.c_int() for _ in range(5)]
+    check(lib.laph_lime_info(str(path).encode(), *[ctypes.byref(x) for x in v]), "laph_lime_info")
+    return tuple(x.value for x in v)
+
+
+def sourceshape(V, L, evals=None, device=0):
+    """psi(r) of an eigensystem V [3 V3][nev] on the grid r_i = 0, 2, ... < L (device kernel)."""
+    V = np.asfortranarray(V, dtype=np.complex128)
+    psi = np.empty((L // 2) ** 3)
+    ev = None if evals is None else np.ascontiguousarray(evals, dtype=np.float64)
+    check(lib.laph_sourceshape(ctypes.c_void_p(V.ctypes.data), L, V.shape[1],
+                               None if ev is None else _ptr(ev), 0, _ptr(psi), device), "laph_sourceshape")
+    return psi
+
+
+def sourceshape_avg(L, psi):
+    """avg_radii: (radii, averaged psi) in order of first appearance."""
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    r = np.empty(len(psi))
+    a = np.empty(len(psi))
+    n = ctypes.c_int()
+    check(lib.laph_sourceshape_avg(L, _ptr(psi), _ptr(r), _ptr(a), ctypes.byref(n)), "laph_sourceshape_avg")
+    return r[:n.value], a[:n.value]
+
+
+def write_sourceshape(dirname, config, t, nev, r, psi):
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    check(lib.laph_write_sourceshape(str(dirname).encode() if dirname else None, config, t, nev, len(r), _ptr(r),
+                                     _ptr(psi)), "laph_write_sourceshape")
 
 
 def spatial_links(conf_ts):
@@ -277,6 +321,13 @@ class Solver:
         t = (ctypes.c_double * 4)()
         check(lib.laph_solver_timings(self._h, t), "laph_solver_timings")
         return list(t)
+
+    def sourceshape(self, i, weighted=False):
+        """psi(r) of problem i's eigenvectors, computed on the device from the solver's own block."""
+        L = self.problems[i][0]
+        psi = np.empty((L // 2) ** 3)
+        check(lib.laph_solver_sourceshape(self._h, i, int(bool(weighted)), _ptr(psi)), "laph_solver_sourceshape")
+        return psi
 
     def counters(self):
         c = (ctypes.c_longlong * 3)()

@@ -100,6 +100,13 @@ _sig("laph_solver_counters", c_int, c_void_p, P(c_ll))
 _sig("laph_gauge_random", c_int, c_void_p, c_int, c_int, c_double, c_u64)
 _sig("laph_lime_write_gauge", c_int, c_char_p, c_void_p, c_int, c_int)
 _sig("laph_lime_read_gauge", c_int, c_char_p, c_int, c_int, c_int, c_int, c_void_p)
+_sig("laph_lime_read_gauge_any", c_int, c_char_p, c_int, c_int, c_int, c_int, c_void_p, P(c_int))
+_sig("laph_lime_info", c_int, c_char_p, P(c_int), P(c_int), P(c_int), P(c_int), P(c_int))
+_sig("laph_lime_write_gauge_prec", c_int, c_char_p, c_void_p, c_int, c_int, c_int)
+_sig("laph_sourceshape", c_int, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int)
+_sig("laph_solver_sourceshape", c_int, c_void_p, c_int, c_int, c_void_p)
+_sig("laph_sourceshape_avg", c_int, c_int, c_void_p, c_void_p, c_void_p, P(c_int))
+_sig("laph_write_sourceshape", c_int, c_char_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p)
 _sig("laph_write_eigsys_bin", c_int, c_char_p, c_char_p, c_int, c_int, c_int, c_int, c_void_p)
 _sig("laph_write_eigenvalues_bin", c_int, c_char_p, c_char_p, c_int, c_int, c_int, c_void_p)
 _sig("laph_read_eigsys_bin", c_int, c_char_p, c_char_p, c_int, c_int, c_int, c_int, c_void_p)

@@ -196,7 +196,11 @@ int laph_gauge_random(double* conf, int L, int nt, double eps, uint64_t seed) {
   return LAPH_OK;
 }
 
-int laph_lime_write_gauge(const char* path, const double* conf, int L, int T) {
+int laph_lime_write_gauge_prec(const char* path, const double* conf, int L, int T, int precision) {
+  if (!path || !conf || L < 1 || T < 1 || (precision != 32 && precision != 64)) {
+    set_error("laph_lime_write_gauge_prec: bad argument (precision must be 32 or 64)");
+    return LAPH_EINVAL;
+  }
   FILE* f = std::fopen(path, "wb");
   if (!f) {
     set_error("cannot open %s for writing", path);
@@ -207,9 +211,9 @@ int laph_lime_write_gauge(const char* path, const double* conf, int L, int T) {
                 "<?xml version=\"1.0\" encoding=\"UTF-8\"?>\n<ildgFormat xmlns=\"http://www.lqcd.org/ildg\" "
                 "xmlns:xsi=\"http://www.w3.org/2001/XMLSchema-instance\" "
                 "xsi:schemaLocation=\"http://www.lqcd.org/ildg http://www.lqcd.org/ildg/filefmt.xsd\">\n"
-                "  <version>1.0</version>\n  <field>su3gauge</field>\n  <precision>64</precision>\n"
+                "  <version>1.0</version>\n  <field>su3gauge</field>\n  <precision>%d</precision>\n"
                 "  <lx>%d</lx>\n  <ly>%d</ly>\n  <lz>%d</lz>\n  <lt>%d</lt>\n</ildgFormat>\n",
-                L, L, L, T);
+                precision, L, L, L, T);
   const uint64_t xl = std::strlen(xml);
   unsigned char h[144];
   static const unsigned char pad[8] = {0};
@@ -217,10 +221,11 @@ int laph_lime_write_gauge(const char* path, const double* conf, int L, int T) {
   bool ok = std::fwrite(h, 1, 144, f) == 144 && std::fwrite(xml, 1, xl, f) == xl;
   if (ok && xl % 8) ok = std::fwrite(pad, 1, 8 - xl % 8, f) == 8 - xl % 8;
   const long long V3 = (long long)L * L * L;
-  const uint64_t dl = (uint64_t)V3 * T * 72ull * 8ull;
+  const int es = precision / 8;
+  const uint64_t dl = (uint64_t)V3 * T * 72ull * es;
   lime_header(h, false, true, dl, "ildg-binary-data");
   ok = ok && std::fwrite(h, 1, 144, f) == 144;
-  std::vector<unsigned char> buf((size_t)L * 72 * 8);
+  std::vector<unsigned char> buf((size_t)L * 72 * es);
   static const int slot_of_mu[4] = {1, 2, 3, 0};  // ILDG mu order x,y,z,t
   for (int t = 0; ok && t < T; ++t)
     for (int z = 0; ok && z < L; ++z)
@@ -229,9 +234,17 @@ int laph_lime_write_gauge(const char* path, const double* conf, int L, int T) {
           const double* site = conf + ((long long)t * V3 + (long long)x * L * L + (long long)y * L + z) * 72;
           for (int mu = 0; mu < 4; ++mu)
             for (int k = 0; k < 18; ++k) {
-              uint64_t v;
-              std::memcpy(&v, &site[slot_of_mu[mu] * 18 + k], 8);
-              put_be64(&buf[((size_t)x * 72 + mu * 18 + k) * 8], v);
+              unsigned char* o = &buf[((size_t)x * 72 + mu * 18 + k) * es];
+              if (es == 8) {
+                uint64_t v;
+                std::memcpy(&v, &site[slot_of_mu[mu] * 18 + k], 8);
+                put_be64(o, v);
+              } else {
+                const float fv = (float)site[slot_of_mu[mu] * 18 + k];
+                uint32_t v;
+                std::memcpy(&v, &fv, 4);
+                for (int b = 3; b >= 0; --b, v >>= 8) o[b] = (unsigned char)(v & 0xff);
+              }
             }
         }
         ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
@@ -243,6 +256,96 @@ int laph_lime_write_gauge(const char* path, const double* conf, int L, int T) {
   }
   return LAPH_OK;
 }
+
+int laph_lime_write_gauge(const char* path, const double* conf, int L, int T) {
+  return laph_lime_write_gauge_prec(path, conf, L, T, 64);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Integer content of <tag>...</tag> in an XML text, 0 when absent.
+int xml_int(const std::string& xml, const char* tag) {
+  const std::string open = std::string("<") + tag + ">";
+  const size_t a = xml.find(open);
+  if (a == std::string::npos) return 0;
+  return std::atoi(xml.c_str() + a + open.size());
+}
+
+// Walk the LIME records of an open file: keeps the ildg-format payload (if any
+// precedes the binary data) and stops at the ildg-binary-data header, leaving
+// the file positioned at its payload.
+int lime_find_binary(FILE* f, const char* path, uint64_t* len, std::string* xml) {
+  unsigned char h[144];
+  for (;;) {
+    if (std::fread(h, 1, 144, f) != 144) break;
+    if (!(h[0] == 0x45 && h[1] == 0x67 && h[2] == 0x89 && h[3] == 0xab)) {
+      set_error("%s: bad LIME magic number", path);
+      return LAPH_EIO;
+    }
+    const uint64_t n = get_be64(h + 8);
+    char type[129];
+    std::memcpy(type, h + 16, 128);
+    type[128] = 0;
+    if (std::strcmp(type, "ildg-binary-data") == 0) {
+      *len = n;
+      return LAPH_OK;
+    }
+    if (xml && std::strcmp(type, "ildg-format") == 0 && n < (1u << 20)) {
+      std::string s(n, '\0');
+      if (std::fread(&s[0], 1, n, f) != n) break;
+      *xml = s;
+      if (n % 8 && fseeko(f, (off_t)(8 - n % 8), SEEK_CUR) != 0) break;
+      continue;
+    }
+    if (fseeko(f, (off_t)((n + 7) / 8 * 8), SEEK_CUR) != 0) break;
+  }
+  set_error("no ildg-binary-data record found in file %s", path);
+  return LAPH_ENORECORD;
+}
+
+// Timeslices [t_i, t_f] of an ILDG payload with es-byte big-endian reals at the
+// file position, into conf in the LAPH_LAYOUT_CONF order (FP32 widened).
+int lime_read_payload(FILE* f, const char* path, int L, int t_i, int t_f, int es, double* conf) {
+  const long long V3 = (long long)L * L * L;
+  if (fseeko(f, (off_t)((uint64_t)t_i * V3 * 72 * es), SEEK_CUR) != 0) {
+    set_error("%s: seek failed", path);
+    return LAPH_EIO;
+  }
+  std::vector<unsigned char> buf((size_t)L * 72 * es);
+  for (int t = t_i; t <= t_f; ++t)
+    for (int z = 0; z < L; ++z)
+      for (int y = 0; y < L; ++y) {
+        if (std::fread(buf.data(), 1, buf.size(), f) != buf.size()) {
+          set_error("LIME read error while reading file %s", path);
+          return LAPH_EIO;
+        }
+        for (int x = 0; x < L; ++x) {
+          double* site = conf + ((long long)(t - t_i) * V3 + (long long)x * L * L + (long long)y * L + z) * 72;
+          for (int mu = 0; mu < 4; ++mu) {
+            const int slot = (mu == 3) ? 0 : mu + 1;
+            for (int k = 0; k < 18; ++k) {
+              const unsigned char* q = &buf[((size_t)x * 72 + mu * 18 + k) * es];
+              if (es == 8) {
+                const uint64_t v = get_be64(q);
+                std::memcpy(&site[slot * 18 + k], &v, 8);
+              } else {
+                const uint32_t v = (uint32_t)q[0] << 24 | (uint32_t)q[1] << 16 | (uint32_t)q[2] << 8 | q[3];
+                float fv;
+                std::memcpy(&fv, &v, 4);
+                site[slot * 18 + k] = fv;
+              }
+            }
+          }
+        }
+      }
+  return LAPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 // read_lime_gauge_field_doubleprec_timeslices (modules/io.cpp:22-146), but
 // seeking straight to timeslice t_i instead of reading the whole file.
@@ -256,30 +359,11 @@ int laph_lime_read_gauge(const char* path, int T, int L, int t_i, int t_f, doubl
     set_error("Could not open file %s", path);
     return LAPH_EIO;
   }
-  unsigned char h[144];
-  bool found = false;
   uint64_t len = 0;
-  for (;;) {
-    if (std::fread(h, 1, 144, f) != 144) break;
-    if (!(h[0] == 0x45 && h[1] == 0x67 && h[2] == 0x89 && h[3] == 0xab)) {
-      std::fclose(f);
-      set_error("%s: bad LIME magic number", path);
-      return LAPH_EIO;
-    }
-    len = get_be64(h + 8);
-    char type[129];
-    std::memcpy(type, h + 16, 128);
-    type[128] = 0;
-    if (std::strcmp(type, "ildg-binary-data") == 0) {
-      found = true;
-      break;
-    }
-    if (fseeko(f, (off_t)((len + 7) / 8 * 8), SEEK_CUR) != 0) break;
-  }
-  if (!found) {
+  int st = lime_find_binary(f, path, &len, nullptr);
+  if (st != LAPH_OK) {
     std::fclose(f);
-    set_error("no ildg-binary-data record found in file %s", path);
-    return LAPH_ENORECORD;
+    return st;
   }
   const long long V3 = (long long)L * L * L;
   const uint64_t want = (uint64_t)V3 * T * 72ull * 8ull;
@@ -293,32 +377,81 @@ int laph_lime_read_gauge(const char* path, int T, int L, int t_i, int t_f, doubl
               (unsigned long long)len, path, (unsigned long long)want);
     return LAPH_ESIZE;
   }
-  if (fseeko(f, (off_t)((uint64_t)t_i * V3 * 72 * 8), SEEK_CUR) != 0) {
-    std::fclose(f);
-    set_error("%s: seek failed", path);
+  st = lime_read_payload(f, path, L, t_i, t_f, 8, conf);
+  std::fclose(f);
+  return st;
+}
+
+int laph_lime_read_gauge_any(const char* path, int T, int L, int t_i, int t_f, double* conf, int* precision) {
+  if (!path || !conf || T < 1 || L < 1 || t_i < 0 || t_f < t_i || t_f >= T) {
+    set_error("laph_lime_read_gauge_any: bad argument");
+    return LAPH_EINVAL;
+  }
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    set_error("Could not open file %s", path);
     return LAPH_EIO;
   }
-  std::vector<unsigned char> buf((size_t)L * 72 * 8);
-  for (int t = t_i; t <= t_f; ++t)
-    for (int z = 0; z < L; ++z)
-      for (int y = 0; y < L; ++y) {
-        if (std::fread(buf.data(), 1, buf.size(), f) != buf.size()) {
-          std::fclose(f);
-          set_error("LIME read error while reading file %s", path);
-          return LAPH_EIO;
-        }
-        for (int x = 0; x < L; ++x) {
-          double* site = conf + ((long long)(t - t_i) * V3 + (long long)x * L * L + (long long)y * L + z) * 72;
-          for (int mu = 0; mu < 4; ++mu) {
-            const int slot = (mu == 3) ? 0 : mu + 1;
-            for (int k = 0; k < 18; ++k) {
-              uint64_t v = get_be64(&buf[((size_t)x * 72 + mu * 18 + k) * 8]);
-              std::memcpy(&site[slot * 18 + k], &v, 8);
-            }
-          }
-        }
-      }
+  uint64_t len = 0;
+  std::string xml;
+  int st = lime_find_binary(f, path, &len, &xml);
+  if (st != LAPH_OK) {
+    std::fclose(f);
+    return st;
+  }
+  const uint64_t want = (uint64_t)L * L * L * T * 72ull * 8ull;
+  const int es = len == want ? 8 : (len == want / 2 ? 4 : 0);
+  const int declared = xml.empty() ? 0 : xml_int(xml, "precision");
+  if (es == 0 || (declared && declared != 8 * es)) {
+    std::fclose(f);
+    if (es == 0)
+      set_error("%s: %llu bytes of binary data fit neither FP64 nor FP32 links of %d^3 x %d", path,
+                (unsigned long long)len, L, T);
+    else
+      set_error("%s: ildg-format declares precision %d but the binary data holds %d-bit reals", path, declared,
+                8 * es);
+    return LAPH_ESIZE;
+  }
+  st = lime_read_payload(f, path, L, t_i, t_f, es, conf);
   std::fclose(f);
+  if (st == LAPH_OK && precision) *precision = 8 * es;
+  return st;
+}
+
+int laph_lime_info(const char* path, int* lx, int* ly, int* lz, int* lt, int* precision) {
+  if (!path || !lx || !ly || !lz || !lt || !precision) {
+    set_error("laph_lime_info: bad argument");
+    return LAPH_EINVAL;
+  }
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    set_error("Could not open file %s", path);
+    return LAPH_EIO;
+  }
+  uint64_t len = 0;
+  std::string xml;
+  const int st = lime_find_binary(f, path, &len, &xml);
+  std::fclose(f);
+  if (st != LAPH_OK) return st;
+  if (xml.empty()) {
+    set_error("%s: no ildg-format record before the binary data", path);
+    return LAPH_ENORECORD;
+  }
+  *lx = xml_int(xml, "lx");
+  *ly = xml_int(xml, "ly");
+  *lz = xml_int(xml, "lz");
+  *lt = xml_int(xml, "lt");
+  *precision = xml_int(xml, "precision");
+  if (*lx <= 0 || *ly <= 0 || *lz <= 0 || *lt <= 0 || (*precision != 32 && *precision != 64)) {
+    set_error("%s: ildg-format record without valid lx/ly/lz/lt/precision", path);
+    return LAPH_EPARSE;
+  }
+  const uint64_t want = (uint64_t)*lx * *ly * *lz * *lt * 72ull * (*precision / 8);
+  if (len != want) {
+    set_error("%s: ildg-format describes %llu bytes of links, the binary record holds %llu", path,
+              (unsigned long long)want, (unsigned long long)len);
+    return LAPH_ESIZE;
+  }
   return LAPH_OK;
 }
 
@@ -417,6 +550,70 @@ int laph_read_eigenvalues_bin(const char* dir, const char* prefix, int config, i
   std::fclose(f);
   if (got != (size_t)nev) {
     set_error("%s: short read", name);
+    return LAPH_EIO;
+  }
+  return LAPH_OK;
+}
+
+int laph_sourceshape_avg(int L, const double* psi, double* r_out, double* psi_out, int* n_out) {
+  if (L < 2 || (L & 1) || !psi || !r_out || !psi_out || !n_out) {
+    set_error("laph_sourceshape_avg: bad argument (even L >= 2 and all arrays needed)");
+    return LAPH_EINVAL;
+  }
+  std::vector<long long> cnt;
+  std::vector<double> rad, sum;
+  int idx = 0;
+  for (int r1 = 0; r1 < L; r1 += 2)
+    for (int r2 = 0; r2 < L; r2 += 2)
+      for (int r3 = 0; r3 < L; r3 += 2, ++idx) {
+        const double len = std::sqrt((double)r1 * r1 + (double)r2 * r2 + (double)r3 * r3);
+        size_t t = 0;
+        while (t < rad.size() && !(std::fabs(len - rad[t]) < 1e-11)) ++t;
+        if (t == rad.size()) {
+          rad.push_back(len);
+          cnt.push_back(0);
+          sum.push_back(0.0);
+        }
+        ++cnt[t];
+        sum[t] += psi[idx];
+      }
+  for (size_t t = 0; t < rad.size(); ++t) {
+    r_out[t] = rad[t];
+    psi_out[t] = sum[t] / (double)cnt[t];
+  }
+  *n_out = (int)rad.size();
+  return LAPH_OK;
+}
+
+int laph_write_sourceshape(const char* dir, int config, int t, int nev, int n, const double* r, const double* psi) {
+  if (n < 0 || (n > 0 && (!r || !psi))) {
+    set_error("laph_write_sourceshape: bad argument");
+    return LAPH_EINVAL;
+  }
+  const std::string pre = (dir && *dir) ? std::string(dir) + "/" : std::string();
+  char name[1200];
+  std::snprintf(name, sizeof name, "%ssourceshape_nev%d.%d.%d", pre.c_str(), nev, config, t);
+  FILE* f = std::fopen(name, "w");
+  if (!f) {
+    set_error("cannot open %s for writing", name);
+    return LAPH_EIO;
+  }
+  bool ok = std::fprintf(f, "#r\tpsi(r)\n") > 0;
+  for (int i = 0; ok && i < n; ++i) ok = std::fprintf(f, "%.12g %.12g\n", r[i], psi[i]) > 0;
+  if (std::fclose(f) != 0) ok = false;
+  std::snprintf(name, sizeof name, "%ssourceshape_nev%d.%04d.%03d.bin", pre.c_str(), nev, config, t);
+  f = ok ? std::fopen(name, "wb") : nullptr;
+  if (f) {
+    for (int i = 0; ok && i < n; ++i) {
+      const double pair[2] = {r[i], psi[i]};
+      ok = std::fwrite(pair, sizeof(double), 2, f) == 2;
+    }
+    if (std::fclose(f) != 0) ok = false;
+  } else {
+    ok = false;
+  }
+  if (!ok) {
+    set_error("write error on %s", name);
     return LAPH_EIO;
   }
   return LAPH_OK;

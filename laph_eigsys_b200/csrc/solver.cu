@@ -37,6 +37,11 @@
 #include "mlp.cuh"
 #include "smear.cuh"
 
+namespace laph {
+int sourceshape_device(const double2* V, int L, int nev, const double* evals, double2* work, double* psi,
+                       cudaStream_t st);
+}
+
 using namespace laph;
 
 struct laph_solver {
@@ -646,6 +651,24 @@ int laph_solver_stream(laph_solver* s, void** stream) {
 int laph_solver_timings(laph_solver* s, double* ms4) {
   if (!s || !ms4) return LAPH_EINVAL;
   for (int i = 0; i < 4; ++i) ms4[i] = s->ms[i];
+  return LAPH_OK;
+}
+
+int laph_solver_sourceshape(laph_solver* s, int i, int weighted, double* psi) {
+  if (!s || i < 0 || i >= s->np || !s->ran || !psi || (s->hd[i].L & 1)) {
+    set_error("laph_solver_sourceshape: bad argument, solver not run, or odd L");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  const ProbDesc& d = s->hd[i];
+  const int H = d.L / 2, Nc = H * H * H;
+  // scratch: the filtered block W (class-major copy of V) and Y (psi bins) of this
+  // problem, both free once the run has finished and rewritten by the next run
+  double* dpsi = reinterpret_cast<double*>(s->Y + d.blk);
+  LAPH_TRY(sourceshape_device(s->V + d.blk, d.L, d.nev, weighted ? s->theta + d.kv : nullptr, s->W + d.blk, dpsi,
+                              s->st));
+  LAPH_CUDA_TRY(cudaMemcpyAsync(psi, dpsi, sizeof(double) * Nc, cudaMemcpyDeviceToHost, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
   return LAPH_OK;
 }
 

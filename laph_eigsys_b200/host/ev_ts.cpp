@@ -12,6 +12,9 @@
 // MPI ranks (src/ev_ts.cpp:103-119): with LAPH_RANK / LAPH_WORLD_SIZE (or
 // RANK / WORLD_SIZE) set, rank r gets a contiguous block, the first LT % size
 // ranks one extra.  One JSON line per timeslice goes to stdout.
+// Beyond the reference: FP32 ILDG input is read (widened to FP64), and
+// --resume skips timeslices whose three output files are already complete
+// (right sizes, eigenvectors passing check_trace).
 #include <sys/stat.h>
 
 #include <cmath>
@@ -29,7 +32,7 @@ namespace {
 
 void usage() {
   std::fprintf(stderr,
-               "usage: laph_ev_ts --conf N [--phase_reset 0|1] [--parameters FILE]\n"
+               "usage: laph_ev_ts --conf N [--phase_reset 0|1] [--parameters FILE] [--resume]\n"
                "  reads parameters.txt (keys of LapH_EigSys plus smear, rho, alpha, tol, guard, solver)\n");
 }
 
@@ -64,6 +67,23 @@ bool load_window_model(const char* exe, std::vector<float>* model) {
   return ok;
 }
 
+// A timeslice's outputs are complete when all three files have their full
+// size and the eigenvectors pass check_trace (what the writer checks first).
+bool outputs_complete(const char* dir, int config, int t, int dim, int nev) {
+  static const char* kinds[3] = {"eigenvectors", "eigenvalues", "phases"};
+  for (int k = 0; k < 3; ++k) {
+    char name[1200];
+    std::snprintf(name, sizeof name, "%s/%s.%04d.%03d", dir, kinds[k], config, t);
+    struct stat sb;
+    const long long want = k == 0 ? 16LL * dim * nev : 8LL * nev;
+    if (stat(name, &sb) != 0 || (long long)sb.st_size != want) return false;
+  }
+  std::vector<double> V((size_t)2 * dim * nev);
+  if (laph_read_eigsys_bin(dir, "eigenvectors", config, t, dim, nev, V.data()) != LAPH_OK) return false;
+  double tr = 0.0, sum = 0.0;
+  return laph_check_trace(dim, nev, V.data(), &tr, &sum) == 1;
+}
+
 double trace_vdv(int dim, int nev, const double* V) {
   double tr = 0.0, sum = 0.0;
   laph_check_trace(dim, nev, V, &tr, &sum);
@@ -73,7 +93,7 @@ double trace_vdv(int dim, int nev, const double* V) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  int config = -1, phase_reset = 0;
+  int config = -1, phase_reset = 0, resume = 0;
   std::string params = "parameters.txt";
   for (int i = 1; i < argc; ++i) {
     const std::string a = argv[i];
@@ -81,6 +101,7 @@ int main(int argc, char** argv) {
     else if (a.rfind("--conf=", 0) == 0) config = std::atoi(a.c_str() + 7);
     else if (a == "--phase_reset" && i + 1 < argc) phase_reset = std::atoi(argv[++i]);
     else if (a == "--parameters" && i + 1 < argc) params = argv[++i];
+    else if (a == "--resume") resume = 1;
     else if (a == "--help") {
       usage();
       return 1;
@@ -108,8 +129,19 @@ int main(int argc, char** argv) {
   std::snprintf(conf_name, sizeof conf_name, "%s/conf.%04d", P.config_path, config);
   std::vector<double> conf((size_t)std::max(ntodo, 1) * V3 * 72);
   if (ntodo > 0) {
-    st = laph_lime_read_gauge(conf_name, LT, L, t0, t0 + ntodo - 1, conf.data());
+    int prec = 64;
+    st = laph_lime_read_gauge_any(conf_name, LT, L, t0, t0 + ntodo - 1, conf.data(), &prec);
     if (st != LAPH_OK) return die(st, "read gauge");
+    if (prec == 32) std::printf("Reading single-precision ILDG data, widened to double\n");
+  }
+  // timeslices of this process still to solve (all of them without --resume)
+  std::vector<int> todo;
+  for (int ts = 0; ts < ntodo; ++ts) {
+    if (resume && outputs_complete(P.result_path, config, t0 + ts, dim, nev)) {
+      std::printf("{\"t\": %d, \"skipped\": \"outputs complete\"}\n", t0 + ts);
+      continue;
+    }
+    todo.push_back(ts);
   }
   const double p1 = P.smear == LAPH_SMEAR_HYP ? P.alpha_1 : (P.smear == LAPH_SMEAR_STOUT ? P.rho : P.alpha);
   const double p2 = P.smear == LAPH_SMEAR_HYP ? P.alpha_2 : 0.0;
@@ -121,7 +153,7 @@ int main(int argc, char** argv) {
     laph_ctx* ctx = nullptr;
     st = laph_ctx_create(&ctx, &lp);
     if (st != LAPH_OK) return die(st, "context");
-    for (int ts = 0; ts < ntodo; ++ts) {
+    for (int ts : todo) {
       PetscLogDouble v1, v2;
       PetscTime(&v1);
       st = laph_set_links(ctx, conf.data() + (size_t)ts * V3 * 72, LAPH_LAYOUT_CONF);
@@ -179,8 +211,9 @@ int main(int argc, char** argv) {
   }
 
   // ---- block: every timeslice of this process in one batched solve
-  if (ntodo == 0) return 0;
-  std::vector<laph_problem> probs(ntodo, laph_problem{L, nev});
+  const int nsolve = (int)todo.size();
+  if (nsolve == 0) return 0;
+  std::vector<laph_problem> probs(nsolve, laph_problem{L, nev});
   laph_solve_opts o;
   laph_solve_opts_default(&o);
   o.smear_kind = P.smear;
@@ -192,7 +225,7 @@ int main(int argc, char** argv) {
   o.tol = P.tol > 0 ? P.tol : 1e-9;
   o.window = P.window;
   laph_solver* s = nullptr;
-  st = laph_solver_create(&s, probs.data(), ntodo, &o, device);
+  st = laph_solver_create(&s, probs.data(), nsolve, &o, device);
   if (st != LAPH_OK) return die(st, "solver");
   if (o.window == LAPH_WINDOW_MLP) {
     std::vector<float> model;
@@ -203,17 +236,18 @@ int main(int argc, char** argv) {
     st = laph_solver_set_window_model(s, model.data(), (int)model.size());
     if (st != LAPH_OK) return die(st, "window model");
   }
-  for (int ts = 0; ts < ntodo; ++ts) {
-    st = laph_solver_set_links(s, ts, conf.data() + (size_t)ts * V3 * 72, LAPH_LAYOUT_CONF, 0);
+  for (int i = 0; i < nsolve; ++i) {
+    st = laph_solver_set_links(s, i, conf.data() + (size_t)todo[i] * V3 * 72, LAPH_LAYOUT_CONF, 0);
     if (st != LAPH_OK) return die(st, "links");
   }
-  std::vector<laph_result> res(ntodo);
+  std::vector<laph_result> res(nsolve);
   st = laph_solver_run(s, res.data());
   if (st != LAPH_OK && st != LAPH_ENOTCONV) return die(st, "solve");
   double ms[4];
   laph_solver_timings(s, ms);
-  for (int ts = 0; ts < ntodo; ++ts) {
-    st = laph_solver_get(s, ts, evals.data(), vfix.data(), phases.data(), 0);
+  for (int i = 0; i < nsolve; ++i) {
+    const int ts = todo[i];
+    st = laph_solver_get(s, i, evals.data(), vfix.data(), phases.data(), 0);
     if (st != LAPH_OK) return die(st, "fetch");
     st = laph_write_eigsys_bin(P.result_path, "eigenvectors", config, t0 + ts, dim, nev, vfix.data());
     if (st != LAPH_OK) return die(st, "write eigenvectors");
@@ -221,7 +255,7 @@ int main(int argc, char** argv) {
     laph_write_eigenvalues_bin(P.result_path, "phases", config, t0 + ts, nev, phases.data());
     std::printf("{\"t\": %d, \"solver\": \"block\", \"status\": %d, \"iters\": %d, \"max_resid\": %.3e, "
                 "\"trace_vdv\": %.12f, \"eval0\": %.12f, \"batch_ms\": %.2f}\n",
-                t0 + ts, res[ts].status, res[ts].iters, res[ts].max_resid, res[ts].trace_vdv, evals[0], ms[3]);
+                t0 + ts, res[i].status, res[i].iters, res[i].max_resid, res[i].trace_vdv, evals[0], ms[3]);
   }
   laph_solver_destroy(s);
   return 0;

@@ -51,6 +51,8 @@ _sig("orc_recover_spectrum", None, _i, _vp, _i, _d, _d, _vp)
 _sig("orc_fix_phase", None, _i, _i, _vp, _vp, _vp)
 _sig("orc_build_neglap_dense", None, _vp, _i, _vp)
 _sig("orc_mlp_loss_grad", _d, _vp, _vp, _vp, _i, _vp)
+_sig("orc_sourceshape", None, _vp, _i, _i, _vp)
+_sig("orc_sourceshape_avg", _i, _i, _vp, _vp, _vp)
 
 
 def _p(a):
@@ -173,6 +175,24 @@ def neglap_dense(U, L):
     A = np.zeros((dim, dim), dtype=np.complex128)
     _lib.orc_build_neglap_dense(_p(U), L, _p(A))
     return A
+
+
+def sourceshape(V, L):
+    """psi(r) on the grid r_i = 0, 2, ... < L (r1 outer, r3 inner)."""
+    V = np.asfortranarray(V, dtype=np.complex128)
+    n = ((L + 1) // 2) ** 3
+    psi = np.empty(n)
+    _lib.orc_sourceshape(ctypes.c_void_p(V.ctypes.data), L, V.shape[1], _p(psi))
+    return psi
+
+
+def sourceshape_avg(L, psi):
+    """avg_radii: (radii, psi averages) in order of first appearance."""
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    r = np.empty(len(psi))
+    a = np.empty(len(psi))
+    n = _lib.orc_sourceshape_avg(L, _p(psi), _p(r), _p(a))
+    return r[:n], a[:n]
 
 
 def free_spectrum(L):

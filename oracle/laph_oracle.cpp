@@ -19,6 +19,7 @@
 #include "laph_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -750,6 +751,70 @@ double orc_mlp_loss_grad(const double* P, const double* X, const double* Y, int 
     }
   }
   return loss / (n * O);
+}
+
+// source_shape_complete (modules/sourceshape_funcs.cpp:58-81) with dll_op
+// (:30-55) and get_vectorial_dst_ind (:11-27): for r = (r1, r2, r3) on the grid
+// r_i = 0, 2, ... < L (r1 outer, r3 inner), psi(r) = sum over sites x of
+// sqrt(tr(M M^dag)), M = V_{x+r} V_x^dag with V_y the 3 x nev block of rows
+// 3y .. 3y+2 of the column-major eigensystem; x+r steps r_i times up in
+// direction i with the periodic neighbours of modules/navigation.cpp.
+void orc_sourceshape(const double* Vd, int L, int nev, double* psi) {
+  const cd* V = reinterpret_cast<const cd*>(Vd);
+  const long long V3 = (long long)L * L * L, dim = 3 * V3;
+  int idx = 0;
+  std::vector<std::array<int, 3>> grid;
+  for (int r1 = 0; r1 < L; r1 += 2)
+    for (int r2 = 0; r2 < L; r2 += 2)
+      for (int r3 = 0; r3 < L; r3 += 2) grid.push_back({r1, r2, r3});
+  for (const auto& r : grid) {
+    double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+    for (long long s = 0; s < V3; ++s) {
+      const int x = (int)(s / (L * L)), y = (int)((s / L) % L), z = (int)(s % L);
+      const long long dst = (long long)((x + r[0]) % L) * L * L + ((y + r[1]) % L) * L + (z + r[2]) % L;
+      double fro = 0.0;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          cd m = 0.0;
+          for (int n = 0; n < nev; ++n) m += V[3 * dst + a + n * dim] * std::conj(V[3 * s + b + n * dim]);
+          fro += std::norm(m);
+        }
+      acc += std::sqrt(fro);
+    }
+    psi[idx++] = acc;
+  }
+}
+
+// avg_radii (modules/sourceshape_funcs.cpp:100-135): psi averaged over grid
+// points of equal |r| (within 1e-11), radii in order of first appearance.
+int orc_sourceshape_avg(int L, const double* psi, double* r_out, double* psi_out) {
+  std::vector<int> cnt;
+  std::vector<double> rad, sum;
+  int idx = 0;
+  for (int r1 = 0; r1 < L; r1 += 2)
+    for (int r2 = 0; r2 < L; r2 += 2)
+      for (int r3 = 0; r3 < L; r3 += 2) {
+        const double len = std::sqrt((double)(r1 * r1 + r2 * r2 + r3 * r3));
+        bool found = false;
+        for (size_t t = 0; t < rad.size(); ++t)
+          if (std::fabs(len - rad[t]) < 1e-11) {
+            ++cnt[t];
+            sum[t] += psi[idx];
+            found = true;
+          }
+        if (!found) {
+          cnt.push_back(1);
+          rad.push_back(len);
+          sum.push_back(psi[idx]);
+        }
+        ++idx;
+      }
+  for (size_t t = 0; t < rad.size(); ++t) {
+    r_out[t] = rad[t];
+    psi_out[t] = sum[t] / cnt[t];
+  }
+  return (int)rad.size();
 }
 
 }  // extern "C"

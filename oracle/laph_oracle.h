@@ -86,6 +86,13 @@ void orc_fix_phase(int dim, int nev, const double* V, double* Vfix, double* phas
  * modules/config_utils.cpp:18-58), complex128 row-major [dim][dim]. */
 void orc_build_neglap_dense(const double* links3, int L, double* A);
 
+/* Source shape psi(r) (modules/sourceshape_funcs.cpp:30-81) on the grid
+ * r_i = 0, 2, ... < L, r1 outer and r3 inner: psi[(L+1)/2 cubed].  V is the
+ * column-major complex128 eigensystem [3*V3][nev]. */
+void orc_sourceshape(const double* V, int L, int nev, double* psi);
+/* avg_radii (sourceshape_funcs.cpp:100-135); returns the number of radii. */
+int orc_sourceshape_avg(int L, const double* psi, double* r_out, double* psi_out);
+
 /* Window MLP (16->64->64->3, tanh) mean-squared loss and gradient, FP64. */
 double orc_mlp_loss_grad(const double* params, const double* X, const double* Y, int n, double* grad);
 

@@ -45,3 +45,42 @@ def test_ev_ts_cli(gpu, orc, tmp_path, solver):
         assert np.abs(np.sort(-ev) - refs[t][:nev]).max() < tol
         assert np.abs(V[0].imag).max() < 1e-12
         assert ph.shape == (nev,)
+
+
+def test_ev_ts_cli_fp32_input_and_resume(gpu, orc, tmp_path):
+    """Single-precision ILDG input (widened to FP64 on reading) and --resume, which solves only the timeslices
+    whose outputs are missing or incomplete."""
+    L, T, nev, cfgno = 6, 3, 10, 1228
+    conf = lb.gauge_random(L, T, 0.4, 1228)
+    gdir = tmp_path / "gauges"
+    gdir.mkdir()
+    lb.lime_write_gauge(gdir / f"conf.{cfgno:04d}", conf, L, T, precision=32)
+    conf32, _ = lb.lime_read_gauge_any(gdir / f"conf.{cfgno:04d}", T, L, 0, T - 1)
+    out = tmp_path / "out"
+    out.mkdir()
+    refs = []
+    for t in range(T):
+        Us = orc.smear_hyp(lb.spatial_links(conf32[t]), L, 0.62, 0.52, 2)
+        refs.append(np.linalg.eigvalsh(orc.neglap_dense(Us, L)))
+    (tmp_path / "parameters.txt").write_text(
+        f"config_path = {gdir}\nresult_path = {out}\nLT = {T}\nLX = {L}\nNEV = {nev}\n"
+        f"alpha_1 = 0.62\nalpha_2 = 0.52\niter = 2\nLAM_L = 12.0\nLAM_C = 1.0\nDEG = 8\nOMP_THRDS = 2\n"
+        f"tol = 1e-11\nsolver = block\n")
+    r = subprocess.run([EXE, "--conf", str(cfgno)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "single-precision" in r.stdout
+    for t in range(T):
+        ev = lb.read_eigenvalues_bin(out, "eigenvalues", cfgno, t, nev)
+        assert np.abs(np.sort(-ev) - refs[t][:nev]).max() < 1e-9
+    before = lb.read_eigenvalues_bin(out, "eigenvalues", cfgno, 1, nev)
+    # damage timeslice 1's phases file; resume must redo exactly that timeslice
+    (out / f"phases.{cfgno:04d}.001").write_bytes(b"\0" * 8)
+    r = subprocess.run([EXE, "--conf", str(cfgno), "--resume"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert sum('"skipped"' in ln for ln in lines) == T - 1
+    assert sum('"solver": "block"' in ln and '"t": 1,' in ln for ln in lines) == 1
+    assert os.path.getsize(out / f"phases.{cfgno:04d}.001") == 8 * nev
+    after = lb.read_eigenvalues_bin(out, "eigenvalues", cfgno, 1, nev)
+    assert np.abs(after - before).max() < 1e-9

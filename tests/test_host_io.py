@@ -144,3 +144,58 @@ def test_gauge_random_deterministic_and_seeded():
     # eps = 0 gives the unit field
     u = lb.gauge_random(3, 1, 0.0, 1)
     assert np.abs(u - np.eye(3)).max() < 1e-14
+
+
+def test_lime_fp32_roundtrip_and_info(tmp_path):
+    """FP32 ILDG files (the reference stops at them, io.cpp:72-79): written big-endian with an ildg-format record,
+    read back widened to FP64 equal to the FP32-rounded links; the strict reader keeps the reference's error."""
+    L, T = 4, 3
+    conf = lb.gauge_random(L, T, 0.3, 1234)
+    p32, p64 = tmp_path / "c32", tmp_path / "c64"
+    lb.lime_write_gauge(p32, conf, L, T, precision=32)
+    lb.lime_write_gauge(p64, conf, L, T)
+    assert lb.lime_info(p32) == (L, L, L, T, 32)
+    assert lb.lime_info(p64) == (L, L, L, T, 64)
+    got, prec = lb.lime_read_gauge_any(p32, T, L, 1, 2)
+    assert prec == 32
+    want = conf[1:3].real.astype(np.float32).astype(np.float64) + 1j * conf[1:3].imag.astype(np.float32)
+    assert np.array_equal(got, want)
+    got64, prec64 = lb.lime_read_gauge_any(p64, T, L, 0, T - 1)
+    assert prec64 == 64 and np.array_equal(got64, conf)
+    with pytest.raises(lb.LaphError) as e:
+        lb.lime_read_gauge(p32, T, L, 0, 0)
+    assert e.value.status == _lib.LAPH_ESINGLE
+    # the record sizes of an FP32 file: 144 + xml (padded) + 144 + V3 T 72 4
+    raw = open(p32, "rb").read()
+    assert len(raw) % 8 == 0 and len(raw) > L ** 3 * T * 72 * 4
+
+
+def test_lime_precision_mismatch_and_missing_format(tmp_path):
+    L, T = 3, 2
+    n64 = L ** 3 * T * 72 * 8
+    xml = ("<?xml version=\"1.0\"?><ildgFormat><precision>32</precision><lx>3</lx><ly>3</ly><lz>3</lz>"
+           "<lt>2</lt></ildgFormat>").encode()
+    p = tmp_path / "mismatch"
+    p.write_bytes(_lime_record("ildg-format", xml, me=False) + _lime_record("ildg-binary-data", b"\0" * n64,
+                                                                          mb=False))
+    with pytest.raises(lb.LaphError) as e:
+        lb.lime_read_gauge_any(p, T, L, 0, 0)
+    assert e.value.status == _lib.LAPH_ESIZE
+    with pytest.raises(lb.LaphError) as e:
+        lb.lime_info(p)
+    assert e.value.status == _lib.LAPH_ESIZE
+    # the strict reader ignores the XML, as the reference does
+    conf = lb.lime_read_gauge(p, T, L, 0, 0)
+    assert np.all(conf == 0)
+    q = tmp_path / "noformat"
+    q.write_bytes(_lime_record("ildg-binary-data", b"\0" * (n64 // 2)))
+    with pytest.raises(lb.LaphError) as e:
+        lb.lime_info(q)
+    assert e.value.status == _lib.LAPH_ENORECORD
+    got, prec = lb.lime_read_gauge_any(q, T, L, 0, T - 1)
+    assert prec == 32 and np.all(got == 0)
+    r = tmp_path / "badsize"
+    r.write_bytes(_lime_record("ildg-binary-data", b"\0" * 800))
+    with pytest.raises(lb.LaphError) as e:
+        lb.lime_read_gauge_any(r, T, L, 0, 0)
+    assert e.value.status == _lib.LAPH_ESIZE
