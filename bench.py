@@ -54,6 +54,21 @@ CONFIGS = {
     "c5": dict(L=48, T=96, eps=0.25, seed=1233, smear="stout", p1=0.1, p2=0.0, iters=6, compat=1, nev=220,
                guard=16, link_prec="fp32", tol=1e-9, deg=48, wave=16),
 }
+def hyp_scan_grid(a1i, a1f, a2i, a2f):
+    """tune_hyp's (alpha_1, alpha_2) grid with its own loops (src/tune_hyp.cpp:116-117)."""
+    out, a1 = [], a1i
+    while a1 <= a1f:
+        a2 = a2i
+        while a2 <= a2f:
+            out.append((a1, a2))
+            a2 += 0.05
+        a1 += 0.05
+    return out
+
+
+# 32^3, HYP x 3, nev 120: timeslice 0 of seed 1234 under a 4 x 4 (alpha_1, alpha_2) grid in one batch
+CONFIGS["c6"] = dict(L=32, T=16, eps=0.3, seed=1234, smear="hyp", p1=0.4, p2=0.4, iters=3, compat=1, nev=120,
+                     guard=16, link_prec="fp32", tol=1e-9, deg=56, scan=hyp_scan_grid(0.4, 0.56, 0.4, 0.56))
 HBM_FALLBACK = 6650.0
 # DRAM bytes (read + write) of one k_cheb_mrhs2 launch over its algorithmic bytes, from an ncu capture of the same
 # kernel on 32^3 x 4 timeslices (2.134 GB / 2.155 GB); the filter's traffic grows with the site-vectors processed,
@@ -143,6 +158,9 @@ def generate_links(cfg, seed_offset=0):
     """Spatial links of one batch: list of (L, nev, links (V3, 3, 3, 3))."""
     import laph_eigsys_b200 as lb
     out = []
+    if cfg.get("scan"):
+        conf = lb.gauge_random(cfg["L"], 1, cfg["eps"], cfg["seed"] + seed_offset)
+        return [(cfg["L"], cfg["nev"], np.ascontiguousarray(conf[0, :, 1:4])) for _ in cfg["scan"]]
     for L, T, nev, seed in cfg.get("mixed") or [(cfg["L"], cfg.get("wave") or cfg["T"], cfg["nev"], cfg["seed"])]:
         conf = lb.gauge_random(L, T, cfg["eps"], seed + seed_offset)
         for t in range(T):
@@ -154,7 +172,7 @@ def make_solver(cfg, device, batch):
     import laph_eigsys_b200 as lb
     kinds = {"stout": lb.SMEAR_STOUT, "ape": lb.SMEAR_APE, "hyp": lb.SMEAR_HYP, "none": lb.SMEAR_NONE}
     probs = [(L, nev) for L, nev, _ in batch]
-    return lb.Solver(probs, device=device, smear_kind=kinds[cfg["smear"]], smear_p1=cfg["p1"], smear_p2=cfg["p2"],
+    s = lb.Solver(probs, device=device, smear_kind=kinds[cfg["smear"]], smear_p1=cfg["p1"], smear_p2=cfg["p2"],
                      smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
                      link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
                      max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
@@ -162,6 +180,9 @@ def make_solver(cfg, device, batch):
                      lam_cut=cfg.get("lam_cut0", 0.0),
                      window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
                          cfg.get("window", "mlp")])
+    for i, (a1, a2) in enumerate(cfg.get("scan") or []):
+        s.set_smear(i, a1, a2)  # the batched tune_hyp scan: one copy of the timeslice per grid point
+    return s
 
 
 def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads, L=None, nev=None):
@@ -250,6 +271,11 @@ def run_reference(args, cfg):
 def workload_config(cfg):
     if cfg.get("mixed"):
         shape = " + ".join(f"{L}^3x{T} (nev {nev})" for L, T, nev, _ in cfg["mixed"]) + " in one batch"
+    elif cfg.get("scan"):
+        a1 = sorted({round(a, 6) for a, _ in cfg["scan"]})
+        a2 = sorted({round(b, 6) for _, b in cfg["scan"]})
+        shape = (f"{cfg['L']}^3 timeslice 0 x {len(cfg['scan'])} HYP (alpha_1, alpha_2) grid points "
+                 f"(alpha_1 {a1[0]}..{a1[-1]}, alpha_2 {a2[0]}..{a2[-1]}, step 0.05) in one batch, nev {cfg['nev']}")
     elif cfg.get("wave"):
         shape = f"{cfg['L']}^3x{cfg['T']} in waves of {cfg['wave']} timeslices (one wave per step), nev {cfg['nev']}"
     else:

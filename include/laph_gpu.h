@@ -229,6 +229,12 @@ int laph_solver_features(laph_solver* s, float* feats, double* bound);
 /* All k Ritz values of problem i after the last run (k returned). */
 int laph_solver_ritz(laph_solver* s, int i, double* theta, int* k);
 
+/* Smearing parameters of problem i (p1, p2 as in laph_solve_opts), replacing
+ * the options' for that problem only: a batch of copies of one timeslice with
+ * different parameters is the batched form of tune_hyp's (alpha_1, alpha_2)
+ * scan (src/tune_hyp.cpp:116-255).  Kind and iterations stay global. */
+int laph_solver_set_smear(laph_solver* s, int i, double p1, double p2);
+
 /* ---- source shape (the reference's sourceshape program) ------------------
  * psi(r) = sum_x || V_{x+r} V_x^dag ||_F over the grid r_i = 0, 2, ..., L-2,
  * V_y the 3 x nev block of rows 3y .. 3y+2 of the eigensystem: replaces
@@ -302,6 +308,7 @@ typedef struct {
   double tol;           /* residual target                                             */
   int guard, block, window, solver; /* solver: 0 = block (default), 1 = plain MatShell */
   int V3, MAT_ENTRIES, V_TS;
+  double alpha_1_i, alpha_1_f, alpha_2_i, alpha_2_f; /* tune_hyp scan range (par_io.cpp:75-89) */
 } laph_config;
 int laph_parse_parameters(const char* path, laph_config* cfg);
 

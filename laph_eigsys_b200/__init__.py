@@ -14,9 +14,10 @@ from . import _lib
 from ._lib import (LAYOUT_CONF, LAYOUT_EIGEN, LAYOUT_ROWMAJOR, LINKS_BF16, LINKS_FP32, SMEAR_APE, SMEAR_HYP,
                    SMEAR_NONE, SMEAR_STOUT, WINDOW_FIXED, WINDOW_LANCZOS, WINDOW_MLP, LaphError, check, lib)
 
-__all__ = ["Context", "Solver", "gauge_random", "lime_write_gauge", "lime_read_gauge", "parse_parameters",
-           "lime_read_gauge_any", "lime_info", "sourceshape", "sourceshape_avg", "write_sourceshape", "check_trace", "fix_phase", "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin",
-           "read_eigsys_bin", "read_eigenvalues_bin", "LaphError", "lib"]
+__all__ = ["Context", "Solver", "gauge_random", "lime_write_gauge", "lime_read_gauge", "lime_read_gauge_any",
+           "lime_info", "parse_parameters", "sourceshape", "sourceshape_avg", "write_sourceshape", "check_trace",
+           "fix_phase", "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin", "read_eigsys_bin",
+           "read_eigenvalues_bin", "LaphError", "lib"]
 
 
 def _ptr(a):
@@ -321,6 +322,10 @@ class Solver:
         t = (ctypes.c_double * 4)()
         check(lib.laph_solver_timings(self._h, t), "laph_solver_timings")
         return list(t)
+
+    def set_smear(self, i, p1, p2=0.0):
+        """Smearing parameters of problem i only (the batched tune_hyp scan)."""
+        check(lib.laph_solver_set_smear(self._h, i, p1, p2), "laph_solver_set_smear")
 
     def sourceshape(self, i, weighted=False):
         """psi(r) of problem i's eigenvectors, computed on the device from the solver's own block."""

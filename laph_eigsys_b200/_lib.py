@@ -56,7 +56,8 @@ class laph_config(ctypes.Structure):
                 ("OMP_THRDS", c_int), ("alpha_1", c_double), ("alpha_2", c_double), ("LAM_L", c_double),
                 ("LAM_C", c_double), ("smear", c_int), ("rho", c_double), ("alpha", c_double),
                 ("tol", c_double), ("guard", c_int), ("block", c_int), ("window", c_int), ("solver", c_int),
-                ("V3", c_int), ("MAT_ENTRIES", c_int), ("V_TS", c_int)]
+                ("V3", c_int), ("MAT_ENTRIES", c_int), ("V_TS", c_int), ("alpha_1_i", c_double),
+                ("alpha_1_f", c_double), ("alpha_2_i", c_double), ("alpha_2_f", c_double)]
 
 
 def _sig(name, res, *args):
@@ -105,6 +106,7 @@ _sig("laph_lime_info", c_int, c_char_p, P(c_int), P(c_int), P(c_int), P(c_int), 
 _sig("laph_lime_write_gauge_prec", c_int, c_char_p, c_void_p, c_int, c_int, c_int)
 _sig("laph_sourceshape", c_int, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int)
 _sig("laph_solver_sourceshape", c_int, c_void_p, c_int, c_int, c_void_p)
+_sig("laph_solver_set_smear", c_int, c_void_p, c_int, c_double, c_double)
 _sig("laph_sourceshape_avg", c_int, c_int, c_void_p, c_void_p, c_void_p, P(c_int))
 _sig("laph_write_sourceshape", c_int, c_char_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p)
 _sig("laph_write_eigsys_bin", c_int, c_char_p, c_char_p, c_int, c_int, c_int, c_int, c_void_p)

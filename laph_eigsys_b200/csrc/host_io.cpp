@@ -755,6 +755,10 @@ int laph_parse_parameters(const char* path, laph_config* cfg) {
   cfg->V3 = cfg->LX * cfg->LX * cfg->LX;
   cfg->MAT_ENTRIES = 3 * cfg->V3;
   cfg->V_TS = cfg->V3 * 72;
+  cfg->alpha_1_i = F("alpha_1_i", 0.0);
+  cfg->alpha_1_f = F("alpha_1_f", 0.0);
+  cfg->alpha_2_i = F("alpha_2_i", 0.0);
+  cfg->alpha_2_f = F("alpha_2_f", 0.0);
   return LAPH_OK;
 }
 

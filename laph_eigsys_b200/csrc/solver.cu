@@ -72,6 +72,7 @@ struct laph_solver {
   unsigned long long* tstamp = nullptr;  // [np][kSmallPhases] phase boundaries of the small dense step
   size_t blk_total = 0;
   std::vector<int> links_set;
+  std::vector<double> sp1, sp2;  // per-problem smearing parameters (opts' by default)
   std::vector<int> degs;  // filter degree of each pass of the last run
   double ms[4] = {0, 0, 0, 0};
   long long cnt[3] = {0, 0, 0};
@@ -287,6 +288,8 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   cudaEventCreate(&s->ev1);
   cudaEventCreate(&s->ev2);
   s->links_set.assign(n, 0);
+  s->sp1.assign(n, opts->smear_p1);
+  s->sp2.assign(n, opts->smear_p2);
   s->hps.assign(n, ProbState{});
   *out = s;
   return LAPH_OK;
@@ -413,12 +416,12 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   long long nlaunch = 0;
   LAPH_CUDA_TRY(cudaMemcpyAsync(s->U64, s->U64raw, s->hd.back().u64 * sizeof(double2) + 27 * sizeof(double2) * s->hd.back().V3,
                                 cudaMemcpyDeviceToDevice, s->st));
-  // smearing, per run of equal L
+  // smearing, per run of consecutive problems with equal L and parameters
   for (int i = 0; i < s->np;) {
     int j = i;
-    while (j < s->np && s->hd[j].L == s->hd[i].L) ++j;
-    LAPH_TRY(smear_batch(s->U64 + s->hd[i].u64, s->Utmp, s->dec, s->hd[i].L, j - i, o.smear_kind, o.smear_p1,
-                         o.smear_p2, o.smear_iters, o.smear_compat, s->st));
+    while (j < s->np && s->hd[j].L == s->hd[i].L && s->sp1[j] == s->sp1[i] && s->sp2[j] == s->sp2[i]) ++j;
+    LAPH_TRY(smear_batch(s->U64 + s->hd[i].u64, s->Utmp, s->dec, s->hd[i].L, j - i, o.smear_kind, s->sp1[i],
+                         s->sp2[i], o.smear_iters, o.smear_compat, s->st));
     if (o.smear_kind != LAPH_SMEAR_NONE) nlaunch += (long long)o.smear_iters * (o.smear_kind == LAPH_SMEAR_HYP ? 2 : 1);
     i = j;
   }
@@ -651,6 +654,16 @@ int laph_solver_stream(laph_solver* s, void** stream) {
 int laph_solver_timings(laph_solver* s, double* ms4) {
   if (!s || !ms4) return LAPH_EINVAL;
   for (int i = 0; i < 4; ++i) ms4[i] = s->ms[i];
+  return LAPH_OK;
+}
+
+int laph_solver_set_smear(laph_solver* s, int i, double p1, double p2) {
+  if (!s || i < 0 || i >= s->np || !std::isfinite(p1) || !std::isfinite(p2)) {
+    set_error("laph_solver_set_smear: bad argument");
+    return LAPH_EINVAL;
+  }
+  s->sp1[i] = p1;
+  s->sp2[i] = p2;
   return LAPH_OK;
 }
 

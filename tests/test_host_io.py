@@ -113,12 +113,14 @@ def test_parameters_parser_quirks(tmp_path):
     p = tmp_path / "parameters.txt"
     p.write_text("# comment\nconfig_path = /gauges\nLT = 48\nLX = 24\nNEV = 120\nalpha_1 = 0.62\n"
                  "alpha_2 = 0.52\niter = 3\nLAM_L = 11.8\nLAM_C = 0.6\nDEG = 8\nOMP_THRDS = 2\n"
+                 "alpha_1_i = 0.4\nalpha_1_f = 0.7\nalpha_2_i = 0.3\nalpha_2_f = 0.6\n"
                  "LT=99\nsmear = stout\nDEG = 12")  # unterminated last line is dropped
     c = lb.parse_parameters(p)
     assert c["config_path"] == "/gauges" and c["LT"] == 48 and c["LX"] == 24 and c["NEV"] == 120
     assert c["DEG"] == 8 and c["iter"] == 3 and abs(c["LAM_L"] - 11.8) < 1e-15
     assert c["V3"] == 24 ** 3 and c["MAT_ENTRIES"] == 3 * 24 ** 3 and c["V_TS"] == 72 * 24 ** 3
     assert c["smear"] == lb.SMEAR_STOUT
+    assert (c["alpha_1_i"], c["alpha_1_f"], c["alpha_2_i"], c["alpha_2_f"]) == (0.4, 0.7, 0.3, 0.6)
     p.write_text("LT = 4\n\nLX = 4\n")
     with pytest.raises(lb.LaphError) as e:
         lb.parse_parameters(p)
