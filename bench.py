@@ -296,6 +296,31 @@ def sourceshape_flops(L, nev):
     return 8 * (t * (t + 1) // 2) * 32 * 32 * 9 * nev * 8.0
 
 
+def measure_displacement(solver, stream, batch, reps=4):
+    """Covariant displacement of the solved eigenvectors along x, y, z in place on the device (CUDA events on the
+    solver's stream); HBM roofline: 48 B read + 48 B written per site and eigenvector plus the forward links."""
+    import torch
+    L, nev, _ = batch[0]
+    n = min(reps, len(batch))
+    W = torch.empty(3 * L ** 3 * nev, dtype=torch.complex128, device="cuda")
+    solver.displace_device(0, 0, W.data_ptr())  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(n):
+        for d in range(3):
+            solver.displace_device(i, d, W.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (3 * n)
+    byts = L ** 3 * nev * 96.0 + L ** 3 * 144.0 * ((nev + 15) // 16)
+    hbm, src = peaks()
+    del W
+    return {"workload": f"{L}^3 x nev {nev} eigenvectors, one direction per launch, FP64", "ms_per_launch": ms,
+            "bytes_per_launch": byts, "achieved_gbs": byts / (ms / 1e3) / 1e9, "peak_gbs": hbm, "peak_source": src,
+            "frac": byts / (ms / 1e3) / 1e9 / hbm, "launches": 3 * n}
+
+
 def measure_sourceshape(solver, stream, batch, no_cpu, reps=4):
     """psi(r) of the first solved timeslices in place on the device (CUDA events on the solver's stream), and the
     oracle's restatement on one 16^3 eigensystem beside the device kernel on the same input."""
@@ -501,9 +526,10 @@ def main():
         plain["chosen_over_plain"] = value / plain["value"] if plain.get("value") else None
 
     # ---- source shape of the solved eigenvectors (next row of the path) ------
-    shape = None
+    shape = disp = None
     if rank == 0 and world == 1 and not args.no_shape and all(L_ % 2 == 0 for L_, _, _ in batch):
         shape = measure_sourceshape(solver, stream, batch, args.no_cpu)
+        disp = measure_displacement(solver, stream, batch)
 
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
     cpu = None
@@ -524,7 +550,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
                 "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-                "sourceshape": shape,
+                "sourceshape": shape, "displacement": disp,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid, "filter_ms_per_step": filt_ms / args.steps,
                            "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
                                                        solver.timings()))}}

@@ -235,6 +235,17 @@ int laph_solver_ritz(laph_solver* s, int i, double* theta, int* k);
  * scan (src/tune_hyp.cpp:116-255).  Kind and iterations stay global. */
 int laph_solver_set_smear(laph_solver* s, int i, double p1, double p2);
 
+/* ---- covariant displacement ---------------------------------------------
+ * W_i(x) = 1/2 (U_dir(x) V_i(x+dir) - U_dir(x-dir)^dag V_i(x-dir)) for every
+ * column of V (column-major complex128 [3 V3][nev], index 3 site + colour),
+ * dir 0/1/2 = x/y/z: right_displacement_one_dir (modules/config_utils.cpp:
+ * 344-382), FP64 on the device.  laph_displace uses a context's current
+ * (smeared) links and host or device V/W (must not overlap); laph_solver_displace
+ * displaces problem i's phase-fixed eigenvectors with its smeared links, in
+ * place on the device, W to host or device memory. */
+int laph_displace(laph_ctx* ctx, int dir, const double* V, double* W, int nev, int on_device);
+int laph_solver_displace(laph_solver* s, int i, int dir, double* W, int on_device);
+
 /* ---- source shape (the reference's sourceshape program) ------------------
  * psi(r) = sum_x || V_{x+r} V_x^dag ||_F over the grid r_i = 0, 2, ..., L-2,
  * V_y the 3 x nev block of rows 3y .. 3y+2 of the eigensystem: replaces

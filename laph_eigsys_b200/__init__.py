@@ -246,6 +246,14 @@ class Context:
             check(st, "laph_eps_solve")
         return st, theta, V, nconv.value, its.value, nmv.value
 
+    def displace(self, V, direction):
+        """Covariant displacement of the columns of V along direction 0/1/2 with this context's links."""
+        V = np.asfortranarray(V, dtype=np.complex128)
+        W = np.empty_like(V, order="F")
+        check(lib.laph_displace(self._h, direction, ctypes.c_void_p(V.ctypes.data), ctypes.c_void_p(W.ctypes.data),
+                                V.shape[1], 0), "laph_displace")
+        return W
+
     def plaquette(self):
         p = ctypes.c_double()
         check(lib.laph_plaquette(self._h, ctypes.byref(p)), "laph_plaquette")
@@ -322,6 +330,18 @@ class Solver:
         t = (ctypes.c_double * 4)()
         check(lib.laph_solver_timings(self._h, t), "laph_solver_timings")
         return list(t)
+
+    def displace(self, i, direction):
+        """Covariant displacement of problem i's eigenvectors along direction 0/1/2 (device, FP64)."""
+        L, nev = self.problems[i]
+        W = np.empty((3 * L ** 3, nev), dtype=np.complex128, order="F")
+        check(lib.laph_solver_displace(self._h, i, direction, ctypes.c_void_p(W.ctypes.data), 0),
+              "laph_solver_displace")
+        return W
+
+    def displace_device(self, i, direction, ptr):
+        """As displace(), writing [3 V3][nev] complex128 to device memory at ptr."""
+        check(lib.laph_solver_displace(self._h, i, direction, ctypes.c_void_p(ptr), 1), "laph_solver_displace")
 
     def set_smear(self, i, p1, p2=0.0):
         """Smearing parameters of problem i only (the batched tune_hyp scan)."""

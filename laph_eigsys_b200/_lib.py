@@ -107,6 +107,8 @@ _sig("laph_lime_write_gauge_prec", c_int, c_char_p, c_void_p, c_int, c_int, c_in
 _sig("laph_sourceshape", c_int, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int)
 _sig("laph_solver_sourceshape", c_int, c_void_p, c_int, c_int, c_void_p)
 _sig("laph_solver_set_smear", c_int, c_void_p, c_int, c_double, c_double)
+_sig("laph_displace", c_int, c_void_p, c_int, c_void_p, c_void_p, c_int, c_int)
+_sig("laph_solver_displace", c_int, c_void_p, c_int, c_int, c_void_p, c_int)
 _sig("laph_sourceshape_avg", c_int, c_int, c_void_p, c_void_p, c_void_p, P(c_int))
 _sig("laph_write_sourceshape", c_int, c_char_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p)
 _sig("laph_write_eigsys_bin", c_int, c_char_p, c_char_p, c_int, c_int, c_int, c_int, c_void_p)

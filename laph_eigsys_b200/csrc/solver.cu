@@ -38,6 +38,8 @@
 #include "smear.cuh"
 
 namespace laph {
+int displace_device(const double2* U, int L, int dir, int nev, long long ldv, const double2* V, double2* W,
+                    cudaStream_t st);
 int sourceshape_device(const double2* V, int L, int nev, const double* evals, double2* work, double* psi,
                        cudaStream_t st);
 }
@@ -681,6 +683,22 @@ int laph_solver_sourceshape(laph_solver* s, int i, int weighted, double* psi) {
   LAPH_TRY(sourceshape_device(s->V + d.blk, d.L, d.nev, weighted ? s->theta + d.kv : nullptr, s->W + d.blk, dpsi,
                               s->st));
   LAPH_CUDA_TRY(cudaMemcpyAsync(psi, dpsi, sizeof(double) * Nc, cudaMemcpyDeviceToHost, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return LAPH_OK;
+}
+
+int laph_solver_displace(laph_solver* s, int i, int dir, double* W, int on_device) {
+  if (!s || i < 0 || i >= s->np || !s->ran || !W || dir < 0 || dir > 2) {
+    set_error("laph_solver_displace: bad argument or solver not run");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  const ProbDesc& d = s->hd[i];
+  // host output goes through this problem's filtered block W, free after the run
+  double2* out = on_device ? reinterpret_cast<double2*>(W) : s->W + d.blk;
+  LAPH_TRY(displace_device(s->U64 + d.u64, d.L, dir, d.nev, d.dim, s->V + d.blk, out, s->st));
+  if (!on_device)
+    LAPH_CUDA_TRY(cudaMemcpyAsync(W, out, sizeof(double2) * d.dim * d.nev, cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
   return LAPH_OK;
 }

@@ -52,6 +52,7 @@ _sig("orc_fix_phase", None, _i, _i, _vp, _vp, _vp)
 _sig("orc_build_neglap_dense", None, _vp, _i, _vp)
 _sig("orc_mlp_loss_grad", _d, _vp, _vp, _vp, _i, _vp)
 _sig("orc_sourceshape", None, _vp, _i, _i, _vp)
+_sig("orc_displace", None, _vp, _i, _i, _vp, _i, _vp)
 _sig("orc_sourceshape_avg", _i, _i, _vp, _vp, _vp)
 
 
@@ -175,6 +176,15 @@ def neglap_dense(U, L):
     A = np.zeros((dim, dim), dtype=np.complex128)
     _lib.orc_build_neglap_dense(_p(U), L, _p(A))
     return A
+
+
+def displace(U, L, direction, V):
+    """right_displacement_one_dir: W = (U V(x+dir) - U(x-dir)^dag V(x-dir)) / 2 for every column."""
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    V = np.asfortranarray(V, dtype=np.complex128)
+    W = np.empty_like(V, order="F")
+    _lib.orc_displace(_p(U), L, direction, ctypes.c_void_p(V.ctypes.data), V.shape[1], ctypes.c_void_p(W.ctypes.data))
+    return W
 
 
 def sourceshape(V, L):

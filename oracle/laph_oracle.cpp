@@ -753,6 +753,30 @@ double orc_mlp_loss_grad(const double* P, const double* X, const double* Y, int 
   return loss / (n * O);
 }
 
+// right_displacement_one_dir (modules/config_utils.cpp:344-382):
+// W_i(x) = 1/2 (U_dir(x) V_i(x+dir) - U_dir(x-dir)^dag V_i(x-dir)).
+void orc_displace(const double* links3, int L, int dir, const double* Vd, int nev, double* Wd) {
+  const cd* V = reinterpret_cast<const cd*>(Vd);
+  cd* W = reinterpret_cast<cd*>(Wd);
+  const long long V3 = (long long)L * L * L, dim = 3 * V3;
+  const Geo nav(L);
+#pragma omp parallel for schedule(static)
+  for (long long s = 0; s < V3; ++s) {
+    const int up = nav.up((int)s, dir), dn = nav.dn((int)s, dir);
+    const M3 U = load(links3 + ((size_t)s * 3 + dir) * 18);
+    const M3 Ud = adj(load(links3 + ((size_t)dn * 3 + dir) * 18));
+    for (int n = 0; n < nev; ++n)
+      for (int a = 0; a < 3; ++a) {
+        cd f = 0.0, b = 0.0;
+        for (int c = 0; c < 3; ++c) {
+          f += U.m[3 * a + c] * V[3 * up + c + n * dim];
+          b += Ud.m[3 * a + c] * V[3 * dn + c + n * dim];
+        }
+        W[3 * s + a + n * dim] = 0.5 * (f - b);
+      }
+  }
+}
+
 // source_shape_complete (modules/sourceshape_funcs.cpp:58-81) with dll_op
 // (:30-55) and get_vectorial_dst_ind (:11-27): for r = (r1, r2, r3) on the grid
 // r_i = 0, 2, ... < L (r1 outer, r3 inner), psi(r) = sum over sites x of

@@ -86,6 +86,10 @@ void orc_fix_phase(int dim, int nev, const double* V, double* Vfix, double* phas
  * modules/config_utils.cpp:18-58), complex128 row-major [dim][dim]. */
 void orc_build_neglap_dense(const double* links3, int L, double* A);
 
+/* right_displacement_one_dir (modules/config_utils.cpp:344-382) on the
+ * column-major complex128 block V [3*V3][nev] -> W, links3 as above. */
+void orc_displace(const double* links3, int L, int dir, const double* V, int nev, double* W);
+
 /* Source shape psi(r) (modules/sourceshape_funcs.cpp:30-81) on the grid
  * r_i = 0, 2, ... < L, r1 outer and r3 inner: psi[(L+1)/2 cubed].  V is the
  * column-major complex128 eigensystem [3*V3][nev]. */
