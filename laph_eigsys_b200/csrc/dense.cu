@@ -618,8 +618,8 @@ __global__ void __launch_bounds__(128) k_residual64(const ProbDesc* __restrict__
       double2 xu[3], xd[3];
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        xu[b] = __ldg(x + 3 * (size_t)u + b);
-        xd[b] = __ldg(x + 3 * (size_t)dn + b);
+        xu[b] = __ldg(x + (size_t)b * d.V3 + u);
+        xd[b] = __ldg(x + (size_t)b * d.V3 + dn);
       }
 #pragma unroll
       for (int a = 0; a < 3; ++a)
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(128) k_residual64(const ProbDesc* __restrict__
     const double sc = -2.0 * ps[p].c_hop;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const double2 xs = __ldg(x + 3 * (size_t)s + a);
+      const double2 xs = __ldg(x + (size_t)a * d.V3 + s);
       const double2 r = make_double2((6.0 - th) * xs.x - acc[a].x, (6.0 - th) * xs.y - acc[a].y);
       rr += r.x * r.x + r.y * r.y;
       Sp[col + (size_t)a * d.V3 + s] = make_float2((float)(sc * r.x), (float)(sc * r.y));  // colour-major
@@ -735,7 +735,22 @@ __global__ void k_phase_fix(const ProbDesc* __restrict__ pd, const int* __restri
   }
 }
 
+// --------------------------------------------------------------- output ---
+// Colour-major columns (c*V3 + site) -> the reference's 3*site + colour order.
+__global__ void k_to_reference(const double2* __restrict__ in, double2* __restrict__ out, int V3, int nev) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= V3) return;
+  const size_t col = (size_t)blockIdx.y * 3 * V3;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[col + 3 * (size_t)s + c] = __ldg(in + col + (size_t)c * V3 + s);
+}
+
 // ------------------------------------------------------------- launchers ---
+int to_reference(const double2* in, double2* out, int V3, int nev, cudaStream_t st) {
+  k_to_reference<<<dim3((V3 + 255) / 256, nev), 256, 0, st>>>(in, out, V3, nev);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
 int dense_init() {
   LAPH_CUDA_TRY(cudaFuncSetAttribute(k_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, kGramSmem));
   LAPH_CUDA_TRY(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, kRotSmem));

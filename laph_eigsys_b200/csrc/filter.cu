@@ -10,9 +10,10 @@
 // 3 backward links U_mu(x-mu)) are read from HBM once per kb vectors and held
 // in 108 registers; the vector reads of consecutive threads are consecutive
 // site values (fully coalesced), neighbour reuse comes from L1/L2.  Inside
-// each column the FP32 buffers (S and the E ring) are colour-major,
+// each column the blocks (FP32 S and E ring, FP64 V, W, Y) are colour-major,
 // element (site, c) at c*V3 + site, so every warp load is one dense 256-byte
-// access; the FP64 blocks keep the reference's 3*site + colour order.
+// (FP32) or 512-byte (FP64) access; the solver converts to the reference's
+// 3*site + colour order only on output.
 // Per-column coefficients (a_j, z_j, g_j) come from a device table written by
 // the Rayleigh-Ritz step, so every launch of an iteration is identical.
 // Algorithmic bytes per site and vector: 24 (X) + 24 (S) + 24 (Z) + 24 (Y)
@@ -91,9 +92,9 @@ __global__ void __launch_bounds__(128, 3)
   if (FINAL) {
     // locked columns: W_j = V_j
     for (int j = cb * kb; j < min(j1, nlock); ++j) {
-      const size_t i = (size_t)d.blk + (size_t)j * d.dim + 3 * (size_t)s;
+      const size_t i = (size_t)d.blk + (size_t)j * d.dim + s;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) Wp[i + a] = __ldg(Vp + i + a);
+      for (int a = 0; a < 3; ++a) Wp[i + (size_t)a * d.V3] = __ldg(Vp + i + (size_t)a * d.V3);
     }
   }
   const int j0 = max(cb * kb, nlock);
@@ -138,7 +139,9 @@ __global__ void __launch_bounds__(128, 3)
       l2_prefetch(Sp + col + (size_t)c * d.V3 + s0, bytes);
       if (HAS_Z) l2_prefetch(Zp + col + (size_t)c * d.V3 + s0, bytes);
     }
-    if (FINAL) l2_prefetch(Vp + col + 3 * (size_t)s0, 6 * bytes);
+    if (FINAL)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) l2_prefetch(Vp + col + (size_t)c * d.V3 + s0, 2 * bytes);
   };
 #pragma unroll 1
   for (int j = j0; j < min(j1, j0 + kPrefetch); ++j) prefetch(j);
@@ -182,9 +185,9 @@ __global__ void __launch_bounds__(128, 3)
         r.y = fmaf(zc, zz.y, r.y);
       }
       if (FINAL) {
-        // W = T_m(theta_B) V + E_m in FP64 (FP64 blocks keep the 3*site + colour order)
+        // W = T_m(theta_B) V + E_m in FP64 (FP64 blocks are colour-major too)
         const double tm = __ldg(tc + (size_t)3 * d.k + j);
-        const size_t iv = col + 3 * (size_t)s + a;
+        const size_t iv = col + (size_t)a * d.V3 + s;
         const double2 v = __ldg(Vp + iv);
         Wp[iv] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
       } else {
@@ -225,9 +228,9 @@ __global__ void __launch_bounds__(128, 3)
   const int nlock = ps[p].nlock;
   if (FINAL && valid) {
     for (int j = cb * kb; j < min(j1, nlock); ++j) {
-      const size_t i = (size_t)d.blk + (size_t)j * d.dim + 3 * (size_t)s;
+      const size_t i = (size_t)d.blk + (size_t)j * d.dim + s;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) Wp[i + a] = __ldg(Vp + i + a);
+      for (int a = 0; a < 3; ++a) Wp[i + (size_t)a * d.V3] = __ldg(Vp + i + (size_t)a * d.V3);
     }
   }
   const int j0 = max(cb * kb, nlock);
@@ -277,7 +280,9 @@ __global__ void __launch_bounds__(128, 3)
       l2_prefetch(Sp + col + (size_t)c * d.V3 + s0, bytes);
       if (HAS_Z) l2_prefetch(Zp + col + (size_t)c * d.V3 + s0, bytes);
     }
-    if (FINAL) l2_prefetch(Vp + col + 3 * (size_t)s0, 6 * bytes);
+    if (FINAL)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) l2_prefetch(Vp + col + (size_t)c * d.V3 + s0, 2 * bytes);
   };
   auto fetch = [&](int j, ChebCol& c) {
     const size_t col = base + (size_t)j * d.dim;
@@ -319,7 +324,7 @@ __global__ void __launch_bounds__(128, 3)
         r.y = fmaf(q.z, c.zz[a].y, r.y);
       }
       if (FINAL) {
-        const size_t iv = col + 3 * (size_t)s + a;
+        const size_t iv = col + (size_t)a * d.V3 + s;
         const double2 v = __ldg(Vp + iv);
         const double tm = ctm[j - j0];
         Wp[iv] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
@@ -366,8 +371,8 @@ __global__ void __launch_bounds__(128) k_neglap64_batch(const ProbDesc* __restri
     double2 xu[3], xd[3];
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
-      xu[b] = __ldg(x + 3 * (size_t)u + b);
-      xd[b] = __ldg(x + 3 * (size_t)dn + b);
+      xu[b] = __ldg(x + (size_t)b * d.V3 + u);
+      xd[b] = __ldg(x + (size_t)b * d.V3 + dn);
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -379,8 +384,8 @@ __global__ void __launch_bounds__(128) k_neglap64_batch(const ProbDesc* __restri
   }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const double2 xs = __ldg(x + 3 * (size_t)s + a);
-    Yp[col + 3 * (size_t)s + a] = make_double2(6.0 * xs.x - acc[a].x, 6.0 * xs.y - acc[a].y);
+    const double2 xs = __ldg(x + (size_t)a * d.V3 + s);
+    Yp[col + (size_t)a * d.V3 + s] = make_double2(6.0 * xs.x - acc[a].x, 6.0 * xs.y - acc[a].y);
   }
 }
 

@@ -599,8 +599,15 @@ int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double*
     for (auto& v : th) v = -v;  // eigenvalues of Delta (recover_spectrum convention)
     LAPH_CUDA_TRY(cudaMemcpy(evals, th.data(), d.nev * sizeof(double), on_device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost));
   }
-  if (evecs)
-    LAPH_CUDA_TRY(cudaMemcpyAsync(evecs, s->V + d.blk, (size_t)d.dim * d.nev * sizeof(double2), kd, s->st));
+  if (evecs) {
+    // the block is colour-major on the device; the caller gets 3*site + colour
+    if (on_device) {
+      LAPH_TRY(to_reference(s->V + d.blk, reinterpret_cast<double2*>(evecs), d.V3, d.nev, s->st));
+    } else {
+      LAPH_TRY(to_reference(s->V + d.blk, s->W + d.blk, d.V3, d.nev, s->st));
+      LAPH_CUDA_TRY(cudaMemcpyAsync(evecs, s->W + d.blk, (size_t)d.dim * d.nev * sizeof(double2), kd, s->st));
+    }
+  }
   if (phases) LAPH_CUDA_TRY(cudaMemcpyAsync(phases, s->phases + d.kv, d.nev * sizeof(double), kd, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
   return LAPH_OK;
@@ -677,10 +684,11 @@ int laph_solver_sourceshape(laph_solver* s, int i, int weighted, double* psi) {
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const ProbDesc& d = s->hd[i];
   const int H = d.L / 2, Nc = H * H * H;
-  // scratch: the filtered block W (class-major copy of V) and Y (psi bins) of this
-  // problem, both free once the run has finished and rewritten by the next run
-  double* dpsi = reinterpret_cast<double*>(s->Y + d.blk);
-  LAPH_TRY(sourceshape_device(s->V + d.blk, d.L, d.nev, weighted ? s->theta + d.kv : nullptr, s->W + d.blk, dpsi,
+  // scratch, all free once the run has finished and rewritten by the next run:
+  // Y (V in 3*site + colour order), W (its class-major copy), E0 (psi bins)
+  double* dpsi = reinterpret_cast<double*>(s->E[0] + d.blk);
+  LAPH_TRY(to_reference(s->V + d.blk, s->Y + d.blk, d.V3, d.nev, s->st));
+  LAPH_TRY(sourceshape_device(s->Y + d.blk, d.L, d.nev, weighted ? s->theta + d.kv : nullptr, s->W + d.blk, dpsi,
                               s->st));
   LAPH_CUDA_TRY(cudaMemcpyAsync(psi, dpsi, sizeof(double) * Nc, cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
@@ -694,9 +702,10 @@ int laph_solver_displace(laph_solver* s, int i, int dir, double* W, int on_devic
   }
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const ProbDesc& d = s->hd[i];
-  // host output goes through this problem's filtered block W, free after the run
+  // V goes through Y (reference order) and host output through W, both free after the run
   double2* out = on_device ? reinterpret_cast<double2*>(W) : s->W + d.blk;
-  LAPH_TRY(displace_device(s->U64 + d.u64, d.L, dir, d.nev, d.dim, s->V + d.blk, out, s->st));
+  LAPH_TRY(to_reference(s->V + d.blk, s->Y + d.blk, d.V3, d.nev, s->st));
+  LAPH_TRY(displace_device(s->U64 + d.u64, d.L, dir, d.nev, d.dim, s->Y + d.blk, out, s->st));
   if (!on_device)
     LAPH_CUDA_TRY(cudaMemcpyAsync(W, out, sizeof(double2) * d.dim * d.nev, cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
