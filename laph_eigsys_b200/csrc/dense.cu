@@ -735,6 +735,31 @@ __global__ void k_phase_fix(const ProbDesc* __restrict__ pd, const int* __restri
   }
 }
 
+// ---------------------------------------------------------- start window --
+// State of a random start block used without a first Rayleigh-Ritz (window
+// from the learned model or fixed): every column gets the Ritz value lam_max,
+// where T_n(theta_B) = (-1)^n, so the first filter pass runs entirely through
+// the FP32 correction E = T_m(B) V - V T_m(theta_B) (accurate to FP32, which
+// is all a first pass needs); the window is the one already in the state.
+__global__ void k_start_window(const ProbDesc* __restrict__ pd, ProbState* __restrict__ ps, int np,
+                               double* __restrict__ theta) {
+  const int p = blockIdx.x;
+  if (p >= np) return;
+  const ProbDesc d = pd[p];
+  ProbState& S = ps[p];
+  for (int j = threadIdx.x; j < d.k; j += blockDim.x) theta[d.kv + j] = S.lam_max;
+  if (threadIdx.x == 0) {
+    double cut = S.lam_cut;
+    if (cut >= S.lam_max - 1e-3) cut = S.lam_max - 1e-3;
+    if (cut < 1e-6) cut = 1e-6;
+    S.lam_cut = cut;
+    S.c_hop = 2.0 / (S.lam_max - cut);
+    S.c_diag = (S.lam_max + cut - 12.0) / (S.lam_max - cut);
+    S.chol_fail = 0;
+    S.theta_min = S.lam_max;
+  }
+}
+
 // --------------------------------------------------------------- output ---
 // Colour-major columns (c*V3 + site) -> the reference's 3*site + colour order.
 __global__ void k_to_reference(const double2* __restrict__ in, double2* __restrict__ out, int V3, int nev) {
@@ -746,6 +771,11 @@ __global__ void k_to_reference(const double2* __restrict__ in, double2* __restri
 }
 
 // ------------------------------------------------------------- launchers ---
+int start_window(const ProbDesc* pd, ProbState* ps, int np, double* theta, cudaStream_t st) {
+  k_start_window<<<np, 256, 0, st>>>(pd, ps, np, theta);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
 int to_reference(const double2* in, double2* out, int V3, int nev, cudaStream_t st) {
   k_to_reference<<<dim3((V3 + 255) / 256, nev), 256, 0, st>>>(in, out, V3, nev);
   LAPH_CUDA_TRY(cudaGetLastError());

@@ -26,6 +26,9 @@ int residual64(const ProbDesc* pd, const ProbState* ps, const int* start, int np
                const double2* V, const double* theta, float2* S, double* rpart, cudaStream_t st);
 int resid_check(const ProbDesc* pd, ProbState* ps, int np, const double* rpart, double* resid, double tol,
                 int* n_active, cudaStream_t st);
+// Ritz values lam_max and filter map of the state's window for a start block that
+// skips the first Rayleigh-Ritz.
+int start_window(const ProbDesc* pd, ProbState* ps, int np, double* theta, cudaStream_t st);
 // nev colour-major columns of 3*V3 -> 3*site + colour order (out must not overlap in).
 int to_reference(const double2* in, double2* out, int V3, int nev, cudaStream_t st);
 int phase_fix(const ProbDesc* pd, const int* start, int np, int nblk, double2* V, double* phases, double* norms,

@@ -463,10 +463,24 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
       nlaunch += 3;
     }
   }
-  LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->W, o.seed, s->st));
-  LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
-  LAPH_TRY(iteration_rr(s, 1));
-  nlaunch += 2 + 7;  // pack, random block, first Rayleigh-Ritz
+  // With the window known before any Ritz value (learned or fixed), the random
+  // block goes straight into the first filter pass; otherwise a first
+  // Rayleigh-Ritz of the random block sets the window.
+  const bool window_known = o.window == LAPH_WINDOW_MLP || (o.window == LAPH_WINDOW_FIXED && o.lam_cut > 0.0);
+  if (window_known) {
+    LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->V, o.seed, s->st));
+    LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
+    LAPH_TRY(start_window(s->d_pd, s->d_ps, s->np, s->theta, s->st));
+    LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
+    LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
+    LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
+    nlaunch += 2 + 4;  // pack, random block, window state, residual, check
+  } else {
+    LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->W, o.seed, s->st));
+    LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
+    LAPH_TRY(iteration_rr(s, 1));
+    nlaunch += 2 + 7;  // pack, random block, first Rayleigh-Ritz
+  }
   s->cnt[0] = s->cnt[1] = s->cnt[2] = 0;
   s->degs.clear();
   double filt_ms = 0.0;
