@@ -82,7 +82,11 @@ __device__ __forceinline__ void ffma2(unsigned long long& d, unsigned long long 
 }
 
 // ---------------------------------------------------------- the filter -----
-constexpr int kPrefetch = 6;
+// columns of lookahead of the L2 bulk prefetch
+#ifndef LAPH_PREFETCH_COLS
+#define LAPH_PREFETCH_COLS 4
+#endif
+constexpr int kPrefetch = LAPH_PREFETCH_COLS;
 // Bulk prefetch of [p, p+bytes) into L2 (16-byte aligned, bytes % 16 == 0).
 __device__ __forceinline__ void l2_prefetch(const void* p, unsigned bytes) {
   if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0 && (bytes & 15u) == 0 && bytes > 0)
