@@ -71,9 +71,9 @@ CONFIGS["c6"] = dict(L=32, T=16, eps=0.3, seed=1234, smear="hyp", p1=0.4, p2=0.4
                      guard=16, link_prec="fp32", tol=1e-9, deg=56, scan=hyp_scan_grid(0.4, 0.56, 0.4, 0.56))
 HBM_FALLBACK = 6650.0
 # DRAM bytes (read + write) of one k_cheb_mrhs2 launch over its algorithmic bytes, from an ncu capture of the same
-# kernel on 32^3 x 4 timeslices (2.134 GB / 2.155 GB); the filter's traffic grows with the site-vectors processed,
+# kernel on 32^3 x 4 timeslices (2.125 GB / 2.155 GB); the filter's traffic grows with the site-vectors processed,
 # so a bench launch's traffic is this ratio times its algorithmic bytes
-NCU_TRAFFIC_RATIO = 0.990
+NCU_TRAFFIC_RATIO = 0.986
 
 
 def peaks():

@@ -24,7 +24,7 @@ namespace {
 constexpr int kDispCols = 16;
 
 __global__ void __launch_bounds__(128) k_displace(const double2* __restrict__ U, int L, int dir, int nev, long long ldv,
-                                                  const double2* __restrict__ V, double2* __restrict__ W) {
+                                                  const double2* __restrict__ V, double2* __restrict__ W, int cm) {
   const Lat g{L, L * L, L * L * L};
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= g.V3) return;
@@ -43,8 +43,9 @@ __global__ void __launch_bounds__(128) k_displace(const double2* __restrict__ U,
     double2 vu[3], vd[3];
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
-      vu[b] = __ldg(v + 3 * (size_t)up + b);
-      vd[b] = __ldg(v + 3 * (size_t)dn + b);
+      // input 3*site + colour, or colour-major (cm: colour*V3 + site, the solver's own blocks)
+      vu[b] = __ldg(v + (cm ? (size_t)b * g.V3 + up : 3 * (size_t)up + b));
+      vd[b] = __ldg(v + (cm ? (size_t)b * g.V3 + dn : 3 * (size_t)dn + b));
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -62,11 +63,12 @@ __global__ void __launch_bounds__(128) k_displace(const double2* __restrict__ U,
 }  // namespace
 
 // W = displacement of V (device blocks, column stride ldv) along dir with site-minor FP64 links U.
-int displace_device(const double2* U, int L, int dir, int nev, long long ldv, const double2* V, double2* W,
+// cm: V colour-major (colour*V3 + site); W is always 3*site + colour.
+int displace_device(const double2* U, int L, int dir, int nev, long long ldv, const double2* V, double2* W, int cm,
                     cudaStream_t st) {
   const int V3 = L * L * L;
   const dim3 grid((V3 + 127) / 128, (nev + kDispCols - 1) / kDispCols);
-  k_displace<<<grid, 128, 0, st>>>(U, L, dir, nev, ldv, V, W);
+  k_displace<<<grid, 128, 0, st>>>(U, L, dir, nev, ldv, V, W, cm);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }
@@ -92,7 +94,7 @@ extern "C" int laph_displace(laph_ctx* ctx, int dir, const double* V, double* W,
       return LAPH_EINVAL;
     }
     LAPH_TRY(displace_device(U, L, dir, nev, dim, reinterpret_cast<const double2*>(V), reinterpret_cast<double2*>(W),
-                             st));
+                             0, st));
     LAPH_CUDA_TRY(cudaStreamSynchronize(st));
     return LAPH_OK;
   }
@@ -108,7 +110,7 @@ extern "C" int laph_displace(laph_ctx* ctx, int dir, const double* V, double* W,
   if (cudaMemcpyAsync(dV, V, sizeof(double2) * dim * nev, cudaMemcpyHostToDevice, st) != cudaSuccess) {
     rc = LAPH_ECUDA;
   } else {
-    rc = displace_device(U, L, dir, nev, dim, dV, dW, st);
+    rc = displace_device(U, L, dir, nev, dim, dV, dW, 0, st);
     if (rc == LAPH_OK && cudaMemcpyAsync(W, dW, sizeof(double2) * dim * nev, cudaMemcpyDeviceToHost, st) != cudaSuccess)
       rc = LAPH_ECUDA;
   }

@@ -38,9 +38,9 @@
 #include "smear.cuh"
 
 namespace laph {
-int displace_device(const double2* U, int L, int dir, int nev, long long ldv, const double2* V, double2* W,
+int displace_device(const double2* U, int L, int dir, int nev, long long ldv, const double2* V, double2* W, int cm,
                     cudaStream_t st);
-int sourceshape_device(const double2* V, int L, int nev, const double* evals, double2* work, double* psi,
+int sourceshape_device(const double2* V, int L, int nev, const double* evals, double2* work, double* psi, int cm,
                        cudaStream_t st);
 }
 
@@ -704,11 +704,10 @@ int laph_solver_sourceshape(laph_solver* s, int i, int weighted, double* psi) {
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const ProbDesc& d = s->hd[i];
   const int H = d.L / 2, Nc = H * H * H;
-  // scratch, all free once the run has finished and rewritten by the next run:
-  // Y (V in 3*site + colour order), W (its class-major copy), E0 (psi bins)
+  // scratch, both free once the run has finished and rewritten by the next run:
+  // W (the class-major copy of the colour-major V), E0 (psi bins)
   double* dpsi = reinterpret_cast<double*>(s->E[0] + d.blk);
-  LAPH_TRY(to_reference(s->V + d.blk, s->Y + d.blk, d.V3, d.nev, s->st));
-  LAPH_TRY(sourceshape_device(s->Y + d.blk, d.L, d.nev, weighted ? s->theta + d.kv : nullptr, s->W + d.blk, dpsi,
+  LAPH_TRY(sourceshape_device(s->V + d.blk, d.L, d.nev, weighted ? s->theta + d.kv : nullptr, s->W + d.blk, dpsi, 1,
                               s->st));
   LAPH_CUDA_TRY(cudaMemcpyAsync(psi, dpsi, sizeof(double) * Nc, cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
@@ -722,10 +721,9 @@ int laph_solver_displace(laph_solver* s, int i, int dir, double* W, int on_devic
   }
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const ProbDesc& d = s->hd[i];
-  // V goes through Y (reference order) and host output through W, both free after the run
+  // reads the colour-major V in place; host output goes through W, free after the run
   double2* out = on_device ? reinterpret_cast<double2*>(W) : s->W + d.blk;
-  LAPH_TRY(to_reference(s->V + d.blk, s->Y + d.blk, d.V3, d.nev, s->st));
-  LAPH_TRY(displace_device(s->U64 + d.u64, d.L, dir, d.nev, d.dim, s->Y + d.blk, out, s->st));
+  LAPH_TRY(displace_device(s->U64 + d.u64, d.L, dir, d.nev, d.dim, s->V + d.blk, out, 1, s->st));
   if (!on_device)
     LAPH_CUDA_TRY(cudaMemcpyAsync(W, out, sizeof(double2) * d.dim * d.nev, cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));

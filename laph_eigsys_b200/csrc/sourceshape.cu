@@ -42,7 +42,7 @@ constexpr int kSsBinsMax = 4096;           // shared bins: (L/2)^3 <= 4096, i.e.
 constexpr int kSsSmem = 2 * kSsStage * (int)sizeof(double2) + kSsBinsMax * (int)sizeof(double);
 
 __global__ void k_ss_pack(const double2* __restrict__ V, int L, int nev, const double* __restrict__ evals,
-                          double2* __restrict__ Vp) {
+                          double2* __restrict__ Vp, int cm) {
   const int H = L / 2, Nc = H * H * H, R = 3 * Nc;
   const long long dim = 3LL * L * L * L;
   const long long total = 8LL * nev * R;
@@ -54,7 +54,8 @@ __global__ void k_ss_pack(const double2* __restrict__ V, int L, int nev, const d
     const int a = sc / (H * H), b = (sc / H) % H, cc = sc % H;
     const int x = 2 * a + (c >> 2), y = 2 * b + ((c >> 1) & 1), z = 2 * cc + (c & 1);
     const long long site = (long long)x * L * L + y * L + z;
-    double2 v = V[3 * site + colour + n * dim];
+    // input 3*site + colour, or colour-major (cm: colour*V3 + site, the solver's own blocks)
+    double2 v = V[(cm ? colour * (dim / 3) + site : 3 * site + colour) + n * dim];
     if (evals) {
       const double w = sqrt(fabs(evals[n]));
       v = make_double2(v.x * w, v.y * w);
@@ -167,9 +168,9 @@ bool g_ss_attr[64] = {false};
 
 }  // namespace
 
-// psi[(L/2)^3] (device) from a device eigensystem V [3 V3][nev] (column stride 3 V3);
-// work: 8 nev (3 V3 / 8) double2 of device scratch owned by the caller.
-int sourceshape_device(const double2* V, int L, int nev, const double* evals, double2* work, double* psi,
+// psi[(L/2)^3] (device) from a device eigensystem V [3 V3][nev] (column stride 3 V3,
+// colour-major rows when cm); work: 8 nev (3 V3 / 8) double2 of device scratch owned by the caller.
+int sourceshape_device(const double2* V, int L, int nev, const double* evals, double2* work, double* psi, int cm,
                        cudaStream_t st) {
   int dev = 0;
   LAPH_CUDA_TRY(cudaGetDevice(&dev));
@@ -182,7 +183,7 @@ int sourceshape_device(const double2* V, int L, int nev, const double* evals, do
   LAPH_CUDA_TRY(cudaMemsetAsync(psi, 0, sizeof(double) * Nc, st));
   const long long total = 8LL * nev * 3 * Nc;
   const int pb = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-  k_ss_pack<<<pb, 256, 0, st>>>(V, L, nev, evals, work);
+  k_ss_pack<<<pb, 256, 0, st>>>(V, L, nev, evals, work, cm);
   LAPH_CUDA_TRY(cudaGetLastError());
   k_ss_tile<<<8 * T * (T + 1) / 2, 512, kSsSmem, st>>>(work, L, nev, psi);
   LAPH_CUDA_TRY(cudaGetLastError());
@@ -250,7 +251,7 @@ extern "C" int laph_sourceshape(const double* V, int L, int nev, const double* e
     Vuse = dV;
     ev_use = dev_ev;
   }
-  rc = sourceshape_device(Vuse, L, nev, ev_use, work, dpsi, st);
+  rc = sourceshape_device(Vuse, L, nev, ev_use, work, dpsi, 0, st);
   if (rc == LAPH_OK && (cudaMemcpyAsync(psi, dpsi, sizeof(double) * Nc, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
                         cudaStreamSynchronize(st) != cudaSuccess)) {
     set_error("laph_sourceshape: %s", cudaGetErrorString(cudaGetLastError()));
