@@ -13,6 +13,7 @@
 // kind for tcgen05, and its FP64 DMMA rate equals its FP64 FMA rate.
 #include "batch.cuh"
 #include "dense.cuh"
+#include "filter.cuh"
 
 namespace laph {
 
@@ -784,6 +785,7 @@ int to_reference(const double2* in, double2* out, int V3, int nev, cudaStream_t 
 int dense_init() {
   LAPH_CUDA_TRY(cudaFuncSetAttribute(k_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, kGramSmem));
   LAPH_CUDA_TRY(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, kRotSmem));
+  LAPH_TRY(neglap64_init());
   return LAPH_OK;
 }
 int gram(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int chunk_rows,

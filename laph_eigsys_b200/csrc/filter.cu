@@ -20,6 +20,7 @@
 // plus (108 + 4) / kb for BF16 links; see the solver for the recurrence.
 #include "batch.cuh"
 #include "filter.cuh"
+#include "stencil64cols.cuh"
 
 #include <cuda_bf16.h>
 
@@ -392,47 +393,44 @@ __global__ void __launch_bounds__(128, 4)
 }
 
 // ------------------------------------------------ FP64 block stencil: A W --
-// Y_j = (-Delta) W_j = 6 W_j - hop(W_j), FP64, one thread per (site, column).
-__global__ void __launch_bounds__(128) k_neglap64_batch(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
+// Y_j = (-Delta) W_j = 6 W_j - hop(W_j), FP64; CTA = 128 sites x a block of
+// kColsFP64 columns (stencil64cols.cuh).
+__global__ void __launch_bounds__(128, 3) k_neglap64_batch(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
                                                         const int* __restrict__ start, int np,
                                                         const double2* __restrict__ U64, const double2* __restrict__ Wp,
                                                         double2* __restrict__ Yp) {
   const int p = find_prob(start, np, blockIdx.x);
   if (!ps[p].active) return;
   const ProbDesc d = pd[p];
-  const int nst = (d.V3 + 127) >> 7;
+  const int nst = (d.V3 + kSites64 - 1) / kSites64;
   const int t = blockIdx.x - start[p];
-  const int st = t % nst, j = t / nst;
-  const int s = st * 128 + threadIdx.x;
-  if (s >= d.V3 || j >= d.k) return;
+  const int st = t % nst, cb = t / nst;
+  const int s = st * kSites64 + threadIdx.x;
+  if (s >= d.V3) return;
   const Lat g{d.L, d.L * d.L, d.V3};
-  const double2* U = U64 + d.u64;
-  const size_t col = (size_t)d.blk + (size_t)j * d.dim;
-  const double2* x = Wp + col;
-  int sx, sy, sz;
+  int sx, sy, sz, up[3], dn[3];
   site_xyz(g, s, sx, sy, sz);
-  double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
 #pragma unroll
   for (int mu = 0; mu < 3; ++mu) {
-    const int u = nb_up(g, sx, sy, sz, mu), dn = nb_dn(g, sx, sy, sz, mu);
-    double2 xu[3], xd[3];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      xu[b] = __ldg(x + (size_t)b * d.V3 + u);
-      xd[b] = __ldg(x + (size_t)b * d.V3 + dn);
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        cfma(acc[a], __ldg(U + (size_t)(mu * 9 + 3 * a + b) * d.V3 + s), xu[b]);
-        cfmac(acc[a], __ldg(U + (size_t)(mu * 9 + 3 * b + a) * d.V3 + dn), xd[b]);
-      }
+    up[mu] = nb_up(g, sx, sy, sz, mu);
+    dn[mu] = nb_dn(g, sx, sy, sz, mu);
   }
+  extern __shared__ double2 s64[];
+  double2 (*sUb)[kSites64] = reinterpret_cast<double2 (*)[kSites64]>(s64);
+  Links64 l;
+  load_links64(U64 + d.u64, g, s, dn, l, sUb);
+  const int j1 = min(d.k, (cb + 1) * kColsFP64);
+#pragma unroll 1
+  for (int j = cb * kColsFP64; j < j1; ++j) {
+    const size_t col = (size_t)d.blk + (size_t)j * d.dim;
+    const double2* x = Wp + col;
+    double2 acc[3];
+    hop64_col(l, sUb, d.V3, up, dn, x, acc);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const double2 xs = __ldg(x + (size_t)a * d.V3 + s);
-    Yp[col + (size_t)a * d.V3 + s] = make_double2(6.0 * xs.x - acc[a].x, 6.0 * xs.y - acc[a].y);
+    for (int a = 0; a < 3; ++a) {
+      const double2 xs = __ldg(x + (size_t)a * d.V3 + s);
+      Yp[col + (size_t)a * d.V3 + s] = make_double2(6.0 * xs.x - acc[a].x, 6.0 * xs.y - acc[a].y);
+    }
   }
 }
 
@@ -509,9 +507,14 @@ int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np,
   return LAPH_OK;
 }
 
+int neglap64_init() {
+  LAPH_CUDA_TRY(cudaFuncSetAttribute(k_neglap64_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, kStencil64Smem));
+  return LAPH_OK;
+}
+
 int neglap64_batch(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
                    const double2* W, double2* Y, cudaStream_t st) {
-  k_neglap64_batch<<<nblk, 128, 0, st>>>(pd, ps, start, np, U64, W, Y);
+  k_neglap64_batch<<<nblk, kSites64, kStencil64Smem, st>>>(pd, ps, start, np, U64, W, Y);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

@@ -14,6 +14,8 @@ int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np,
               const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
               const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant,
               cudaStream_t st);
+// Opt the FP64 stencil into its dynamic shared memory on the current device.
+int neglap64_init();
 // Y = (-Delta) W for every column, FP64.
 int neglap64_batch(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
                    const double2* W, double2* Y, cudaStream_t st);

@@ -36,6 +36,7 @@
 #include "links.cuh"
 #include "mlp.cuh"
 #include "smear.cuh"
+#include "stencil64cols.cuh"
 
 namespace laph {
 int displace_device(const double2* U, int L, int dir, int nev, long long ldv, const double2* V, double2* W, int cm,
@@ -56,9 +57,9 @@ struct laph_solver {
   ProbState* d_ps = nullptr;
   std::vector<ProbState> hps;
   // CTA -> problem prefix tables
-  int *st_site = nullptr, *st_filt = nullptr, *st_nl = nullptr, *st_gram = nullptr, *st_gred = nullptr,
+  int *st_site = nullptr, *st_filt = nullptr, *st_nl = nullptr, *st_res = nullptr, *st_gram = nullptr, *st_gred = nullptr,
       *st_rot = nullptr, *st_rand = nullptr, *st_col = nullptr;
-  int nb_site = 0, nb_filt = 0, nb_nl = 0, nb_gram = 0, nb_gred = 0, nb_rot = 0, nb_rand = 0, nb_col = 0;
+  int nb_site = 0, nb_filt = 0, nb_nl = 0, nb_res = 0, nb_gram = 0, nb_gred = 0, nb_rot = 0, nb_rand = 0, nb_col = 0;
   // pools
   double2 *U64raw = nullptr, *U64 = nullptr, *Utmp = nullptr, *dec = nullptr, *stage = nullptr;
   float2* Uf32 = nullptr;
@@ -140,7 +141,7 @@ int laph_solver_destroy(laph_solver* s) {
   if (!s) return LAPH_OK;
   cudaSetDevice(s->dev);
   if (s->st) cudaStreamSynchronize(s->st);
-  void* ptrs[] = {s->d_pd, s->d_ps, s->st_site, s->st_filt, s->st_nl, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
+  void* ptrs[] = {s->d_pd, s->d_ps, s->st_site, s->st_filt, s->st_nl, s->st_res, s->st_gram, s->st_gred, s->st_rot, s->st_rand,
                   s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
                   s->phases, s->norms, s->d_nactive, s->model, s->feats, s->mwork, s->bound, s->plaq, s->wdeg,
@@ -203,7 +204,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   // descriptors and pool offsets
   long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
   size_t max_run = 0, max_v3 = 0;
-  std::vector<int> per_site, per_filt, per_nl, per_gram, per_gred, per_rot, per_rand, per_col;
+  std::vector<int> per_site, per_filt, per_nl, per_res, per_gram, per_gred, per_rot, per_rand, per_col;
   for (int i = 0; i < n; ++i) {
     ProbDesc d{};
     d.L = probs[i].L;
@@ -239,7 +240,8 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     const int nst = (d.V3 + 127) / 128;
     per_site.push_back(nst);
     per_filt.push_back(nst * ((d.k + s->kb - 1) / s->kb));
-    per_nl.push_back(nst * d.k);
+    per_nl.push_back(nst * ((d.k + kColsFP64 - 1) / kColsFP64));
+    per_res.push_back(nst * d.k);
     per_gram.push_back(d.nchunk * npair);
     per_gred.push_back((2 * npair * kGramTile * kGramTile + 255) / 256);
     per_rot.push_back(((d.dim + kRotRows - 1) / kRotRows) * (d.k / 32));
@@ -278,7 +280,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     return fail(LAPH_ENOMEM);
   }
   if ((rc = upload_prefix(per_site, &s->st_site, &s->nb_site)) || (rc = upload_prefix(per_filt, &s->st_filt, &s->nb_filt)) ||
-      (rc = upload_prefix(per_nl, &s->st_nl, &s->nb_nl)) || (rc = upload_prefix(per_gram, &s->st_gram, &s->nb_gram)) ||
+      (rc = upload_prefix(per_nl, &s->st_nl, &s->nb_nl)) || (rc = upload_prefix(per_res, &s->st_res, &s->nb_res)) || (rc = upload_prefix(per_gram, &s->st_gram, &s->nb_gram)) ||
       (rc = upload_prefix(per_gred, &s->st_gred, &s->nb_gred)) || (rc = upload_prefix(per_rot, &s->st_rot, &s->nb_rot)) ||
       (rc = upload_prefix(per_rand, &s->st_rand, &s->nb_rand)) || (rc = upload_prefix(per_col, &s->st_col, &s->nb_col)))
     return fail(rc);
@@ -342,7 +344,7 @@ static int iteration_rr(laph_solver* s, int first_iter) {
   LAPH_TRY(small_dense(s->d_pd, s->d_ps, s->np, s->KK, s->theta, s->tcoef, s->scol, s->dwork, first_iter, fixed ? 1 : 0,
                        s->o.jacobi_sweeps > 0 ? s->o.jacobi_sweeps : 2, s->tstamp, s->st));
   LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->KK, s->V, s->st));
-  LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
+  LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_res, s->np, s->nb_res, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
   LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
   LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
   return LAPH_OK;
@@ -477,7 +479,7 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->V, o.seed, s->st));
     LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
     LAPH_TRY(start_window(s->d_pd, s->d_ps, s->np, s->theta, s->st));
-    LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
+    LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_res, s->np, s->nb_res, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
     LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
     LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
     nlaunch += 2 + 4;  // pack, random block, window state, residual, check
