@@ -321,6 +321,35 @@ def measure_displacement(solver, stream, batch, reps=4):
             "frac": byts / (ms / 1e3) / 1e9 / hbm, "launches": 3 * n}
 
 
+def measure_matvec_fp64(cfg, batch, device, deg=12, reps=20):
+    """The plain form's MatShell MatMult y = T_deg(B) x (FP64, one vector, device pointers), CUDA events around
+    `reps` products on the context's stream.  Algorithmic bytes per site and B application: the 6 links a site
+    reads once (its 3 forward links; the backward ones are other sites' forward links) = 432, plus x read,
+    z read, y written = 3 x 48."""
+    import torch
+    import laph_eigsys_b200 as lb
+    L = batch[0][0]
+    ctx = lb.Context(L, 12.0, 0.6, deg, device=device)
+    ctx.set_links(batch[0][2])
+    dim = 3 * L ** 3
+    x = torch.randn(dim, dtype=torch.complex128, device="cuda")
+    y = torch.empty_like(x)
+    ctx.matmult_device(x.data_ptr(), y.data_ptr(), deg)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ctx.matmult_device(x.data_ptr(), y.data_ptr(), deg)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / reps
+    ctx.close()
+    byts = deg * L ** 3 * (432.0 + 3 * 48.0)
+    hbm, src = peaks()
+    return {"workload": f"T_{deg}(B) x on one {L}^3 vector, FP64 (laph_matmult, device pointers)",
+            "ms_per_matmult": ms, "bytes_per_matmult": byts, "achieved_gbs": byts / (ms / 1e3) / 1e9,
+            "peak_gbs": hbm, "peak_source": src, "frac": byts / (ms / 1e3) / 1e9 / hbm,
+            "timing": "host clock around synchronised device-pointer calls (each call synchronises its stream)"}
+
+
 def measure_sourceshape(solver, stream, batch, no_cpu, reps=4):
     """psi(r) of the first solved timeslices in place on the device (CUDA events on the solver's stream), and the
     oracle's restatement on one 16^3 eigensystem beside the device kernel on the same input."""
@@ -523,6 +552,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_plain:
         ev0, _, _ = solver.get(0, vectors=False)
         plain = plain_gpu(cfg, batch, float(1.1 * (-ev0)[-1]), args.plain_timeslices, local)
+        plain["matvec_fp64"] = measure_matvec_fp64(cfg, batch, local)
         plain["chosen_over_plain"] = value / plain["value"] if plain.get("value") else None
 
     # ---- source shape of the solved eigenvectors (next row of the path) ------
