@@ -34,6 +34,8 @@ struct ProbState {
   int iters;                 // outer iterations done
   int chol_fail;             // Cholesky pivot clamped in the last iteration
   int nlock;                 // leading Ritz columns converged well below tol: not filtered
+  int c0;                    // nlock rounded down to the Gram tile: columns [0, c0) are frozen
+                             // (left out of the Rayleigh-Ritz, projected out of the rest)
 };
 
 // Block index b -> problem p with start[p] <= b < start[p+1].

@@ -8,6 +8,9 @@
 //   k_residual64  R = (-Delta) V - V diag(theta) (FP64 stencil), S = -2 c_hop R
 //                 (FP32), residual partial sums
 //   k_resid       residual norms, convergence mask
+// Columns [0, c0) of a problem (whole tiles of locked Ritz vectors) are frozen:
+// the Gram skips frozen x frozen tiles, the small problem projects the active
+// block against them, and the rotation and residual write active columns only.
 // These replace SLEPc's BV orthogonalisation and DS dense eigensolve inside
 // EPSSolve (src/ev_ts.cpp:263).  Complex FP64 on CUDA cores: B200 has no FP64
 // kind for tcgen05, and its FP64 DMMA rate equals its FP64 FMA rate.
@@ -44,6 +47,7 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
     ++ti;
   }
   const int tj = ti + pr;
+  if ((tj + 1) * GT <= ps[p].c0) return;  // both tiles frozen: not needed
   const double2* A = W + d.blk + (size_t)(ti * GT) * d.dim;
   const double2* BW = W + d.blk + (size_t)(tj * GT) * d.dim;
   const double2* BY = Y + d.blk + (size_t)(tj * GT) * d.dim;
@@ -136,6 +140,7 @@ __global__ void k_gram_reduce(const ProbDesc* __restrict__ pd, const ProbState* 
     ++ti;
   }
   const int tj = ti + pr;
+  if ((tj + 1) * GT <= ps[p].c0) return;  // frozen tile pair: not computed
   double2 s = make_double2(0.0, 0.0);
   for (int c = 0; c < d.nchunk; ++c) s = cadd(s, gpart[d.gp + ((size_t)(c * 2 + which) * npair + tile - which * npair) * (GT * GT) + w]);
   const int i = ti * GT + w / GT, j = tj * GT + w % GT;
@@ -176,69 +181,106 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
   stamp(0);
   const ProbDesc d = pd[p];
   const int k = d.k, tid = threadIdx.x, nt = blockDim.x;
+  // Locked columns [0, c0) (a multiple of the tile width) stay as they are: the
+  // Rayleigh-Ritz runs on the active block a = [c0, k), with W_a projected
+  // against the locked Ritz vectors V_l (= W_l).  n = k - c0; every matrix
+  // below keeps the leading dimension k.
+  const int c0 = ps[p].c0, n = k - c0;
   const size_t kk2 = (size_t)k * k;
   double2* G = KK + d.kk;
   double2* H = G + kk2;
   double2* Mi = G + 2 * kk2;
   double2* Q = G + 3 * kk2;
   double2* Ht = G + 4 * kk2;
+  double2* Ga = G + c0 + (size_t)c0 * k;  // G_aa -> R (scaled Cholesky factor)
+  double2* Ha = H + c0 + (size_t)c0 * k;  // H_aa
   double* dinv = dwork + d.kv * 4;  // 4 k-length scratch vectors per problem
   double* lam = dinv + k;
   int* perm = reinterpret_cast<int*>(lam + k);
+  double* th = theta + d.kv;
   __shared__ int s_flag;
   __shared__ double s_red[32];
+  const int nn = n * n;
 
-  // (a) column scaling D = sqrt(diag G)
-  for (int i = tid; i < k; i += nt) {
-    const double g = G[i + (size_t)i * k].x;
+  // (0) projection against the locked block: with G_la = V_l^H W_a and
+  // H_la = V_l^H A W_a (Gram tiles of the locked rows), V_l^H V_l = I and
+  // V_l^H A V_l = Theta_l,  W_a' = W_a - V_l G_la  has
+  //   G' = G_aa - G_la^H G_la,
+  //   H' = H_aa - G_la^H H_la - H_la^H G_la + G_la^H Theta_l G_la.
+  if (c0 > 0) {
+    for (int e = tid; e < nn; e += nt) {
+      const int i = e % n, j = e / n;
+      const double2* gi = G + (size_t)(c0 + i) * k;
+      const double2* gj = G + (size_t)(c0 + j) * k;
+      const double2* hi = H + (size_t)(c0 + i) * k;
+      const double2* hj = H + (size_t)(c0 + j) * k;
+      double2 sg = make_double2(0.0, 0.0), sh = make_double2(0.0, 0.0);
+      for (int q = 0; q < c0; ++q) {
+        const double2 a = gi[q], b = gj[q];
+        cfmac(sg, a, b);                                 // conj(G_qi) G_qj
+        cfmac(sh, a, hj[q]);                             // conj(G_qi) H_qj
+        cfmac(sh, hi[q], b);                             // conj(H_qi) G_qj
+        const double2 t = cmulc(a, b);
+        sh = make_double2(sh.x - th[q] * t.x, sh.y - th[q] * t.y);  // - theta_q conj(G_qi) G_qj
+      }
+      double2& g = Ga[i + (size_t)j * k];
+      double2& h = Ha[i + (size_t)j * k];
+      g = csub(g, sg);
+      h = csub(h, sh);
+    }
+    __syncthreads();
+  }
+  // (a) column scaling D = sqrt(diag G')
+  for (int i = tid; i < n; i += nt) {
+    const double g = Ga[i + (size_t)i * k].x;
     dinv[i] = g > 0.0 ? 1.0 / sqrt(g) : 1.0;
   }
   if (tid == 0) s_flag = 0;
   __syncthreads();
-  for (size_t e = tid; e < kk2; e += nt) {
-    const int i = (int)(e % k), j = (int)(e / k);
-    G[e] = cscal(G[e], dinv[i] * dinv[j]);
+  for (int e = tid; e < nn; e += nt) {
+    const int i = e % n, j = e / n;
+    Ga[i + (size_t)j * k] = cscal(Ga[i + (size_t)j * k], dinv[i] * dinv[j]);
   }
   __syncthreads();
-  // (b) Cholesky G = R^H R, R upper, in place (right-looking)
-  for (int q = 0; q < k; ++q) {
+  // (b) Cholesky G' = R^H R, R upper, in place (right-looking)
+  for (int q = 0; q < n; ++q) {
     if (tid == 0) {
-      double piv = at(G, k, q, q).x;
+      double piv = at(Ga, k, q, q).x;
       if (!(piv > 1e-28)) {
         piv = 1e-28;
         s_flag = 1;
       }
-      at(G, k, q, q) = make_double2(sqrt(piv), 0.0);
+      at(Ga, k, q, q) = make_double2(sqrt(piv), 0.0);
     }
     __syncthreads();
-    const double rinv = 1.0 / at(G, k, q, q).x;
-    for (int j = q + 1 + tid; j < k; j += nt) at(G, k, q, j) = cscal(at(G, k, q, j), rinv);
+    const double rinv = 1.0 / at(Ga, k, q, q).x;
+    for (int j = q + 1 + tid; j < n; j += nt) at(Ga, k, q, j) = cscal(at(Ga, k, q, j), rinv);
     __syncthreads();
-    const int m = k - q - 1;
+    const int m = n - q - 1;
     for (int e = tid; e < m * m; e += nt) {
       const int i = q + 1 + e / m, j = q + 1 + e % m;
       if (i <= j) {
-        double2 v = at(G, k, i, j);
-        const double2 a = at(G, k, q, i), b = at(G, k, q, j);
+        double2 v = at(Ga, k, i, j);
+        const double2 a = at(Ga, k, q, i), b = at(Ga, k, q, j);
         // v -= conj(a) b
         v.x -= a.x * b.x + a.y * b.y;
         v.y -= a.x * b.y - a.y * b.x;
-        at(G, k, i, j) = v;
+        at(Ga, k, i, j) = v;
       }
     }
     __syncthreads();
   }
   stamp(1);
   // (c) Minv = D^{-1} R^{-1} (upper triangular), column by column
-  for (size_t e = tid; e < kk2; e += nt) Mi[e] = make_double2(0.0, 0.0);
+  for (int e = tid; e < nn; e += nt) Mi[e % n + (size_t)(e / n) * k] = make_double2(0.0, 0.0);
   __syncthreads();
-  for (int j = 0; j < k; ++j) {
-    const double rjj = at(G, k, j, j).x;
+  for (int j = 0; j < n; ++j) {
+    const double rjj = at(Ga, k, j, j).x;
     for (int i = tid; i <= j; i += nt) {
       double2 s = make_double2(i == j ? 1.0 : 0.0, 0.0);
       for (int q = i; q < j; ++q) {
         // s -= Rinv(i,q) R(q,j)
-        const double2 a = at(Mi, k, i, q), b = at(G, k, q, j);
+        const double2 a = at(Mi, k, i, q), b = at(Ga, k, q, j);
         s.x -= a.x * b.x - a.y * b.y;
         s.y -= a.x * b.y + a.y * b.x;
       }
@@ -246,29 +288,29 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     }
     __syncthreads();
   }
-  for (size_t e = tid; e < kk2; e += nt) {
-    const int i = (int)(e % k);
-    Mi[e] = cscal(Mi[e], dinv[i]);
+  for (int e = tid; e < nn; e += nt) {
+    const int i = e % n, j = e / n;
+    Mi[i + (size_t)j * k] = cscal(Mi[i + (size_t)j * k], dinv[i]);
   }
   __syncthreads();
   stamp(2);
-  // (d) T1 = H Minv ; Ht = Minv^H T1 (Hermitian part)
-  for (size_t e = tid; e < kk2; e += nt) {
-    const int i = (int)(e % k), j = (int)(e / k);
+  // (d) T1 = H' Minv ; Ht = Minv^H T1 (Hermitian part)
+  for (int e = tid; e < nn; e += nt) {
+    const int i = e % n, j = e / n;
     double2 s = make_double2(0.0, 0.0);
-    for (int q = 0; q <= j; ++q) cfma(s, at(H, k, i, q), at(Mi, k, q, j));
-    Q[e] = s;
+    for (int q = 0; q <= j; ++q) cfma(s, at(Ha, k, i, q), at(Mi, k, q, j));
+    Q[i + (size_t)j * k] = s;
   }
   __syncthreads();
-  for (size_t e = tid; e < kk2; e += nt) {
-    const int i = (int)(e % k), j = (int)(e / k);
+  for (int e = tid; e < nn; e += nt) {
+    const int i = e % n, j = e / n;
     double2 s = make_double2(0.0, 0.0);
     for (int q = 0; q <= i; ++q) cfmac(s, at(Mi, k, q, i), at(Q, k, q, j));
-    Ht[e] = s;
+    Ht[i + (size_t)j * k] = s;
   }
   __syncthreads();
-  for (size_t e = tid; e < kk2; e += nt) {
-    const int i = (int)(e % k), j = (int)(e / k);
+  for (int e = tid; e < nn; e += nt) {
+    const int i = e % n, j = e / n;
     if (i < j) {
       const double2 a = at(Ht, k, i, j), b = at(Ht, k, j, i);
       const double2 h = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
@@ -277,32 +319,33 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     } else if (i == j) {
       at(Ht, k, i, i).y = 0.0;
     }
-    Q[e] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    Q[i + (size_t)j * k] = make_double2(i == j ? 1.0 : 0.0, 0.0);
   }
   __syncthreads();
   stamp(3);
   // (e) cyclic Jacobi in "position order": in every step position i is paired
-  // with its mirror k-1-i, and after the rotations positions 1..k-1 shift by
-  // one (round-robin tournament: every pair meets once in k-1 steps).  The
+  // with its mirror n-1-i, and after the rotations positions 1..n-1 shift by
+  // one (round-robin tournament: every pair meets once in n-1 steps).  The
   // shift is folded into the update, which writes the rotated 2x2 blocks of
   // Ht (and the rotated column pairs of Q) to their new positions in a second
   // buffer, so each step is one read and one write of both matrices with
   // unit-stride warp accesses.  Ht ping-pongs with the H storage, Q with the
-  // G storage; Q's rows stay in the original basis order and its columns
-  // follow Ht's diagonal, which is all the sort below needs.
+  // active block of the G storage (the Cholesky factor, no longer needed);
+  // Q's rows stay in the basis order and its columns follow Ht's diagonal,
+  // which is all the sort below needs.
   __shared__ double s_c[256], s_s[256];
   __shared__ double2 s_e[256];
-  const int half = k / 2;
+  const int half = n / 2;
   double2* hc = Ht;  // current Ht
   double2* hn = H;   // next Ht
   double2* qc = Q;
-  double2* qn = G;
-  auto shift = [&](int pos) { return pos == 0 ? 0 : (pos == k - 1 ? 1 : pos + 1); };
+  double2* qn = Ga;
+  auto shift = [&](int pos) { return pos == 0 ? 0 : (pos == n - 1 ? 1 : pos + 1); };
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     double off = 0.0, dia = 0.0;
-    for (size_t e = tid; e < kk2; e += nt) {
-      const int i = (int)(e % k), j = (int)(e / k);
-      const double2 v = hc[e];
+    for (int e = tid; e < nn; e += nt) {
+      const int i = e % n, j = e / n;
+      const double2 v = hc[i + (size_t)j * k];
       if (i != j) off += v.x * v.x + v.y * v.y;
       else dia += v.x * v.x;
     }
@@ -329,10 +372,10 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     // |off| <= 3e-14 |diag|: with eigenvalue gaps >= 1e-3 lambda_max this
     // leaves eigenvector errors below 1e-10, far under the residual target
     if (s_red[0] <= 1e-27 * s_red[1]) break;
-    for (int step = 0; step < k - 1; ++step) {
-      // rotation of pair r = (r, k-1-r): J (p,p)=c (p,q)=s (q,p)=-s e (q,q)=c e, e = e^{-i phi}
+    for (int step = 0; step < n - 1; ++step) {
+      // rotation of pair r = (r, n-1-r): J (p,p)=c (p,q)=s (q,p)=-s e (q,q)=c e, e = e^{-i phi}
       for (int r = tid; r < half; r += nt) {
-        const int pa = r, qb = k - 1 - r;
+        const int pa = r, qb = n - 1 - r;
         const double2 g = at(hc, k, pa, qb);
         const double rr = hypot(g.x, g.y);
         const double app = at(hc, k, pa, pa).x, aqq = at(hc, k, qb, qb).x;
@@ -350,10 +393,10 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
         s_e[r] = em;
       }
       __syncthreads();
-      // Ht <- J^H Ht J on every 2x2 block (rows r', k-1-r'; columns r, k-1-r), shifted
+      // Ht <- J^H Ht J on every 2x2 block (rows r', n-1-r'; columns r, n-1-r), shifted
       for (int e = tid; e < half * half; e += nt) {
         const int r = e / half, rp = e - r * half;
-        const int p = r, q = k - 1 - r, pp = rp, qq = k - 1 - rp;
+        const int p = r, q = n - 1 - r, pp = rp, qq = n - 1 - rp;
         const double c = s_c[r], s = s_s[r];
         const double2 em = s_e[r];
         const double c2 = s_c[rp], s2 = s_s[rp];
@@ -385,9 +428,9 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
         at(hn, k, nqq, nq_) = b_qq;
       }
       // Q <- Q J, columns shifted
-      for (int e = tid; e < half * k; e += nt) {
-        const int r = e / k, i = e - r * k;
-        const int p = r, q = k - 1 - r;
+      for (int e = tid; e < half * n; e += nt) {
+        const int r = e / n, i = e - r * n;
+        const int p = r, q = n - 1 - r;
         const double c = s_c[r], s = s_s[r];
         const double2 em = s_e[r];
         const double2 qp = at(qc, k, i, p), qq = cmul(at(qc, k, i, q), em);
@@ -404,35 +447,55 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
     }
   }
   if (qc != Q) {
-    // C below is written to the G storage: bring Q home first
-    for (size_t e = tid; e < kk2; e += nt) Q[e] = qc[e];
+    // bring Q home: its other buffer is written below
+    for (int e = tid; e < nn; e += nt) {
+      const size_t o = e % n + (size_t)(e / n) * k;
+      Q[o] = qc[o];
+    }
     __syncthreads();
   }
   stamp(4);
   // (f) sort ascending (rank sort, ties by index)
-  for (int i = tid; i < k; i += nt) lam[i] = at(hc, k, i, i).x;
+  for (int i = tid; i < n; i += nt) lam[i] = at(hc, k, i, i).x;
   __syncthreads();
-  for (int i = tid; i < k; i += nt) {
+  for (int i = tid; i < n; i += nt) {
     const double li = lam[i];
     int r = 0;
-    for (int j = 0; j < k; ++j) {
+    for (int j = 0; j < n; ++j) {
       const double lj = lam[j];
       r += (lj < li) || (lj == li && j < i);
     }
     perm[r] = i;
   }
   __syncthreads();
-  double* th = theta + d.kv;
-  for (int r = tid; r < k; r += nt) th[r] = lam[perm[r]];
-  // (g) C = Minv Q[:, perm] -> G storage
-  for (size_t e = tid; e < kk2; e += nt) {
-    const int i = (int)(e % k), j = (int)(e / k);
+  for (int r = tid; r < n; r += nt) th[c0 + r] = lam[perm[r]];
+  // (g) C_a = Minv Q[:, perm]; the rotation's coefficients of the active
+  // columns over the whole block are [-G_la C_a ; C_a] (the V_l part undoes
+  // the projection), stored in columns c0.. of the G storage
+  double2* T = c0 > 0 ? H : Ga;  // C_a (H is free after the sort)
+  for (int e = tid; e < nn; e += nt) {
+    const int i = e % n, j = e / n;
     const int pj = perm[j];
     double2 s = make_double2(0.0, 0.0);
-    for (int q = i; q < k; ++q) cfma(s, at(Mi, k, i, q), at(Q, k, q, pj));
-    G[e] = s;
+    for (int q = i; q < n; ++q) cfma(s, at(Mi, k, i, q), at(Q, k, q, pj));
+    T[i + (size_t)j * k] = s;
   }
   __syncthreads();
+  if (c0 > 0) {
+    // X = -G_la C_a into Ht (free), then both parts into G's columns c0..
+    for (int e = tid; e < c0 * n; e += nt) {
+      const int q = e % c0, j = e / c0;
+      double2 s = make_double2(0.0, 0.0);
+      for (int i = 0; i < n; ++i) cfma(s, G[q + (size_t)(c0 + i) * k], T[i + (size_t)j * k]);
+      Ht[q + (size_t)j * k] = make_double2(-s.x, -s.y);
+    }
+    __syncthreads();
+    for (int e = tid; e < k * n; e += nt) {
+      const int row = e % k, j = e / k;
+      G[row + (size_t)(c0 + j) * k] = row < c0 ? Ht[row + (size_t)j * k] : T[(row - c0) + (size_t)j * k];
+    }
+    __syncthreads();
+  }
   stamp(5);
   // (h) next window [lam_cut, lam_max] and Chebyshev coefficients
   if (tid == 0) {
@@ -520,6 +583,7 @@ __global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd,
   const int t = blockIdx.x - start[p];
   const int rt = t / nct, ct = t - rt * nct;
   const int row0 = rt * RR, col0 = ct * RC;
+  if (col0 < ps[p].c0) return;  // frozen columns keep their Ritz vectors
   const int k = d.k;
   const double2* C = KK + d.kk;  // C in G storage, column-major k x k
   const double2* Wb = Wp + d.blk;
@@ -603,6 +667,7 @@ __global__ void __launch_bounds__(128) k_residual64(const ProbDesc* __restrict__
   const int nst = (d.V3 + 127) >> 7;
   const int t = blockIdx.x - start[p];
   const int st = t % nst, j = t / nst;
+  if (j < ps[p].c0) return;  // frozen column: its residual partials stand
   const int s = st * 128 + threadIdx.x;
   double rr = 0.0;
   if (s < d.V3) {
@@ -695,6 +760,9 @@ __global__ void k_resid(const ProbDesc* __restrict__ pd, ProbState* __restrict__
     int nl = 0;
     while (nl < d.nev && resid[d.kv + nl] <= 0.3 * tol) ++nl;
     S.nlock = nl;
+    // frozen block for the Rayleigh-Ritz: whole Gram tiles of locked columns,
+    // never shrinking (a frozen column is not re-measured, so it stays locked)
+    S.c0 = max(S.c0, min(nl / GT * GT, d.k - GT));
     if (c >= d.nev) S.active = 0;
     else atomicAdd(n_active, 1);
   }

@@ -405,6 +405,7 @@ __global__ void __launch_bounds__(128, 3) k_neglap64_batch(const ProbDesc* __res
   const int nst = (d.V3 + kSites64 - 1) / kSites64;
   const int t = blockIdx.x - start[p];
   const int st = t % nst, cb = t / nst;
+  if ((cb + 1) * kColsFP64 <= ps[p].c0) return;  // frozen columns: Y not needed
   const int s = st * kSites64 + threadIdx.x;
   if (s >= d.V3) return;
   const Lat g{d.L, d.L * d.L, d.V3};

@@ -121,3 +121,22 @@ def test_filter_variants_match_dense(gpu, orc, variant, L, nev, prec):
     A, w, X = dense_ref(orc, U, L)
     check_solution(A, w, X, ev, V, ph, nev, tol)
     s.close()
+
+
+def test_block_solver_frozen_tiles(gpu, orc):
+    """A wide block (nev 100, k 128) converges far enough that whole 32-column tiles of locked Ritz vectors are
+    frozen: later Rayleigh-Ritz passes run on the remaining columns, projected against the frozen ones.  The
+    result must still be the dense eigendecomposition's."""
+    L, nev = 8, 100
+    U = random_links(L, 0.4, 2100)
+    tol = 1e-11
+    s = gpu.Solver([(L, nev), (8, 40)], guard=16, tol=tol, deg=16, max_it=400, link_prec=gpu.LINKS_FP32)
+    s.set_links(0, U)
+    s.set_links(1, random_links(8, 0.4, 2101))
+    st, res = s.run()
+    assert st == 0, res
+    ev, V, ph = s.get(0)
+    A, w, X = dense_ref(orc, U, L)
+    check_solution(A, w, X, ev, V, ph, nev, tol)
+    assert abs(res[0]["trace_vdv"] - nev) < 1e-9
+    s.close()
