@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     # 32^3 x 64, eps 0.3, stout 5 x 0.1, nev 120 (+16 guard), FP32 filter links
     "c3": dict(L=32, T=64, eps=0.3, seed=1229, smear="stout", p1=0.1, p2=0.0, iters=5, compat=1, nev=120,
-               guard=16, link_prec="fp32", tol=1e-9, deg=56),
+               guard=16, link_prec="fp32", tol=1e-9, deg=60),
     # 24^3 x 48, eps 0.3, HYP 0.62/0.62 x 1, nev 120
     "c2": dict(L=24, T=48, eps=0.3, seed=1228, smear="hyp", p1=0.62, p2=0.62, iters=1, compat=0, nev=120,
                guard=16, link_prec="fp32", tol=1e-9, deg=12),
