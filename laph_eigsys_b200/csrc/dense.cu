@@ -12,18 +12,27 @@
 // the Gram skips frozen x frozen tiles, the small problem projects the active
 // block against them, and the rotation and residual write active columns only.
 // These replace SLEPc's BV orthogonalisation and DS dense eigensolve inside
-// EPSSolve (src/ev_ts.cpp:263).  Complex FP64 on CUDA cores: B200 has no FP64
-// kind for tcgen05, and its FP64 DMMA rate equals its FP64 FMA rate.
+// EPSSolve (src/ev_ts.cpp:263).  tcgen05 has no FP64 kind, so the Gram and the
+// rotation run on the FP64 tensor path of mma.sync (m8n8k4 f64, four real
+// MMAs per complex product): at the same peak as the FP64 FMA pipe, but one
+// instruction per 256 FMAs, which measured 7-10% faster for each kernel.
 #include "batch.cuh"
 #include "dense.cuh"
 #include "filter.cuh"
 
 namespace laph {
 
+// d(8x8, 2 per thread) += a(8x4, 1 per thread) b(4x8, 1 per thread), FP64 tensor MMA
+__device__ __forceinline__ void dmma884(double (&acc)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(acc[0]), "+d"(acc[1])
+               : "d"(a), "d"(b));
+}
+
 // ------------------------------------------------------------------ Gram ---
 // CTA: 64 threads, output tiles G[ti,tj] = W_ti^H W_tj and H[ti,tj] = W_ti^H Y_tj
-// (32 x 32 each, thread 4x4 complex of both), over the rows of one chunk;
-// the W_ti tile is staged once for both products.  Rows arrive through a
+// (32 x 32 each; warp 0 forms G, warp 1 H), over the rows of one chunk; the
+// W_ti tile is staged once for both products.  Rows arrive through a
 // two-stage cp.async ring (dynamic shared memory [stage][A|W|Y][col][GP]),
 // so the next 16 rows load while the current 16 are multiplied.
 constexpr int GT = 32, GK = 16, GP = GK + 1;
@@ -53,7 +62,6 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
   const double2* BY = Y + d.blk + (size_t)(tj * GT) * d.dim;
   const int r0 = chunk * chunk_rows, r1 = min(d.dim, r0 + chunk_rows);
   extern __shared__ double2 gsm[];
-  const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
   // thread -> (column c, row q) of each staged 32 x 16 slab: 16 threads per column, 256 B contiguous
   auto load = [&](int r, int b) {
     double2* s = gsm + b * 3 * GT * GP;
@@ -70,11 +78,15 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
     }
     cp_async_commit();
   };
-  double2 ag[4][4], ah[4][4];
+  // FP64 tensor path: warp 0 forms G = W_ti^H W_tj, warp 1 H = W_ti^H Y_tj, each
+  // as 4 x 4 8x8 MMA tiles; conj(w) b = (wr br + wi bi) + i (wr bi - wi br)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int fr = lane >> 2, fk = lane & 3;
+  double accr[4][4][2], acci[4][4][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) ag[a][b] = ah[a][b] = make_double2(0.0, 0.0);
+    for (int j = 0; j < 4; ++j) accr[i][j][0] = accr[i][j][1] = acci[i][j][0] = acci[i][j][1] = 0.0;
   const int nstep = (r1 - r0 + GK - 1) / GK;
   load(r0, 0);
   for (int it = 0; it < nstep; ++it) {
@@ -87,39 +99,47 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
     }
     __syncthreads();
     const double2* sA = gsm + b * 3 * GT * GP;
-    const double2* sW = sA + GT * GP;
-    const double2* sY = sW + GT * GP;
+    const double2* sB = sA + (1 + warp) * GT * GP;  // W_tj or Y_tj
 #pragma unroll
-    for (int q = 0; q < GK; ++q) {
-      double2 a[4], bw[4], by[4];
+    for (int ks = 0; ks < GK / 4; ++ks) {
+      const int q = 4 * ks + fk;
+      double wr[4], wi[4], wn[4], br[4], bi[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = sA[(ty + 8 * i) * GP + q];
+      for (int i = 0; i < 4; ++i) {
+        const double2 a = sA[(8 * i + fr) * GP + q];
+        wr[i] = a.x;
+        wi[i] = a.y;
+        wn[i] = -a.y;
+      }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        bw[j] = sW[(tx + 8 * j) * GP + q];
-        by[j] = sY[(tx + 8 * j) * GP + q];
+        const double2 bb = sB[(8 * j + fr) * GP + q];
+        br[j] = bb.x;
+        bi[j] = bb.y;
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          cfmac(ag[i][j], a[i], bw[j]);
-          cfmac(ah[i][j], a[i], by[j]);
+          dmma884(accr[i][j], wr[i], br[j]);
+          dmma884(accr[i][j], wi[i], bi[j]);
+          dmma884(acci[i][j], wr[i], bi[j]);
+          dmma884(acci[i][j], wn[i], br[j]);
         }
     }
     __syncthreads();
   }
   // partial layout: [chunk][which][pair][32*32]
-  double2* og = gpart + d.gp + ((size_t)(chunk * 2 + 0) * npair + pair) * (GT * GT);
-  double2* oh = gpart + d.gp + ((size_t)(chunk * 2 + 1) * npair + pair) * (GT * GT);
+  double2* o = gpart + d.gp + ((size_t)(chunk * 2 + warp) * npair + pair) * (GT * GT);
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      og[(ty + 8 * i) * GT + tx + 8 * j] = ag[i][j];
-      oh[(ty + 8 * i) * GT + tx + 8 * j] = ah[i][j];
-    }
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        o[(8 * i + fr) * GT + 8 * j + 2 * fk + e] = make_double2(accr[i][j][e], acci[i][j][e]);
 }
+
 
 // Sum partials (fixed order) and complete the Hermitian matrices G, H
 // (column-major k x k at kk and kk + k*k).
@@ -569,13 +589,6 @@ __global__ void k_coef(const ProbDesc* __restrict__ pd, const ProbState* __restr
 constexpr int RR = 128, RC = 32, RK = 8, RS = 3;
 constexpr int kRotStage = RK * RR + RK * RC;  // double2 per stage
 constexpr int kRotSmem = RS * kRotStage * (int)sizeof(double2);
-
-// d(8x8, 2 per thread) += a(8x4, 1 per thread) b(4x8, 1 per thread), FP64 tensor MMA
-__device__ __forceinline__ void dmma884(double (&acc)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(acc[0]), "+d"(acc[1])
-               : "d"(a), "d"(b));
-}
 
 // V = W C on the FP64 tensor path (mma.sync m8n8k4 f64): CTA tile 128 rows x
 // 32 columns, W and C slabs of RK columns/rows through a three-stage cp.async
