@@ -368,6 +368,7 @@ def measure_sourceshape(solver, stream, batch, no_cpu, reps=4):
     ms = e0.elapsed_time(e1) / n
     fl = sourceshape_flops(L, nev)
     out = {"workload": f"psi(r) of {L}^3 x nev {nev}, (L/2)^3 = {(L // 2) ** 3} displacements, FP64",
+           "kernel": "k_ss_tile, FP64 tensor path (mma.sync m8n8k4.f64)",
            "ms_per_timeslice": ms, "tflops": fl / (ms / 1e3) / 1e12, "bound": "fp64",
            "fp64_peak_tflops": 33.5, "peak_source": "FP64 FMA loop measured on this pool's B200",
            "frac": fl / (ms / 1e3) / 1e12 / 33.5, "timeslices": n}

@@ -256,7 +256,9 @@ int laph_solver_displace(laph_solver* s, int i, int dir, double* W, int on_devic
  * laph_sourceshape takes a column-major complex128 eigensystem [3 V3][nev]
  * in host (on_device = 0) or device memory; laph_solver_sourceshape works on
  * problem i of a solver that has run, in place on the device (weighted != 0:
- * by sqrt of its eigenvalues). */
+ * by sqrt of its eigenvalues).  The tile products run on the FP64 tensor path;
+ * the environment variable LAPH_SOURCESHAPE_KERNEL=0, read once per process,
+ * selects the FP64-FMA kernel instead (same results to rounding). */
 int laph_sourceshape(const double* V, int L, int nev, const double* evals, int on_device, double* psi, int device);
 int laph_solver_sourceshape(laph_solver* s, int i, int weighted, double* psi);
 /* avg_radii (sourceshape_funcs.cpp:100-135): psi averaged over grid points of

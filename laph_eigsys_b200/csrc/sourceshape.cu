@@ -18,13 +18,18 @@
 //               of sourceshape_funcs.cpp:85-96)
 //   k_ss_tile : one CTA per (class, upper 32x32 site-tile pair): FP64 tile
 //               GEMM through a 2-stage cp.async ring, norms, per-CTA shared
-//               bins (L <= 32) flushed with one atomic per touched bin
+//               bins (L <= 32) flushed with one atomic per touched bin.  The
+//               product runs on the FP64 tensor path (mma m8n8k4, 16 warps of
+//               24 x 24 rows x columns, four real MMAs per complex one) by
+//               default; LAPH_SOURCESHAPE_KERNEL=0 selects the FP64-FMA form
+//               (one thread per 2 x 1 site pairs, 18 complex accumulators).
 //
 // FP64 throughout (parity with the FP64 reference to 1e-12 relative); the
 // bins are summed with atomics, so the last bits depend on the order.
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -33,6 +38,13 @@
 
 namespace laph {
 namespace {
+
+// d(8x8, 2 per thread) += a(8x4, 1 per thread) b(4x8, 1 per thread), FP64 tensor MMA
+__device__ __forceinline__ void dmma884(double (&acc)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(acc[0]), "+d"(acc[1])
+               : "d"(a), "d"(b));
+}
 
 constexpr int kSsSites = 32;               // sites per tile side
 constexpr int kSsRows = 3 * kSsSites;      // rows per tile side
@@ -64,6 +76,9 @@ __global__ void k_ss_pack(const double2* __restrict__ V, int L, int nev, const d
   }
 }
 
+// kDmma: the tile product on the FP64 tensor path (mma m8n8k4), else FP64 FMAs with one
+// thread per site pair
+template <bool kDmma>
 __global__ void __launch_bounds__(512, 1) k_ss_tile(const double2* __restrict__ Vp, int L, int nev,
                                                  double* __restrict__ psi) {
   const int H = L / 2, Nc = H * H * H, R = 3 * Nc;
@@ -97,6 +112,92 @@ __global__ void __launch_bounds__(512, 1) k_ss_tile(const double2* __restrict__ 
     }
     cp_async_commit();
   };
+  if constexpr (kDmma) {
+  // FP64 tensor path: the tile pair is a 96 x 96 complex product P = A B^H over
+  // K = nev; warp (wr, wc) of the 4 x 4 warp grid owns the 24 x 24 block of
+  // rows 24 wr.., columns 24 wc.. (8 x 8 site pairs, 3 x 3 MMA tiles of 8 x 8);
+  // a conj(b) = (ar br + ai bi) + i (ai br - ar bi) as four real MMAs.
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wr = warp >> 2, wc = warp & 3;
+  const int fr = lane >> 2, fk = lane & 3;
+  double accr[3][3][2], acci[3][3][2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) accr[i][j][0] = accr[i][j][1] = acci[i][j][0] = acci[i][j][1] = 0.0;
+  const int nstep = (nev + kSsK - 1) / kSsK;
+  load(0, 0);
+  for (int it = 0; it < nstep; ++it) {
+    const int st = it & 1;
+    if (it + 1 < nstep) {
+      load((it + 1) * kSsK, st ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double2* A = ssm + st * kSsStage;
+    const double2* B = A + kSsK * kSsRows;
+#pragma unroll
+    for (int ks = 0; ks < kSsK / 4; ++ks) {
+      const int q = 4 * ks + fk;
+      double ar[3], ai[3], br[3], bi[3], bn[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double2 a = A[q * kSsRows + 24 * wr + 8 * i + fr];
+        ar[i] = a.x;
+        ai[i] = a.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double2 b = B[q * kSsRows + 24 * wc + 8 * j + fr];
+        br[j] = b.x;
+        bi[j] = b.y;
+        bn[j] = -b.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          dmma884(accr[i][j], ar[i], br[j]);
+          dmma884(accr[i][j], ai[i], bi[j]);
+          dmma884(acci[i][j], ai[i], br[j]);
+          dmma884(acci[i][j], ar[i], bn[j]);
+        }
+    }
+    __syncthreads();
+  }
+  // |P_ab|^2 summed per site pair in shared memory (the staging ring is free now)
+  double* sq = reinterpret_cast<double*>(ssm) + warp * 64;  // [8 y sites][8 x sites] of this warp
+  for (int e = lane; e < 64; e += 32) sq[e] = 0.0;
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int rr = 8 * i + fr, cc = 8 * j + 2 * fk + e;  // within the warp's 24 x 24 block
+        atomicAdd(&sq[(rr / 3) * 8 + cc / 3], accr[i][j][e] * accr[i][j][e] + acci[i][j][e] * acci[i][j][e]);
+      }
+  __syncwarp();
+  for (int e = lane; e < 64; e += 32) {
+    const int ys = ty * kSsSites + 8 * wr + e / 8, xs = tx * kSsSites + 8 * wc + e % 8;
+    if (ys >= Nc || xs >= Nc) continue;
+    const double f = sqrt(sq[e]);
+    const int ay = ys / (H * H), by = (ys / H) % H, cy = ys % H;
+    const int ax = xs / (H * H), bx = (xs / H) % H, cx = xs % H;
+    const int da = ay - ax, db = by - bx, dc = cy - cx;
+    const int r_fw = ((da + H) % H) * H * H + ((db + H) % H) * H + (dc + H) % H;
+    if (shared_bins) atomicAdd(&bins[r_fw], f);
+    else atomicAdd(&psi[r_fw], f);
+    if (tx != ty) {
+      const int r_bw = ((H - da) % H) * H * H + ((H - db) % H) * H + (H - dc) % H;
+      if (shared_bins) atomicAdd(&bins[r_bw], f);
+      else atomicAdd(&psi[r_bw], f);
+    }
+  }
+  } else {
   // thread: y sites py, py + 16 of tile ty; x site px of tile tx (a warp shares py)
   const int py = threadIdx.x >> 5, px = threadIdx.x & 31;
   double2 acc[2][9];
@@ -157,6 +258,7 @@ __global__ void __launch_bounds__(512, 1) k_ss_tile(const double2* __restrict__ 
       else atomicAdd(&psi[r_bw], f);
     }
   }
+  }
   if (shared_bins) {
     __syncthreads();
     for (int b = threadIdx.x; b < nbins; b += blockDim.x)
@@ -165,6 +267,15 @@ __global__ void __launch_bounds__(512, 1) k_ss_tile(const double2* __restrict__ 
 }
 
 bool g_ss_attr[64] = {false};
+
+// LAPH_SOURCESHAPE_KERNEL=0 selects the FP64-FMA tile kernel, 1 (default) the FP64 tensor-path one
+bool ss_use_dmma() {
+  static const bool v = [] {
+    const char* e = std::getenv("LAPH_SOURCESHAPE_KERNEL");
+    return !(e && e[0] == '0');
+  }();
+  return v;
+}
 
 }  // namespace
 
@@ -175,7 +286,8 @@ int sourceshape_device(const double2* V, int L, int nev, const double* evals, do
   int dev = 0;
   LAPH_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 64 && !g_ss_attr[dev]) {
-    LAPH_CUDA_TRY(cudaFuncSetAttribute(k_ss_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, kSsSmem));
+    LAPH_CUDA_TRY(cudaFuncSetAttribute(k_ss_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSsSmem));
+    LAPH_CUDA_TRY(cudaFuncSetAttribute(k_ss_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSsSmem));
     g_ss_attr[dev] = true;
   }
   const int H = L / 2, Nc = H * H * H;
@@ -185,7 +297,10 @@ int sourceshape_device(const double2* V, int L, int nev, const double* evals, do
   const int pb = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
   k_ss_pack<<<pb, 256, 0, st>>>(V, L, nev, evals, work, cm);
   LAPH_CUDA_TRY(cudaGetLastError());
-  k_ss_tile<<<8 * T * (T + 1) / 2, 512, kSsSmem, st>>>(work, L, nev, psi);
+  if (ss_use_dmma())
+    k_ss_tile<true><<<8 * T * (T + 1) / 2, 512, kSsSmem, st>>>(work, L, nev, psi);
+  else
+    k_ss_tile<false><<<8 * T * (T + 1) / 2, 512, kSsSmem, st>>>(work, L, nev, psi);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

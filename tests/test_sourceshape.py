@@ -2,6 +2,8 @@
 against the oracle's restatement of source_shape_complete, the radius average
 and the output files; analytic checks on the free field."""
 import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -88,6 +90,25 @@ def test_sourceshape_free_field_gpu(gpu):
     for c in range(3):
         V[c::3, c] = 1.0 / np.sqrt(V3)
     assert np.allclose(gpu.sourceshape(V, L), np.sqrt(3.0), rtol=0, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["0", "1"])
+def test_sourceshape_tile_kernels_many_tiles(gpu, orc, tmp_path, kernel):
+    """Both tile kernels (0: FP64 FMAs, 1: FP64 tensor path; chosen once per process by LAPH_SOURCESHAPE_KERNEL)
+    on L = 20: 1000 sites per parity class, 32 site tiles with a ragged last one, off-diagonal tile pairs."""
+    L, nev = 20, 16
+    rng = np.random.default_rng(20)
+    V, _ = np.linalg.qr(rng.normal(size=(3 * L ** 3, nev)) + 1j * rng.normal(size=(3 * L ** 3, nev)))
+    np.save(tmp_path / "V.npy", V)
+    script = ("import sys, numpy as np, laph_eigsys_b200 as lb; "
+              "np.save(sys.argv[2], lb.sourceshape(np.load(sys.argv[1]), int(sys.argv[3])))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run([sys.executable, "-c", script, str(tmp_path / "V.npy"), str(tmp_path / "psi.npy"), str(L)],
+                   env=dict(os.environ, LAPH_SOURCESHAPE_KERNEL=kernel), cwd=root, check=True, timeout=300)
+    psi = np.load(tmp_path / "psi.npy")
+    ref = orc.sourceshape(V, L)
+    assert np.abs(psi - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
 def test_sourceshape_rejects_odd_L():
