@@ -165,12 +165,6 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     set_error("laph_solver_create: bad argument");
     return LAPH_EINVAL;
   }
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    set_error("laph_solver_create: no CUDA device");
-    return LAPH_ENODEV;
-  }
   if (opts->deg < 2 || opts->deg > 64 || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1 ||
       opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 1) {
     set_error("laph_solver_create: need 2 <= deg <= 64, guard >= 0, tol > 0, max_it >= 1, 0 <= block <= 512, "
@@ -184,6 +178,13 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
       set_error("laph_solver_create: problem %d: need 3 <= L <= 128, 1 <= nev, block width %d <= min(512, dim/2)", i, k);
       return LAPH_EINVAL;
     }
+  }
+  // every argument is checked before the device, so a bad call reports LAPH_EINVAL on any host
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("laph_solver_create: no CUDA device");
+    return LAPH_ENODEV;
   }
   laph_solver* s = new laph_solver();
   auto fail = [&](int stt) {
