@@ -38,6 +38,15 @@ def main():
     y8 = orc.tv_iter(Us, L, 11.8, 0.6, 8, x)
     np.savez_compressed(os.path.join(OUT, "l4_seed1227.npz"), conf=conf, x=x, tv_iter_deg8_hyp=y8,
                         neglap_eigs_hyp=w, plaquette_hyp=orc.plaquette(Us, L), **smeared)
+    # the eigensystem's consumers on a stored block: the 6 lowest eigenvectors of the HYP-smeared -Delta
+    # (numpy's eigh, stored as input, so nothing depends on its phase or degenerate-subspace choices),
+    # the source shape psi(r) with its radius average, and the covariant displacement along x, y, z
+    _, Vall = np.linalg.eigh(orc.neglap_dense(Us, L))
+    V = np.asfortranarray(Vall[:, :6])
+    psi = orc.sourceshape(V, L)
+    r, avg = orc.sourceshape_avg(L, psi)
+    W = np.stack([orc.displace(Us, L, d, V) for d in range(3)])
+    np.savez_compressed(os.path.join(OUT, "l4_hyp_consumers.npz"), V=V, psi=psi, radii=r, psi_avg=avg, displaced=W)
     np.savez_compressed(os.path.join(OUT, "free_spectrum.npz"), L4=orc.free_spectrum(4), L6=orc.free_spectrum(6),
                         L8=orc.free_spectrum(8))
     print("wrote", sorted(f for f in os.listdir(OUT) if f.endswith(".npz")))

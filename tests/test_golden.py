@@ -60,3 +60,36 @@ def test_cuda_path_reproduces_fixtures(gpu):
     ev, V, ph = s.get(0)
     assert np.abs(-ev - g["neglap_eigs_hyp"][:20]).max() / 12.0 <= 1e-10
     s.close()
+
+
+def test_oracle_reproduces_consumer_fixtures(orc):
+    """Source shape, radius average and displacement of a stored HYP eigenvector block (l4_hyp_consumers.npz)."""
+    g = load("l4_seed1227.npz")
+    c = load("l4_hyp_consumers.npz")
+    L = 4
+    V = c["V"]
+    assert np.abs(V.conj().T @ V - np.eye(V.shape[1])).max() < 1e-13
+    assert np.abs(orc.sourceshape(V, L) - c["psi"]).max() <= 1e-14 * np.abs(c["psi"]).max()
+    r, a = orc.sourceshape_avg(L, c["psi"])
+    assert np.array_equal(r, c["radii"]) and np.abs(a - c["psi_avg"]).max() <= 1e-15 * np.abs(a).max()
+    for d in range(3):
+        assert np.abs(orc.displace(g["hyp"], L, d, V) - c["displaced"][d]).max() < 1e-15
+    # psi(0) = sum_x ||V_x V_x^dag||_F, straight from the definition
+    p0 = sum(np.linalg.norm(V[3 * x:3 * x + 3] @ V[3 * x:3 * x + 3].conj().T) for x in range(L ** 3))
+    assert abs(c["psi"][0] - p0) <= 1e-13 * p0
+
+
+@pytest.mark.gpu
+def test_cuda_consumers_reproduce_fixtures(gpu):
+    g = load("l4_seed1227.npz")
+    c = load("l4_hyp_consumers.npz")
+    L = 4
+    V = c["V"]
+    psi = gpu.sourceshape(V, L)
+    assert np.abs(psi - c["psi"]).max() <= 1e-12 * np.abs(c["psi"]).max()
+    ctx = gpu.Context(L, 11.8, 0.6, 8)
+    ctx.set_links(g["hyp"])
+    for d in range(3):
+        W = ctx.displace(V, d)
+        assert np.abs(W - c["displaced"][d]).max() <= 1e-14 * np.abs(c["displaced"][d]).max()
+    ctx.close()
