@@ -303,6 +303,20 @@ int laph_read_eigenvalues_bin(const char* dir, const char* prefix, int config, i
 int laph_check_trace(int dim, int nev, const double* V, double* trace, double* sum);
 /* fix_phase (modules/eigensystem.cpp:4-30) on host data. */
 int laph_fix_phase_host(int dim, int nev, const double* V, double* Vfix, double* phase);
+/* reset_phase (modules/eigensystem.cpp:32-57) on host data: column n of V
+ * rotated so that its first entry has the phase phase_want[n] (the phases
+ * file of an earlier run); Vreset may equal V. */
+int laph_reset_phase_host(int dim, int nev, const double* V, const double* phase_want, double* Vreset);
+/* read_eigenvalues_ascii (modules/read_write.cpp:99-115): "<prefix>.%03d.%04d"
+ * (timeslice, then configuration), nev whitespace-separated values.  A missing
+ * file is LAPH_EIO and a short one LAPH_ESIZE (the reference skips both
+ * silently). */
+int laph_read_eigenvalues_ascii(const char* prefix, int config, int t, int nev, double* ev);
+/* write_gauge_matrices / read_gauge_matrices (modules/read_write.cpp:117-132,
+ * 253-261): V3 raw 3x3 complex128 matrices in Eigen Matrix3cd memory order
+ * (column-major), 144 bytes each, no header; a short file is LAPH_ESIZE. */
+int laph_write_gauge_matrices(const char* path, int V3, const double* G);
+int laph_read_gauge_matrices(const char* path, int V3, double* G);
 /* recover_spectrum (modules/recover_spec.cpp:45-54). */
 int laph_recover_spectrum(int nev, const double* theta, int deg, double lam_l, double lam_c, double* out);
 

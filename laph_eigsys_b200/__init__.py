@@ -16,7 +16,8 @@ from ._lib import (LAYOUT_CONF, LAYOUT_EIGEN, LAYOUT_ROWMAJOR, LINKS_BF16, LINKS
 
 __all__ = ["Context", "Solver", "gauge_random", "lime_write_gauge", "lime_read_gauge", "lime_read_gauge_any",
            "lime_info", "parse_parameters", "sourceshape", "sourceshape_avg", "write_sourceshape", "check_trace",
-           "fix_phase", "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin", "read_eigsys_bin",
+           "fix_phase", "reset_phase", "read_eigenvalues_ascii", "write_gauge_matrices", "read_gauge_matrices",
+           "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin", "read_eigsys_bin",
            "read_eigenvalues_bin", "LaphError", "lib"]
 
 
@@ -129,6 +130,39 @@ def fix_phase(V):
     check(lib.laph_fix_phase_host(dim, nev, ctypes.c_void_p(V.ctypes.data), ctypes.c_void_p(Vf.ctypes.data),
                                   _ptr(ph)), "laph_fix_phase_host")
     return Vf, ph
+
+
+def reset_phase(V, phase_want):
+    """reset_phase: column n rotated so that its first entry has phase phase_want[n]."""
+    V = np.asfortranarray(V, dtype=np.complex128)
+    dim, nev = V.shape
+    want = np.ascontiguousarray(phase_want, dtype=np.float64)
+    Vr = np.empty_like(V, order="F")
+    check(lib.laph_reset_phase_host(dim, nev, ctypes.c_void_p(V.ctypes.data), _ptr(want),
+                                    ctypes.c_void_p(Vr.ctypes.data)), "laph_reset_phase_host")
+    return Vr
+
+
+def read_eigenvalues_ascii(prefix, config, t, nev):
+    """read_eigenvalues_ascii: nev values from "<prefix>.%03d.%04d" (timeslice, configuration)."""
+    ev = np.empty(nev)
+    check(lib.laph_read_eigenvalues_ascii(str(prefix).encode(), config, t, nev, _ptr(ev)),
+          "laph_read_eigenvalues_ascii")
+    return ev
+
+
+def write_gauge_matrices(path, G):
+    """write_gauge_matrices: (V3, 3, 3) complex128 matrices as raw Eigen (column-major) Matrix3cd."""
+    G = np.asarray(G, dtype=np.complex128)
+    raw = np.ascontiguousarray(np.swapaxes(G, 1, 2))  # row-major (a, b) -> column-major memory
+    check(lib.laph_write_gauge_matrices(str(path).encode(), G.shape[0], _ptr(raw)), "laph_write_gauge_matrices")
+
+
+def read_gauge_matrices(path, V3):
+    """read_gauge_matrices: (V3, 3, 3) complex128 matrices from raw Eigen (column-major) Matrix3cd."""
+    raw = np.empty((V3, 3, 3), dtype=np.complex128)
+    check(lib.laph_read_gauge_matrices(str(path).encode(), V3, _ptr(raw)), "laph_read_gauge_matrices")
+    return np.ascontiguousarray(np.swapaxes(raw, 1, 2))
 
 
 def recover_spectrum(theta, deg, lam_l, lam_c):

@@ -117,6 +117,10 @@ _sig("laph_read_eigsys_bin", c_int, c_char_p, c_char_p, c_int, c_int, c_int, c_i
 _sig("laph_read_eigenvalues_bin", c_int, c_char_p, c_char_p, c_int, c_int, c_int, c_void_p)
 _sig("laph_check_trace", c_int, c_int, c_int, c_void_p, P(c_double), P(c_double))
 _sig("laph_fix_phase_host", c_int, c_int, c_int, c_void_p, c_void_p, c_void_p)
+_sig("laph_reset_phase_host", c_int, c_int, c_int, c_void_p, c_void_p, c_void_p)
+_sig("laph_read_eigenvalues_ascii", c_int, c_char_p, c_int, c_int, c_int, c_void_p)
+_sig("laph_write_gauge_matrices", c_int, c_char_p, c_int, c_void_p)
+_sig("laph_read_gauge_matrices", c_int, c_char_p, c_int, c_void_p)
 _sig("laph_recover_spectrum", c_int, c_int, c_void_p, c_int, c_double, c_double, c_void_p)
 _sig("laph_parse_parameters", c_int, c_char_p, P(laph_config))
 _sig("laph_timeslice_split", c_int, c_int, c_int, c_int, P(c_int), P(c_int))

@@ -631,6 +631,91 @@ int laph_fix_phase_host(int dim, int nev, const double* Vd, double* Vfd, double*
   return LAPH_OK;
 }
 
+int laph_reset_phase_host(int dim, int nev, const double* Vd, const double* phase_want, double* Vrd) {
+  if (dim < 1 || nev < 0 || (nev > 0 && (!Vd || !phase_want || !Vrd))) {
+    set_error("laph_reset_phase_host: bad argument");
+    return LAPH_EINVAL;
+  }
+  // reset_phase (modules/eigensystem.cpp:32-57): rotate column n so that its
+  // first entry has the phase phase_want[n]
+  const cd* V = reinterpret_cast<const cd*>(Vd);
+  cd* Vr = reinterpret_cast<cd*>(Vrd);
+  for (int n = 0; n < nev; ++n) {
+    const cd fac = std::exp(cd(0.0, -(std::arg(V[(size_t)n * dim]) - phase_want[n])));
+    for (long long i = 0; i < dim; ++i) Vr[(size_t)n * dim + i] = fac * V[(size_t)n * dim + i];
+  }
+  return LAPH_OK;
+}
+
+int laph_read_eigenvalues_ascii(const char* prefix, int config, int t, int nev, double* ev) {
+  if (!prefix || nev < 0 || (nev > 0 && !ev)) {
+    set_error("laph_read_eigenvalues_ascii: bad argument");
+    return LAPH_EINVAL;
+  }
+  // read_eigenvalues_ascii (modules/read_write.cpp:99-115): "<prefix>.%03d.%04d"
+  // (timeslice first, then configuration), whitespace-separated values.  The
+  // reference skips a missing file silently and leaves unread values as they
+  // were; here both are errors.
+  char name[1100];
+  std::snprintf(name, sizeof name, "%s.%03d.%04d", prefix, t, config);
+  FILE* f = std::fopen(name, "r");
+  if (!f) {
+    set_error("cannot open %s", name);
+    return LAPH_EIO;
+  }
+  int got = 0;
+  while (got < nev && std::fscanf(f, "%lf", ev + got) == 1) ++got;
+  std::fclose(f);
+  if (got != nev) {
+    set_error("%s: %d of %d values", name, got, nev);
+    return LAPH_ESIZE;
+  }
+  return LAPH_OK;
+}
+
+int laph_write_gauge_matrices(const char* path, int V3, const double* G) {
+  if (!path || V3 < 1 || !G) {
+    set_error("laph_write_gauge_matrices: bad argument");
+    return LAPH_EINVAL;
+  }
+  // write_gauge_matrices (modules/read_write.cpp:253-261): V3 raw Matrix3cd
+  // (column-major complex128, 144 bytes each), no header
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    set_error("cannot create %s", path);
+    return LAPH_EIO;
+  }
+  const size_t n = (size_t)V3 * 18;
+  const bool ok = std::fwrite(G, sizeof(double), n, f) == n;
+  if (std::fclose(f) != 0 || !ok) {
+    set_error("%s: write failed", path);
+    return LAPH_EIO;
+  }
+  return LAPH_OK;
+}
+
+int laph_read_gauge_matrices(const char* path, int V3, double* G) {
+  if (!path || V3 < 1 || !G) {
+    set_error("laph_read_gauge_matrices: bad argument");
+    return LAPH_EINVAL;
+  }
+  // read_gauge_matrices (modules/read_write.cpp:117-132); a short file is an
+  // error here (the reference keeps whatever the failed reads left)
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    set_error("cannot open %s", path);
+    return LAPH_EIO;
+  }
+  const size_t n = (size_t)V3 * 18;
+  const size_t got = std::fread(G, sizeof(double), n, f);
+  std::fclose(f);
+  if (got != n) {
+    set_error("%s: %zu of %zu bytes", path, got * sizeof(double), n * sizeof(double));
+    return LAPH_ESIZE;
+  }
+  return LAPH_OK;
+}
+
 int laph_timeslice_split(int LT, int size, int rank, int* t0, int* count) {
   if (LT < 0 || size < 1 || rank < 0 || rank >= size || !t0 || !count) {
     set_error("laph_timeslice_split: bad argument");

@@ -49,6 +49,7 @@ _sig("orc_eps_solve", _i, _vp, _i, _d, _d, _i, _i, _i, _d, _i, ctypes.c_uint64, 
      ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_longlong))
 _sig("orc_recover_spectrum", None, _i, _vp, _i, _d, _d, _vp)
 _sig("orc_fix_phase", None, _i, _i, _vp, _vp, _vp)
+_sig("orc_reset_phase", None, _i, _i, _vp, _vp, _vp)
 _sig("orc_build_neglap_dense", None, _vp, _i, _vp)
 _sig("orc_mlp_loss_grad", _d, _vp, _vp, _vp, _i, _vp)
 _sig("orc_sourceshape", None, _vp, _i, _i, _vp)
@@ -168,6 +169,15 @@ def fix_phase(V):
     ph = np.empty(nev)
     _lib.orc_fix_phase(dim, nev, ctypes.c_void_p(V.ctypes.data), ctypes.c_void_p(Vf.ctypes.data), _p(ph))
     return Vf, ph
+
+
+def reset_phase(V, phase_want):
+    V = np.asfortranarray(V, dtype=np.complex128)
+    dim, nev = V.shape
+    want = np.ascontiguousarray(phase_want, dtype=np.float64)
+    Vr = np.empty_like(V, order="F")
+    _lib.orc_reset_phase(dim, nev, ctypes.c_void_p(V.ctypes.data), _p(want), ctypes.c_void_p(Vr.ctypes.data))
+    return Vr
 
 
 def neglap_dense(U, L):

@@ -677,6 +677,16 @@ void orc_fix_phase(int dim, int nev, const double* V, double* Vfix, double* phas
   }
 }
 
+/* reset_phase, modules/eigensystem.cpp:32-57: V_reset(:, n) = exp(-i (arg V(0, n) - want_n)) V(:, n) */
+void orc_reset_phase(int dim, int nev, const double* V, const double* phase_want, double* Vreset) {
+  const cd* v = reinterpret_cast<const cd*>(V);
+  cd* vr = reinterpret_cast<cd*>(Vreset);
+  for (int n = 0; n < nev; ++n) {
+    const cd fac = std::exp(cd(0.0, -1.0) * (std::arg(v[(size_t)n * dim]) - phase_want[n]));
+    for (long i = 0; i < dim; ++i) vr[(size_t)n * dim + i] = fac * v[(size_t)n * dim + i];
+  }
+}
+
 /* BuildLaplacian analogue (modules/config_utils.cpp:18-58): 6 on the diagonal,
  * -U_mu(i)(a,b) at (3i+a, 3up+b), -U_mu(dn)^dag(a,b) at (3i+a, 3dn+b). */
 void orc_build_neglap_dense(const double* U, int L, double* Aout) {

@@ -81,6 +81,8 @@ int orc_eps_solve(const double* links3, int L, double lam_l, double lam_c, int d
 void orc_recover_spectrum(int nev, const double* theta, int deg, double lam_l, double lam_c, double* out);
 /* fix_phase (modules/eigensystem.cpp:4-30). */
 void orc_fix_phase(int dim, int nev, const double* V, double* Vfix, double* phase);
+/* reset_phase (modules/eigensystem.cpp:32-57): first entry of column n rotated to phase_want[n]. */
+void orc_reset_phase(int dim, int nev, const double* V, const double* phase_want, double* Vreset);
 
 /* Dense Hermitian matrix of -Delta (BuildLaplacian analogue,
  * modules/config_utils.cpp:18-58), complex128 row-major [dim][dim]. */

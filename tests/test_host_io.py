@@ -201,3 +201,53 @@ def test_lime_precision_mismatch_and_missing_format(tmp_path):
     with pytest.raises(lb.LaphError) as e:
         lb.lime_read_gauge_any(r, T, L, 0, 0)
     assert e.value.status == _lib.LAPH_ESIZE
+
+
+def test_reset_phase_matches_oracle_and_is_overridden_by_fix_phase(orc):
+    """reset_phase rotates each column's first entry to the wanted phase; ev_ts then calls fix_phase on the
+    original block (src/ev_ts.cpp:304-312), so the written vectors are those of fix_phase alone."""
+    rng = np.random.default_rng(7)
+    V = rng.normal(size=(48, 5)) + 1j * rng.normal(size=(48, 5))
+    want = rng.uniform(-np.pi, np.pi, 5)
+    Vr = lb.reset_phase(V, want)
+    assert np.abs(Vr - orc.reset_phase(V, want)).max() < 1e-15
+    assert np.abs(np.angle(Vr[0]) - want).max() < 1e-13
+    assert np.allclose(np.abs(Vr), np.abs(V), rtol=0, atol=1e-15)
+    Vf, ph = lb.fix_phase(V)
+    assert np.abs(lb.reset_phase(V, ph) - V).max() < 1e-14  # the block's own phases: no change
+    assert np.abs(lb.reset_phase(V, np.zeros(5)) - Vf).max() < 1e-14  # phase 0 is fix_phase
+    assert lb.lib.laph_reset_phase_host(0, 1, None, None, None) == _lib.LAPH_EINVAL
+    assert lb.lib.laph_reset_phase_host(48, 1, None, None, None) == _lib.LAPH_EINVAL
+
+
+def test_read_eigenvalues_ascii(tmp_path):
+    ev = -np.sort(np.random.default_rng(3).uniform(0, 2, 7))
+    pre = tmp_path / "eigenvalues"
+    # timeslice first, then configuration; any whitespace between values
+    (tmp_path / "eigenvalues.005.1227").write_text("  ".join(repr(float(v)) for v in ev[:3]) + "\n"
+                                                    + "\n".join(repr(float(v)) for v in ev[3:]) + "\n")
+    assert np.array_equal(lb.read_eigenvalues_ascii(pre, 1227, 5, 7), ev)
+    assert np.array_equal(lb.read_eigenvalues_ascii(pre, 1227, 5, 4), ev[:4])
+    with pytest.raises(lb.LaphError) as e:
+        lb.read_eigenvalues_ascii(pre, 1227, 5, 8)
+    assert e.value.status == _lib.LAPH_ESIZE
+    with pytest.raises(lb.LaphError) as e:
+        lb.read_eigenvalues_ascii(pre, 1227, 6, 7)
+    assert e.value.status == _lib.LAPH_EIO
+
+
+def test_gauge_matrices_file_is_raw_eigen_matrix3cd(tmp_path):
+    G = lb.gauge_random(3, 1, 0.5, 21)[0, :, 0]  # 27 SU(3) matrices, row-major (a, b)
+    p = tmp_path / "gauge_trafo.bin"
+    lb.write_gauge_matrices(p, G)
+    raw = np.fromfile(p, dtype=np.complex128).reshape(27, 9)
+    assert raw.nbytes == 27 * 144
+    # Eigen memory order is column-major: entry (a, b) at 3 b + a
+    assert all(raw[v, 3 * b + a] == G[v, a, b] for v in (0, 13, 26) for a in range(3) for b in range(3))
+    assert np.array_equal(lb.read_gauge_matrices(p, 27), G)
+    with pytest.raises(lb.LaphError) as e:
+        lb.read_gauge_matrices(p, 28)
+    assert e.value.status == _lib.LAPH_ESIZE
+    with pytest.raises(lb.LaphError) as e:
+        lb.read_gauge_matrices(tmp_path / "missing", 27)
+    assert e.value.status == _lib.LAPH_EIO
