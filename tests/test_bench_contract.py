@@ -1,0 +1,51 @@
+"""bench.py's reference arm on CPU: one JSON line with the contract's keys, at
+least 3 warm-up steps, and under torchrun with two ranks only rank 0 works and
+prints while the other exits 0."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ARGS = ["bench.py", "--impl", "reference", "--config", "c1", "--steps", "1", "--warmup", "0"]
+
+
+def _env():
+    e = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        e.pop(k, None)
+    e["OMP_NUM_THREADS"] = "2"
+    return e
+
+
+def _json_lines(out):
+    return [json.loads(ln) for ln in out.splitlines() if ln.startswith("{")]
+
+
+def test_reference_arm_line():
+    r = subprocess.run([sys.executable] + ARGS, cwd=ROOT, capture_output=True, text=True, timeout=600, env=_env())
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1
+    ln = lines[0]
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in ln, k
+    assert ln["impl"] == "reference" and ln["n_gpus"] == 1 and ln["steps"] == 1 and ln["warmup"] >= 3
+    assert ln["value"] > 0 and ln["higher_is_better"] is True and ln["unit"] == "timeslices/s"
+    assert "workload" in ln["config"] and ln["data"] == "synthetic"
+    cb = ln["cpu_baseline"]
+    assert cb["value"] == ln["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    e = ln["e2e"]
+    assert e["value"] == ln["value"] and e["unit"] == ln["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    assert abs(ln["ms_per_step"] - 1000.0 / ln["value"]) <= 1e-6 * ln["ms_per_step"]
+
+
+def test_reference_arm_two_ranks_rank0_only():
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", "29517"] + ARGS + ["--gpus", "2"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900, env=_env())
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1 and lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
