@@ -142,3 +142,44 @@ def test_tune_hyp_argument_and_grid_errors(tmp_path):
         (tmp_path / "parameters.txt").write_text((tmp_path / "parameters.txt").read_text() + "alpha_1_f = 0.5\n")
         r = _run(TUNE, ["--ts", "2", "--conf", "1227"], tmp_path)
         assert r.returncode == 1 and "laph_tune_hyp: solver:" in r.stderr
+
+
+SHAPE = os.path.join(ROOT, "laph_eigsys_b200", "laph_sourceshape")
+
+
+def _shape_setup(tmp_path, L=6, nev=8, cfgno=1227, t=3):
+    ind = tmp_path / "eigsys"
+    ind.mkdir(exist_ok=True)
+    (tmp_path / "parameters.txt").write_text(f"in_path = {ind}\nLT = 8\nLX = {L}\nNEV = {nev}\n")
+    rng = np.random.default_rng(cfgno + t)
+    dim = 3 * L ** 3
+    Q, _ = np.linalg.qr(rng.normal(size=(dim, nev)) + 1j * rng.normal(size=(dim, nev)))
+    Q = np.asfortranarray(Q)
+    lb.write_eigsys_bin(ind, "eigenvectors", cfgno, t, Q)
+    return ind, Q
+
+
+def test_sourceshape_cli_errors(tmp_path):
+    r = _run(SHAPE, [], tmp_path)
+    assert r.returncode == 2 and "configuration timeslice dim(V)" in r.stdout
+    r = _run(SHAPE, ["1", "2"], tmp_path)
+    assert r.returncode == 2
+    r = _run(SHAPE, ["--bogus", "1", "2", "3"], tmp_path)
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = _run(SHAPE, ["1227", "3", "8"], tmp_path)
+    assert r.returncode == 1 and "parameters" in r.stderr
+    ind, Q = _shape_setup(tmp_path)
+    r = _run(SHAPE, ["1227", "4", "8"], tmp_path)  # no eigensystem for timeslice 4
+    assert r.returncode == 1 and "read eigenvectors" in r.stderr
+    r = _run(SHAPE, ["1227", "3", "9"], tmp_path)  # more columns than the file holds
+    assert r.returncode == 1 and "read eigenvectors" in r.stderr
+    r = _run(SHAPE, ["--weighted", "1227", "3", "8"], tmp_path)  # no eigenvalues file
+    assert r.returncode == 1 and "read eigenvalues" in r.stderr
+    (Q * 1.01).tofile(ind / "eigenvectors.1227.003")  # fails check_trace
+    r = _run(SHAPE, ["1227", "3", "8"], tmp_path)
+    assert r.returncode == 1 and "damaged" in r.stderr
+    if not _has_device():
+        _shape_setup(tmp_path)
+        r = _run(SHAPE, ["1227", "3", "8"], tmp_path)
+        assert r.returncode == 1 and "laph_sourceshape: sourceshape:" in r.stderr
+        assert not list(tmp_path.glob("sourceshape_nev*"))

@@ -84,3 +84,31 @@ def test_ev_ts_cli_fp32_input_and_resume(gpu, orc, tmp_path):
     assert os.path.getsize(out / f"phases.{cfgno:04d}.001") == 8 * nev
     after = lb.read_eigenvalues_bin(out, "eigenvalues", cfgno, 1, nev)
     assert np.abs(after - before).max() < 1e-9
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_sourceshape_cli(gpu, orc, tmp_path, weighted):
+    """laph_sourceshape CONFIG T NEV (the reference's sourceshape program) against the oracle's source shape and
+    radius average of the same eigensystem file."""
+    L, nev, cfgno, t = 6, 8, 1227, 3
+    ind = tmp_path / "eigsys"
+    ind.mkdir()
+    (tmp_path / "parameters.txt").write_text(f"in_path = {ind}\nLT = 8\nLX = {L}\nNEV = {nev}\n")
+    rng = np.random.default_rng(5)
+    dim = 3 * L ** 3
+    Q, _ = np.linalg.qr(rng.normal(size=(dim, nev)) + 1j * rng.normal(size=(dim, nev)))
+    Q = np.asfortranarray(Q)
+    lb.write_eigsys_bin(ind, "eigenvectors", cfgno, t, Q)
+    ev = -np.sort(rng.uniform(0.1, 2.0, nev))
+    lb.write_eigenvalues_bin(ind, "eigenvalues", cfgno, t, ev)
+    exe = os.path.join(ROOT, "laph_eigsys_b200", "laph_sourceshape")
+    args = (["--weighted"] if weighted else []) + [str(cfgno), str(t), str(nev)]
+    r = subprocess.run([exe] + args, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    Vw = Q * np.sqrt(np.abs(ev))[None, :] if weighted else Q
+    rr, aa = orc.sourceshape_avg(L, orc.sourceshape(Vw, L))
+    raw = np.fromfile(tmp_path / f"sourceshape_nev{nev}.{cfgno:04d}.{t:03d}.bin", dtype=np.float64).reshape(-1, 2)
+    assert np.array_equal(raw[:, 0], rr)
+    assert np.abs(raw[:, 1] - aa).max() <= 1e-12 * np.abs(aa).max()
+    txt = open(tmp_path / f"sourceshape_nev{nev}.{cfgno}.{t}").read().splitlines()
+    assert txt[0] == "#r\tpsi(r)" and len(txt) == len(rr) + 1
