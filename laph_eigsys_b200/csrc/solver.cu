@@ -584,7 +584,6 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   s->ms[2] = b - a - filt_ms;
   s->ran = 1;
   int status = LAPH_OK;
-  std::vector<double> nrm(s->blk_total ? 0 : 0);
   for (int i = 0; i < s->np; ++i) {
     const ProbState& p = s->hps[i];
     if (p.active) status = LAPH_ENOTCONV;

@@ -140,3 +140,30 @@ def test_block_solver_frozen_tiles(gpu, orc):
     check_solution(A, w, X, ev, V, ph, nev, tol)
     assert abs(res[0]["trace_vdv"] - nev) < 1e-9
     s.close()
+
+
+def test_max_it_reached_reports_not_converged(gpu):
+    """max_it = 2 (the first Rayleigh-Ritz and one filter pass) at tol 1e-13: LAPH_ENOTCONV for the batch and for
+    every problem, where the reference sets nconv = nev and carries on; the block is still orthonormal and can be
+    fetched, and a solver with room to converge returns LAPH_OK on the same links."""
+    L, nev = 6, 12
+    links = [random_links(L, 0.4, 30 + i) for i in range(2)]
+    s = gpu.Solver([(L, nev), (L, nev)], tol=1e-13, deg=8, max_it=2, window=gpu.WINDOW_LANCZOS)
+    for i in range(2):
+        s.set_links(i, links[i])
+    st, res = s.run()
+    assert st == gpu._lib.LAPH_ENOTCONV
+    assert "max_it" in gpu.lib.laph_last_error().decode()
+    for r in res:
+        assert r["status"] == gpu._lib.LAPH_ENOTCONV and 1 <= r["iters"] <= 2
+        assert r["max_resid"] > 1e-13 and r["nconv"] < nev
+        assert abs(r["trace_vdv"] - nev) < 1e-9
+    ev, V, ph = s.get(0)
+    assert np.abs(V.conj().T @ V - np.eye(nev)).max() < 1e-10
+    s.close()
+    s = gpu.Solver([(L, nev), (L, nev)], tol=1e-10, deg=8, max_it=300, window=gpu.WINDOW_LANCZOS)
+    for i in range(2):
+        s.set_links(i, links[i])
+    st, res = s.run()
+    assert st == 0 and all(r["status"] == 0 for r in res)
+    s.close()
