@@ -350,6 +350,49 @@ def measure_matvec_fp64(cfg, batch, device, deg=12, reps=20):
             "timing": "host clock around synchronised device-pointer calls (each call synchronises its stream)"}
 
 
+def measure_lime_io(L=32, T=16, no_cpu=False):
+    """The LIME/ILDG gauge reader on the host: a seeded L^3 x T FP64 configuration written to a scratch directory
+    beside this file, then read whole with laph_lime_read_gauge once after dropping the file from the page cache
+    (fsync + POSIX_FADV_DONTNEED) and once warm; beside it the oracle's restatement of the reference's reader
+    (read_lime_gauge_field_doubleprec_timeslices: one thread, the whole file) on the warm file.  Bytes = the
+    binary record, V3 T 72 8."""
+    import tempfile
+    import laph_eigsys_b200 as lb
+    nbytes = L ** 3 * T * 72 * 8
+    out = {"workload": f"{L}^3 x {T} FP64 ILDG file, all timeslices", "bytes": nbytes, "threads": os.cpu_count()}
+    with tempfile.TemporaryDirectory(dir=os.path.dirname(os.path.abspath(__file__)), prefix="_lime_") as tmp:
+        path = os.path.join(tmp, "conf.1227")
+        conf = lb.gauge_random(L, T, 0.3, 1227)
+        lb.lime_write_gauge(path, conf, L, T)
+        fd = os.open(path, os.O_RDONLY)
+        try:
+            os.fsync(fd)
+            os.posix_fadvise(fd, 0, 0, os.POSIX_FADV_DONTNEED)
+            out["cold_cache"] = "dropped (fsync + POSIX_FADV_DONTNEED)"
+        except OSError as e:
+            out["cold_cache"] = f"not dropped: {e}"
+        finally:
+            os.close(fd)
+        t0 = time.perf_counter()
+        got = lb.lime_read_gauge(path, T, L, 0, T - 1)
+        t1 = time.perf_counter()
+        out["cold_gbs"] = nbytes / (t1 - t0) / 1e9
+        t0 = time.perf_counter()
+        got = lb.lime_read_gauge(path, T, L, 0, T - 1)
+        t1 = time.perf_counter()
+        out["warm_gbs"] = nbytes / (t1 - t0) / 1e9
+        out["matches_written"] = bool(np.array_equal(got, conf))
+        del got
+        if not no_cpu:
+            import oracle as orc
+            t0 = time.perf_counter()
+            st, ref = orc.lime_read_gauge(path, T, L, 0, T - 1)
+            t1 = time.perf_counter()
+            out["oracle_reader_warm_gbs"] = nbytes / (t1 - t0) / 1e9
+            out["oracle_matches"] = bool(st == 0 and np.array_equal(ref, conf))
+    return out
+
+
 def measure_sourceshape(solver, stream, batch, no_cpu, reps=4):
     """psi(r) of the first solved timeslices in place on the device (CUDA events on the solver's stream), and the
     oracle's restatement on one 16^3 eigensystem beside the device kernel on the same input."""
@@ -413,6 +456,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-shape", action="store_true")
+    ap.add_argument("--no-io", action="store_true")
     ap.add_argument("--plain-timeslices", type=int, default=2)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -562,6 +606,14 @@ def main():
         shape = measure_sourceshape(solver, stream, batch, args.no_cpu)
         disp = measure_displacement(solver, stream, batch)
 
+    # ---- the gauge reader (host, rank 0, N = 1) --------------------------------
+    lime_io = None
+    if rank == 0 and world == 1 and not args.no_io:
+        try:
+            lime_io = measure_lime_io(no_cpu=args.no_cpu)
+        except OSError as e:
+            lime_io = {"error": str(e)}
+
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -581,7 +633,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
                 "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-                "sourceshape": shape, "displacement": disp,
+                "sourceshape": shape, "displacement": disp, "lime_io": lime_io,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid, "filter_ms_per_step": filt_ms / args.steps,
                            "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
                                                        solver.timings()))}}

@@ -12,7 +12,9 @@
 #include <string>
 #include <vector>
 #ifdef _OPENMP
+#include <errno.h>
 #include <omp.h>
+#include <unistd.h>
 #endif
 
 #include "../../include/laph_gpu.h"
@@ -307,31 +309,60 @@ int lime_find_binary(FILE* f, const char* path, uint64_t* len, std::string* xml)
 
 // Timeslices [t_i, t_f] of an ILDG payload with es-byte big-endian reals at the
 // file position, into conf in the LAPH_LAYOUT_CONF order (FP32 widened).
+// The file order is t, z, y, x (x fastest), so every (t, z) plane is one
+// contiguous run of L^2 sites; the planes are independent units of work: each
+// OpenMP thread reads whole planes with pread (the FILE position is left as it
+// is) and byte-swaps them into their sites, so the read and the reorder both
+// run on every core and many reads are in flight for a cold file.
 int lime_read_payload(FILE* f, const char* path, int L, int t_i, int t_f, int es, double* conf) {
   const long long V3 = (long long)L * L * L;
-  if (fseeko(f, (off_t)((uint64_t)t_i * V3 * 72 * es), SEEK_CUR) != 0) {
-    set_error("%s: seek failed", path);
+  const off_t base = ftello(f);
+  if (base < 0) {
+    set_error("%s: cannot locate the binary record", path);
     return LAPH_EIO;
   }
-  std::vector<unsigned char> buf((size_t)L * 72 * es);
-  for (int t = t_i; t <= t_f; ++t)
-    for (int z = 0; z < L; ++z)
-      for (int y = 0; y < L; ++y) {
-        if (std::fread(buf.data(), 1, buf.size(), f) != buf.size()) {
-          set_error("LIME read error while reading file %s", path);
-          return LAPH_EIO;
-        }
+  const int fd = fileno(f);
+  const size_t plane = (size_t)L * L * 72 * es;
+  const off_t start = base + (off_t)((uint64_t)t_i * V3 * 72 * es);
+  const long long nplanes = (long long)(t_f - t_i + 1) * L;
+  int failed = 0;
+#pragma omp parallel
+  {
+    std::vector<unsigned char> buf(plane);
+#pragma omp for schedule(dynamic, 1)
+    for (long long pz = 0; pz < nplanes; ++pz) {
+      if (__atomic_load_n(&failed, __ATOMIC_RELAXED)) continue;
+      const off_t off = start + (off_t)(pz * (long long)plane);
+      size_t got = 0;
+      while (got < plane) {
+        const ssize_t r = pread(fd, buf.data() + got, plane - got, off + (off_t)got);
+        if (r < 0 && errno == EINTR) continue;
+        if (r <= 0) break;
+        got += (size_t)r;
+      }
+      if (got != plane) {
+        __atomic_store_n(&failed, 1, __ATOMIC_RELAXED);
+        continue;
+      }
+      const long long t = pz / L;
+      const int z = (int)(pz % L);
+      for (int y = 0; y < L; ++y)
         for (int x = 0; x < L; ++x) {
-          double* site = conf + ((long long)(t - t_i) * V3 + (long long)x * L * L + (long long)y * L + z) * 72;
+          double* site = conf + (t * V3 + (long long)x * L * L + (long long)y * L + z) * 72;
+          const unsigned char* src = &buf[((size_t)y * L + x) * 72 * es];
           for (int mu = 0; mu < 4; ++mu) {
             const int slot = (mu == 3) ? 0 : mu + 1;
             for (int k = 0; k < 18; ++k) {
-              const unsigned char* q = &buf[((size_t)x * 72 + mu * 18 + k) * es];
+              const unsigned char* q = src + (size_t)(mu * 18 + k) * es;
               if (es == 8) {
-                const uint64_t v = get_be64(q);
+                uint64_t v;
+                std::memcpy(&v, q, 8);
+                v = __builtin_bswap64(v);
                 std::memcpy(&site[slot * 18 + k], &v, 8);
               } else {
-                const uint32_t v = (uint32_t)q[0] << 24 | (uint32_t)q[1] << 16 | (uint32_t)q[2] << 8 | q[3];
+                uint32_t v;
+                std::memcpy(&v, q, 4);
+                v = __builtin_bswap32(v);
                 float fv;
                 std::memcpy(&fv, &v, 4);
                 site[slot * 18 + k] = fv;
@@ -339,7 +370,12 @@ int lime_read_payload(FILE* f, const char* path, int L, int t_i, int t_f, int es
             }
           }
         }
-      }
+    }
+  }
+  if (failed) {
+    set_error("LIME read error while reading file %s", path);
+    return LAPH_EIO;
+  }
   return LAPH_OK;
 }
 

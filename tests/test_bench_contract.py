@@ -49,3 +49,12 @@ def test_reference_arm_two_ranks_rank0_only():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)
     assert len(lines) == 1 and lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
+
+
+def test_lime_io_measurement_small():
+    sys.path.insert(0, ROOT)
+    import bench
+    out = bench.measure_lime_io(L=4, T=3)
+    assert out["matches_written"] and out["oracle_matches"]
+    assert out["bytes"] == 4 ** 3 * 3 * 72 * 8 and out["cold_gbs"] > 0 and out["warm_gbs"] > 0
+    assert not [p for p in os.listdir(ROOT) if p.startswith("_lime_")]
