@@ -611,8 +611,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_io:
         try:
             lime_io = measure_lime_io(no_cpu=args.no_cpu)
-        except OSError as e:
-            lime_io = {"error": str(e)}
+        except Exception as e:  # a host file-system problem must not cost the headline line
+            lime_io = {"error": f"{type(e).__name__}: {e}"}
 
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
     cpu = None
