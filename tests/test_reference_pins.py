@@ -1,0 +1,99 @@
+"""Pins against the reference's own code: oracle/_ref/ref_dump is built from the
+reference's modules/par_io.cpp and modules/navigation.cpp (the parts of the path
+that compile without Eigen, PETSc, SLEPc and c-lime).  laph_parse_parameters must
+read every parameters.txt the way IO::set_values does, quirks included, and the
+oracle's site indexing must use the reference's Nav lookup tables."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import laph_eigsys_b200 as lb
+from laph_eigsys_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
+
+pytestmark = pytest.mark.skipif(not os.path.isfile(REF), reason="oracle/_ref/ref_dump not built (no reference here)")
+
+
+def ref(mode, path):
+    r = subprocess.run([REF, mode, str(path)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    return json.loads(r.stdout)
+
+
+FULL = ("# LapH parameters\nconfig_path = /gauges/A40\nresult_path = /out\nin_path = /in\nphase_path = /ph\n"
+        "LT = 48\nLX = 24\nNEV = 120\nalpha_1 = 0.62\nalpha_2 = 0.52\nalpha_1_i = 0.4\nalpha_1_f = 0.75\n"
+        "alpha_2_i = 0.3\nalpha_2_f = 0.65\niter = 3\nLAM_L = 11.8\nLAM_C = 0.6\nDEG = 8\nOMP_THRDS = 4\n")
+
+CASES = {
+    "full": FULL,
+    "unterminated_last_line": FULL + "DEG = 12",
+    "no_space_around_equals": FULL + "LT=99\nNEV=7\n",
+    "duplicate_keys_last_wins": FULL + "LX = 16\nLAM_C = 0.75\n",
+    "extra_space_in_key": FULL.replace("DEG = 8", "DEG  = 8"),
+    "line_without_equals": FULL + "just some words\n",
+    "trailing_space_value": FULL + "iter = \n",
+    "crlf": FULL.replace("\n", "\r\n"),
+    "exponents_and_signs": FULL + "LAM_C = 6e-1\nalpha_1 = +0.5\nNEV = 0120\n",
+    "missing_keys": "LT = 8\nLX = 4\n",
+    "comment_not_first_char": FULL + " # not a comment = 5\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_parser_matches_reference(tmp_path, name):
+    p = tmp_path / "parameters.txt"
+    p.write_bytes(CASES[name].encode())
+    r = ref("params", p)
+    assert not r["threw"]
+    c = lb.parse_parameters(p)
+    for k in ("LT", "LX", "NEV", "iter", "DEG", "OMP_THRDS", "V3", "MAT_ENTRIES", "V_TS"):
+        assert c[k] == r[k], k
+    for k, rk in (("alpha_1", "alpha_1"), ("alpha_2", "alpha_2"), ("alpha_1_i", "alpha_1_i"),
+                  ("alpha_1_f", "alpha_1_f"), ("alpha_2_i", "alpha_2_i"), ("alpha_2_f", "alpha_2_f"),
+                  ("LAM_L", "lambda_l"), ("LAM_C", "lambda_c")):
+        assert c[k] == r[rk], k
+    for k, rk in (("config_path", "conf"), ("result_path", "res"), ("in_path", "in_path"),
+                  ("phase_path", "phase_path")):
+        assert c[k] == r[rk], k
+
+
+@pytest.mark.parametrize("text", ["LT = 4\n\nLX = 4\n", "LT = 4\nLX =\n", FULL + "NEV = 1\n\n"])
+def test_parser_errors_where_reference_throws(tmp_path, text):
+    p = tmp_path / "parameters.txt"
+    p.write_text(text)
+    assert ref("params", p)["threw"]
+    with pytest.raises(lb.LaphError) as e:
+        lb.parse_parameters(p)
+    assert e.value.status == _lib.LAPH_EPARSE
+
+
+@pytest.mark.parametrize("L", [3, 4, 6])
+def test_oracle_indexing_uses_reference_lookup_tables(tmp_path, orc, L):
+    """Site i = x L^2 + y L + z with periodic neighbours (Nav::init): the oracle's assembled -Delta with unit links
+    has -1 exactly at (3i + a, 3 up(i, mu) + a) and (3i + a, 3 dn(i, mu) + a), 6 on the diagonal."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    V3 = L ** 3
+    x, y, z = np.meshgrid(np.arange(L), np.arange(L), np.arange(L), indexing="ij")
+    idx = lambda a, b, c: ((a % L) * L * L + (b % L) * L + (c % L)).ravel()  # noqa: E731
+    assert np.array_equal(up[:, 0], idx(x + 1, y, z)) and np.array_equal(dn[:, 0], idx(x - 1, y, z))
+    assert np.array_equal(up[:, 1], idx(x, y + 1, z)) and np.array_equal(dn[:, 1], idx(x, y - 1, z))
+    assert np.array_equal(up[:, 2], idx(x, y, z + 1)) and np.array_equal(dn[:, 2], idx(x, y, z - 1))
+    U = np.zeros((V3, 3, 3, 3), dtype=np.complex128)
+    U[:, :] = np.eye(3)
+    A = orc.neglap_dense(U, L)
+    B = np.zeros((3 * V3, 3 * V3))
+    for i in range(V3):
+        for a in range(3):
+            B[3 * i + a, 3 * i + a] += 6.0
+            for mu in range(3):
+                B[3 * i + a, 3 * up[i, mu] + a] -= 1.0
+                B[3 * i + a, 3 * dn[i, mu] + a] -= 1.0
+    assert np.array_equal(A.real, B) and not np.any(A.imag)
