@@ -10,6 +10,7 @@
 //                          ("threw": true if set_values threw)
 //   ref_dump nav FILE      {"L": L, "up": [[x, y, z] per site], "dn": [...]}
 //                          after set_values(FILE) and Nav::init()
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -57,7 +58,13 @@ int main(int argc, char** argv) {
     for (const char* k : ints) std::printf("\"%s\": %d, ", k, io->get_int(k));
     const char* floats[] = {"alpha_1", "alpha_1_i", "alpha_1_f", "alpha_2", "alpha_2_i", "alpha_2_f",
                             "lambda_l", "lambda_c"};
-    for (const char* k : floats) std::printf("\"%s\": %.17g, ", k, io->get_float(k));
+    for (const char* k : floats) {
+      const double v = io->get_float(k);
+      // non-finite values in the spellings Python's json module reads
+      if (std::isnan(v)) std::printf("\"%s\": NaN, ", k);
+      else if (std::isinf(v)) std::printf("\"%s\": %sInfinity, ", k, v < 0 ? "-" : "");
+      else std::printf("\"%s\": %.17g, ", k, v);
+    }
     json_str("conf", io->get_path("conf"), true);
     json_str("res", io->get_path("res"), true);
     json_str("in_path", io->get_path("in_path"), true);

@@ -97,3 +97,69 @@ def test_oracle_indexing_uses_reference_lookup_tables(tmp_path, orc, L):
                 B[3 * i + a, 3 * up[i, mu] + a] -= 1.0
                 B[3 * i + a, 3 * dn[i, mu] + a] -= 1.0
     assert np.array_equal(A.real, B) and not np.any(A.imag)
+
+
+KEYS_INT = ["LT", "LX", "NEV", "iter", "DEG", "OMP_THRDS"]
+KEYS_FLOAT = ["alpha_1", "alpha_2", "alpha_1_i", "alpha_1_f", "alpha_2_i", "alpha_2_f", "LAM_L", "LAM_C"]
+KEYS_PATH = ["config_path", "result_path", "in_path", "phase_path"]
+
+
+def _random_file(rng):
+    lines = []
+    for _ in range(int(rng.integers(1, 25))):
+        kind = rng.integers(0, 10)
+        if kind == 0:
+            lines.append("#" + "".join(rng.choice(list("abc =#"), size=int(rng.integers(0, 8)))))
+            continue
+        if kind == 1:
+            lines.append("".join(rng.choice(list("xyz #-"), size=int(rng.integers(1, 8)))))  # no '='
+            continue
+        if kind == 2 and rng.random() < 0.15:
+            lines.append("")  # the reference throws on an empty line
+            continue
+        pool = rng.integers(0, 4)
+        if pool == 0:
+            key = str(rng.choice(KEYS_INT))
+            val = str(rng.choice(["8", "24", "0120", "-3", "+7", "12abc", "", " 5", "3.9"]))
+        elif pool == 1:
+            key = str(rng.choice(KEYS_FLOAT))
+            val = str(rng.choice(["0.62", "6e-1", "+0.5", "-1.25e+1", "11.8", "", "1e", "nan", ".5"]))
+        elif pool == 2:
+            key = str(rng.choice(KEYS_PATH))
+            val = "/" + "".join(rng.choice(list("abc/_ =.-"), size=int(rng.integers(0, 12))))
+        else:
+            key = str(rng.choice(["LY", "ev_path_1", "lambda_l", "foo", "Lx", "NEV2"]))
+            val = "1"
+        sep = str(rng.choice([" = ", "=", " =", "= ", "  = ", " =  "]))
+        pre = " " if rng.random() < 0.05 else ""
+        lines.append(pre + key + sep + val)
+    eol = "\r\n" if rng.random() < 0.1 else "\n"
+    text = eol.join(lines)
+    if rng.random() < 0.8:
+        text += eol
+    return text
+
+
+def test_parser_fuzz_against_reference(tmp_path):
+    rng = np.random.default_rng(2024)
+    p = tmp_path / "parameters.txt"
+    threw = 0
+    for case in range(300):
+        text = _random_file(rng)
+        p.write_bytes(text.encode())
+        r = ref("params", p)
+        if r["threw"]:
+            threw += 1
+            with pytest.raises(lb.LaphError) as e:
+                lb.parse_parameters(p)
+            assert e.value.status == _lib.LAPH_EPARSE, text
+            continue
+        c = lb.parse_parameters(p)
+        for k in KEYS_INT + ["V3", "MAT_ENTRIES", "V_TS"]:
+            assert c[k] == r[k], (k, text)
+        for k in KEYS_FLOAT:
+            rk = {"LAM_L": "lambda_l", "LAM_C": "lambda_c"}.get(k, k)
+            assert c[k] == r[rk] or (np.isnan(c[k]) and np.isnan(r[rk])), (k, text)
+        for k, rk in zip(KEYS_PATH, ["conf", "res", "in_path", "phase_path"]):
+            assert c[k] == r[rk], (k, text)
+    assert 0 < threw < 300
