@@ -168,18 +168,41 @@ def generate_links(cfg, seed_offset=0):
     return out
 
 
-def make_solver(cfg, device, batch):
+def make_opts(cfg):
     import laph_eigsys_b200 as lb
     kinds = {"stout": lb.SMEAR_STOUT, "ape": lb.SMEAR_APE, "hyp": lb.SMEAR_HYP, "none": lb.SMEAR_NONE}
+    return lb.solve_opts(smear_kind=kinds[cfg["smear"]], smear_p1=cfg["p1"], smear_p2=cfg["p2"],
+                         smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
+                         link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
+                         max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
+                         filter_kernel=cfg.get("filter_kernel", 1), jacobi_sweeps=cfg.get("sweeps", 0),
+                         lam_cut=cfg.get("lam_cut0", 0.0),
+                         window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
+                             cfg.get("window", "mlp")])
+
+
+def autotune_cfg(cfg, batch, device, nsample, cache):
+    """laph_solver_autotune on the first nsample timeslices of the batch; the chosen deg / block / guard replace
+    the configuration's before the measured solver is built."""
+    import laph_eigsys_b200 as lb
+    model = None
+    if cfg.get("window", "mlp") == "mlp":
+        from laph_eigsys_b200 import window as lw
+        model = lw.load_model()
+    t0 = time.perf_counter()
+    opts, res = lb.autotune([(L, nev) for L, nev, _ in batch], [U for _, _, U in batch], nsample=nsample,
+                            opts=make_opts(cfg), model=model, device=device, cache=cache)
+    res["seconds"] = time.perf_counter() - t0
+    res["sample_timeslices"] = min(nsample, len(batch))
+    res["before"] = {"deg": cfg["deg"], "block": cfg.get("block", 0) or 32, "guard": cfg["guard"]}
+    cfg["deg"], cfg["block"], cfg["guard"] = opts.deg, opts.block, opts.guard
+    return res
+
+
+def make_solver(cfg, device, batch):
+    import laph_eigsys_b200 as lb
     probs = [(L, nev) for L, nev, _ in batch]
-    s = lb.Solver(probs, device=device, smear_kind=kinds[cfg["smear"]], smear_p1=cfg["p1"], smear_p2=cfg["p2"],
-                     smear_iters=cfg["iters"], smear_compat=cfg["compat"], guard=cfg["guard"],
-                     link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
-                     max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
-                     filter_kernel=cfg.get("filter_kernel", 1), jacobi_sweeps=cfg.get("sweeps", 0),
-                     lam_cut=cfg.get("lam_cut0", 0.0),
-                     window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
-                         cfg.get("window", "mlp")])
+    s = lb.Solver(probs, opts=make_opts(cfg), device=device)
     for i, (a1, a2) in enumerate(cfg.get("scan") or []):
         s.set_smear(i, a1, a2)  # the batched tune_hyp scan: one copy of the timeslice per grid point
     return s
@@ -457,6 +480,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-shape", action="store_true")
     ap.add_argument("--no-io", action="store_true")
+    ap.add_argument("--autotune", type=int, default=0, metavar="NSAMPLE",
+                    help="tune deg / block / guard on the first NSAMPLE timeslices before measuring (0: off)")
+    ap.add_argument("--tune-cache", default=None, help="autotuner cache file")
     ap.add_argument("--plain-timeslices", type=int, default=2)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -503,6 +529,7 @@ def main():
 
     batch = generate_links(cfg, seed_offset=rank * 1000)
     T = len(batch)
+    tune = autotune_cfg(cfg, batch, local, args.autotune, args.tune_cache) if args.autotune > 0 else None
     solver = make_solver(cfg, local, batch)
     if cfg.get("window", "mlp") == "mlp":
         from laph_eigsys_b200 import window as lw
@@ -633,7 +660,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
                 "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-                "sourceshape": shape, "displacement": disp, "lime_io": lime_io,
+                "sourceshape": shape, "displacement": disp, "lime_io": lime_io, "autotune": tune,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid, "filter_ms_per_step": filt_ms / args.steps,
                            "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
                                                        solver.timings()))}}

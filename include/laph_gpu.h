@@ -192,7 +192,8 @@ int laph_solver_create(laph_solver** s, const laph_problem* probs, int n, const 
 int laph_solver_destroy(laph_solver* s);
 /* Links of problem i: FP64, layout as above; host (on_device = 0) or device pointer. */
 int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout, int on_device);
-/* Run: smear + solve all problems.  Results stay on the device. */
+/* Run: smear + solve all problems.  Results stay on the device; results (may be
+ * NULL) receives one laph_result per problem. */
 int laph_solver_run(laph_solver* s, laph_result* results);
 /* Fetch problem i: evals[nev] (reference convention, see top), evecs column-major
  * complex128 [3*V3][nev] (may be NULL), phases[nev] (may be NULL). */
@@ -205,6 +206,41 @@ int laph_solver_timings(laph_solver* s, double* ms4);
 /* Counters of the last run for roofline accounting: filter site-vector-steps,
  * number of filter kernel launches, total device kernel launches. */
 int laph_solver_counters(laph_solver* s, long long* c3);
+
+/* ---- autotuner ------------------------------------------------------------
+ * Picks the filter degree cap (deg), the filter's columns per CTA (block) and
+ * the guard vectors (hence the block width k) for a batch, by timing solves of
+ * a sample of it.  No counterpart in the reference, whose DEG, LAM_L and LAM_C
+ * are set by hand in parameters.txt. */
+typedef struct {
+  int deg, block, guard;   /* the chosen settings (also written to opts)         */
+  double ms_per_problem;   /* device time per problem with them, on the sample   */
+  int trials;              /* settings timed (0 when read from the cache)        */
+  int from_cache;          /* 1: taken from the cache file, nothing timed        */
+} laph_tune_result;
+/* One trial: device ms per problem of the setting, or < 0 if it failed. */
+typedef double (*laph_tune_trial)(void* user, int deg, int block, int guard);
+/* The search with a caller-supplied trial: from (deg0, block0, guard0), each
+ * axis in turn (deg, block, guard), every candidate of the axis timed with the
+ * others at their best so far; a candidate replaces the best only when more
+ * than 1% faster; no setting is timed twice.  LAPH_ENOTCONV if none succeeded. */
+int laph_autotune_search(const int* deg_c, int nd, const int* block_c, int nb, const int* guard_c, int ng, int deg0,
+                         int block0, int guard0, laph_tune_trial trial, void* user, laph_tune_result* out);
+/* Tune opts (deg, block, guard; every other field kept) for a batch shaped like
+ * probs[0..n): the sample is the first min(n, nsample) problems, links[i] their
+ * FP64 host links in `layout`; each setting is timed as the faster of two runs
+ * of a solver over the sample (the first also captures its CUDA graphs), a
+ * setting that does not converge within opts->max_it is dropped.  model /
+ * nmodel: the window model (as laph_solver_set_window_model) when
+ * opts->window is LAPH_WINDOW_MLP, else ignored (may be NULL).  Candidates:
+ * deg 40, 48, 56, 60, 64 (start: opts->deg, or 60 if <= 1), block 16, 32, 64
+ * (start: opts->block, or 32), guard opts->guard and opts->guard + 32.
+ * cache_path (may be NULL): a text file of earlier results, one line per
+ * device and batch shape; a hit sets opts without timing anything, a new
+ * result is appended. */
+int laph_solver_autotune(const laph_problem* probs, int n, const double* const* links, int layout, int nsample,
+                         laph_solve_opts* opts, const float* model, int nmodel, int device, const char* cache_path,
+                         laph_tune_result* out);
 
 /* ---- learned Chebyshev window --------------------------------------------
  * A 16 -> 64 -> 64 -> 3 tanh MLP (FP32) maps per-timeslice features -- the

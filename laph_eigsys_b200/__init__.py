@@ -18,7 +18,7 @@ __all__ = ["Context", "Solver", "gauge_random", "lime_write_gauge", "lime_read_g
            "lime_info", "parse_parameters", "sourceshape", "sourceshape_avg", "write_sourceshape", "check_trace",
            "fix_phase", "reset_phase", "read_eigenvalues_ascii", "write_gauge_matrices", "read_gauge_matrices",
            "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin", "read_eigsys_bin",
-           "read_eigenvalues_bin", "LaphError", "lib"]
+           "read_eigenvalues_bin", "autotune", "autotune_search", "LaphError", "lib"]
 
 
 def _ptr(a):
@@ -292,6 +292,39 @@ class Context:
         p = ctypes.c_double()
         check(lib.laph_plaquette(self._h, ctypes.byref(p)), "laph_plaquette")
         return p.value
+
+
+def _tune_dict(r):
+    return {f: getattr(r, f) for f, _ in r._fields_}
+
+
+def autotune_search(deg_c, block_c, guard_c, start, trial):
+    """laph_autotune_search with a Python trial(deg, block, guard) -> ms per problem (< 0: failed)."""
+    arr = lambda v: (ctypes.c_int * max(len(v), 1))(*v)  # noqa: E731
+    cb = _lib.TUNE_TRIAL(lambda user, d, b, g: float(trial(d, b, g)))
+    r = _lib.laph_tune_result()
+    check(lib.laph_autotune_search(arr(deg_c), len(deg_c), arr(block_c), len(block_c), arr(guard_c), len(guard_c),
+                                   start[0], start[1], start[2], cb, None, ctypes.byref(r)), "laph_autotune_search")
+    return _tune_dict(r)
+
+
+def autotune(problems, links, nsample=4, cache=None, device=0, layout=LAYOUT_ROWMAJOR, opts=None, model=None, **kw):
+    """laph_solver_autotune: (tuned laph_solve_opts, result dict) for a batch shaped like `problems`, timed on
+    the first min(len(problems), nsample) problems with their host links; model: the window model (float32) for
+    window = WINDOW_MLP."""
+    probs = [(int(L), int(n)) for L, n in problems]
+    arr = (_lib.laph_problem * len(probs))(*[_lib.laph_problem(L, n) for L, n in probs])
+    o = opts if opts is not None else solve_opts(**kw)
+    ns = min(len(probs), nsample)
+    keep = [_c128(links[i]) for i in range(ns)]
+    ptrs = (ctypes.c_void_p * ns)(*[ctypes.c_void_p(a.ctypes.data) for a in keep])
+    m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)
+    r = _lib.laph_tune_result()
+    check(lib.laph_solver_autotune(arr, len(probs), ptrs, layout, nsample, ctypes.byref(o),
+                                   None if m is None else ctypes.c_void_p(m.ctypes.data), 0 if m is None else m.size,
+                                   device, str(cache).encode() if cache else None, ctypes.byref(r)),
+          "laph_solver_autotune")
+    return o, _tune_dict(r)
 
 
 def solve_opts(**kw):

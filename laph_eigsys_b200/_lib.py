@@ -49,6 +49,14 @@ class laph_result(ctypes.Structure):
                 ("lam_max", c_double), ("max_resid", c_double), ("trace_vdv", c_double)]
 
 
+class laph_tune_result(ctypes.Structure):
+    _fields_ = [("deg", c_int), ("block", c_int), ("guard", c_int), ("ms_per_problem", c_double),
+                ("trials", c_int), ("from_cache", c_int)]
+
+
+TUNE_TRIAL = ctypes.CFUNCTYPE(c_double, c_void_p, c_int, c_int, c_int)
+
+
 class laph_config(ctypes.Structure):
     _fields_ = [("config_path", ctypes.c_char * 512), ("result_path", ctypes.c_char * 512),
                 ("in_path", ctypes.c_char * 512), ("phase_path", ctypes.c_char * 512),
@@ -98,6 +106,10 @@ _sig("laph_mlp_grad", c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_vo
 _sig("laph_mlp_train", c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, ctypes.c_float, c_void_p, c_int)
 _sig("laph_solver_timings", c_int, c_void_p, P(c_double))
 _sig("laph_solver_counters", c_int, c_void_p, P(c_ll))
+_sig("laph_autotune_search", c_int, P(c_int), c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_int, c_int, TUNE_TRIAL,
+     c_void_p, P(laph_tune_result))
+_sig("laph_solver_autotune", c_int, P(laph_problem), c_int, P(c_void_p), c_int, c_int, P(laph_solve_opts), c_void_p,
+     c_int, c_int, ctypes.c_char_p, P(laph_tune_result))
 _sig("laph_gauge_random", c_int, c_void_p, c_int, c_int, c_double, c_u64)
 _sig("laph_lime_write_gauge", c_int, c_char_p, c_void_p, c_int, c_int)
 _sig("laph_lime_read_gauge", c_int, c_char_p, c_int, c_int, c_int, c_int, c_void_p)

@@ -57,7 +57,7 @@ def test_learned_window_ablation(gpu):
     from laph_eigsys_b200 import window
     model = window.load_model()
     L, T, nev = 16, 16, 60
-    conf = gpu.gauge_random(L, T, 0.3, 1230)  # survey config 4's 16^3 lattice seed, not a training seed
+    conf = gpu.gauge_random(L, T, 0.3, 1230)  # the 16^3 lattice seed of the mixed-volume workload, not a training seed
     out = {}
     for mode in (gpu.WINDOW_LANCZOS, gpu.WINDOW_MLP):
         s = gpu.Solver([(L, nev)] * T, smear_kind=gpu.SMEAR_APE, smear_p1=0.5, smear_iters=10, guard=16,
