@@ -372,6 +372,9 @@ typedef struct {
   int guard, block, window, solver; /* solver: 0 = block (default), 1 = plain MatShell */
   int V3, MAT_ENTRIES, V_TS;
   double alpha_1_i, alpha_1_f, alpha_2_i, alpha_2_f; /* tune_hyp scan range (par_io.cpp:75-89) */
+  int autotune;         /* > 0: laph_ev_ts tunes deg / block / guard on that many
+                           timeslices first (laph_solver_autotune); 0: off      */
+  int filter_deg;       /* block solver's filter degree cap (0: by lattice size) */
 } laph_config;
 int laph_parse_parameters(const char* path, laph_config* cfg);
 

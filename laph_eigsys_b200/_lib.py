@@ -65,7 +65,8 @@ class laph_config(ctypes.Structure):
                 ("LAM_C", c_double), ("smear", c_int), ("rho", c_double), ("alpha", c_double),
                 ("tol", c_double), ("guard", c_int), ("block", c_int), ("window", c_int), ("solver", c_int),
                 ("V3", c_int), ("MAT_ENTRIES", c_int), ("V_TS", c_int), ("alpha_1_i", c_double),
-                ("alpha_1_f", c_double), ("alpha_2_i", c_double), ("alpha_2_f", c_double)]
+                ("alpha_1_f", c_double), ("alpha_2_i", c_double), ("alpha_2_f", c_double), ("autotune", c_int),
+                ("filter_deg", c_int)]
 
 
 def _sig(name, res, *args):

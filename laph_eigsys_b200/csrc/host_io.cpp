@@ -880,6 +880,8 @@ int laph_parse_parameters(const char* path, laph_config* cfg) {
   cfg->alpha_1_f = F("alpha_1_f", 0.0);
   cfg->alpha_2_i = F("alpha_2_i", 0.0);
   cfg->alpha_2_f = F("alpha_2_f", 0.0);
+  cfg->autotune = I("autotune", 0);
+  cfg->filter_deg = I("filter_deg", 0);
   return LAPH_OK;
 }
 

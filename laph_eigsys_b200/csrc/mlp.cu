@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(64) k_mlp_backward(const float* __restrict__ P
                                                      const float* __restrict__ H2, const float* __restrict__ O,
                                                      float* __restrict__ gpart, float* __restrict__ lpart) {
   __shared__ float g[kMlpParams];
-  __shared__ float sx[kMlpIn], sh1[kMlpH], sh2[kMlpH], sdo[kMlpOut], sd2[kMlpH], sd1[kMlpH];
+  __shared__ float sx[kMlpIn], sh1[kMlpH], sh2[kMlpH], sdo[kMlpOut], sd2[kMlpH];
   const int j = threadIdx.x;
   for (int e = j; e < kMlpParams; e += blockDim.x) g[e] = 0.f;
   float loss = 0.f;
@@ -99,7 +99,6 @@ __global__ void __launch_bounds__(64) k_mlp_backward(const float* __restrict__ P
     float dh1 = 0.f;
     for (int r = 0; r < kMlpH; ++r) dh1 = fmaf(P[o_W2() + r * kMlpH + j], sd2[r], dh1);
     const float d1 = dh1 * (1.f - sh1[j] * sh1[j]);
-    sd1[j] = d1;
     // layer 1
 #pragma unroll
     for (int q = 0; q < kMlpIn; ++q) g[o_W1() + j * kMlpIn + q] += d1 * sx[q];

@@ -17,6 +17,7 @@
 // (right sizes, eigenvectors passing check_trace).
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -33,7 +34,8 @@ namespace {
 void usage() {
   std::fprintf(stderr,
                "usage: laph_ev_ts --conf N [--phase_reset 0|1] [--parameters FILE] [--resume]\n"
-               "  reads parameters.txt (keys of LapH_EigSys plus smear, rho, alpha, tol, guard, solver)\n");
+               "  reads parameters.txt (keys of LapH_EigSys plus smear, rho, alpha, tol, guard, block, filter_deg,\n"
+               "  window, solver, autotune)\n");
 }
 
 int env_int(const char* a, const char* b, int def) {
@@ -83,6 +85,12 @@ bool outputs_complete(const char* dir, int config, int t, int dim, int nev) {
   double tr = 0.0, sum = 0.0;
   return laph_check_trace(dim, nev, V.data(), &tr, &sum) == 1;
 }
+
+// The block solver's filter degree cap when parameters.txt gives none: the
+// best degree measured for the production lattice sizes (24^3 and 32^3: 60;
+// 48^3: 48); small lattices keep the library default, which they converge
+// with in a few passes.  `autotune = N` measures it for the run's own batch.
+int default_filter_deg(int L, int library_default) { return L >= 40 ? 48 : (L >= 20 ? 60 : library_default); }
 
 double trace_vdv(int dim, int nev, const double* V) {
   double tr = 0.0, sum = 0.0;
@@ -224,15 +232,31 @@ int main(int argc, char** argv) {
   o.guard = P.guard;
   o.tol = P.tol > 0 ? P.tol : 1e-9;
   o.window = P.window;
+  o.block = P.block;
+  o.deg = P.filter_deg > 0 ? P.filter_deg : default_filter_deg(L, o.deg);
+  std::vector<float> model;
+  if (o.window == LAPH_WINDOW_MLP && !load_window_model(argv[0], &model)) {
+    std::fprintf(stderr, "laph_ev_ts: window = mlp but data/window_mlp.bin is missing or invalid\n");
+    return 1;
+  }
+  if (P.autotune > 0) {
+    // deg / block / guard from timed solves of the first timeslices, cached beside the results
+    const int ns = std::min(nsolve, P.autotune);
+    std::vector<const double*> sample(ns);
+    for (int i = 0; i < ns; ++i) sample[i] = conf.data() + (size_t)todo[i] * V3 * 72;
+    const std::string cache = std::string(P.result_path) + "/laph_autotune.txt";
+    laph_tune_result tr;
+    st = laph_solver_autotune(probs.data(), nsolve, sample.data(), LAPH_LAYOUT_CONF, ns, &o,
+                              model.empty() ? nullptr : model.data(), (int)model.size(), device, cache.c_str(), &tr);
+    if (st != LAPH_OK) return die(st, "autotune");
+    std::printf("{\"autotune\": {\"deg\": %d, \"block\": %d, \"guard\": %d, \"ms_per_timeslice\": %.3f, "
+                "\"trials\": %d, \"from_cache\": %d}}\n",
+                tr.deg, tr.block, tr.guard, tr.ms_per_problem, tr.trials, tr.from_cache);
+  }
   laph_solver* s = nullptr;
   st = laph_solver_create(&s, probs.data(), nsolve, &o, device);
   if (st != LAPH_OK) return die(st, "solver");
   if (o.window == LAPH_WINDOW_MLP) {
-    std::vector<float> model;
-    if (!load_window_model(argv[0], &model)) {
-      std::fprintf(stderr, "laph_ev_ts: window = mlp but data/window_mlp.bin is missing or invalid\n");
-      return 1;
-    }
     st = laph_solver_set_window_model(s, model.data(), (int)model.size());
     if (st != LAPH_OK) return die(st, "window model");
   }

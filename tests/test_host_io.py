@@ -113,7 +113,7 @@ def test_parameters_parser_quirks(tmp_path):
     p = tmp_path / "parameters.txt"
     p.write_text("# comment\nconfig_path = /gauges\nLT = 48\nLX = 24\nNEV = 120\nalpha_1 = 0.62\n"
                  "alpha_2 = 0.52\niter = 3\nLAM_L = 11.8\nLAM_C = 0.6\nDEG = 8\nOMP_THRDS = 2\n"
-                 "alpha_1_i = 0.4\nalpha_1_f = 0.7\nalpha_2_i = 0.3\nalpha_2_f = 0.6\n"
+                 "alpha_1_i = 0.4\nalpha_1_f = 0.7\nalpha_2_i = 0.3\nalpha_2_f = 0.6\nautotune = 4\nfilter_deg = 56\n"
                  "LT=99\nsmear = stout\nDEG = 12")  # unterminated last line is dropped
     c = lb.parse_parameters(p)
     assert c["config_path"] == "/gauges" and c["LT"] == 48 and c["LX"] == 24 and c["NEV"] == 120
@@ -121,6 +121,7 @@ def test_parameters_parser_quirks(tmp_path):
     assert c["V3"] == 24 ** 3 and c["MAT_ENTRIES"] == 3 * 24 ** 3 and c["V_TS"] == 72 * 24 ** 3
     assert c["smear"] == lb.SMEAR_STOUT
     assert (c["alpha_1_i"], c["alpha_1_f"], c["alpha_2_i"], c["alpha_2_f"]) == (0.4, 0.7, 0.3, 0.6)
+    assert c["autotune"] == 4 and c["filter_deg"] == 56
     p.write_text("LT = 4\n\nLX = 4\n")
     with pytest.raises(lb.LaphError) as e:
         lb.parse_parameters(p)
