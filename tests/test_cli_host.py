@@ -116,8 +116,9 @@ def test_ev_ts_resume_detects_incomplete_outputs(tmp_path, damage):
 def test_ev_ts_without_device_fails_loudly(tmp_path):
     if _has_device():
         pytest.skip("a device is present")
-    for solver, stage in (("block", "solver"), ("plain", "context")):
-        _setup(tmp_path, solver=solver)
+    for solver, extra, stage in (("block", "", "solver"), ("plain", "", "context"),
+                                 ("block", "autotune = 2\n", "autotune")):
+        _setup(tmp_path, solver=solver, extra=extra)
         r = _run(EV_TS, ["--conf", "1227"], tmp_path)
         assert r.returncode == 1 and f"laph_ev_ts: {stage}:" in r.stderr, (solver, r.stderr)
         assert not any(p.name.startswith("eigen") for p in (tmp_path / "out").iterdir())
