@@ -207,6 +207,16 @@ int laph_solver_timings(laph_solver* s, double* ms4);
  * number of filter kernel launches, total device kernel launches. */
 int laph_solver_counters(laph_solver* s, long long* c3);
 
+/* Device memory a solver for probs[0..n) with opts allocates (bytes, each
+ * allocation rounded up to 2 MiB), without touching a device. */
+int laph_solver_footprint(const laph_problem* probs, int n, const laph_solve_opts* opts, long long* bytes);
+/* Largest m <= n such that a solver for probs[0..m) fits in `fraction` of the
+ * device's free memory now: the wave size for batches that do not fit at once
+ * (48^3 x 96 at nev 220 needs ~650 GB).  LAPH_ENOMEM (nmax = 0) if even one
+ * problem does not fit. */
+int laph_solver_max_batch(const laph_problem* probs, int n, const laph_solve_opts* opts, int device, double fraction,
+                          int* nmax);
+
 /* ---- autotuner ------------------------------------------------------------
  * Picks the filter degree cap (deg), the filter's columns per CTA (block) and
  * the guard vectors (hence the block width k) for a batch, by timing solves of

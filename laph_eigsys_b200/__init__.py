@@ -18,7 +18,8 @@ __all__ = ["Context", "Solver", "gauge_random", "lime_write_gauge", "lime_read_g
            "lime_info", "parse_parameters", "sourceshape", "sourceshape_avg", "write_sourceshape", "check_trace",
            "fix_phase", "reset_phase", "read_eigenvalues_ascii", "write_gauge_matrices", "read_gauge_matrices",
            "recover_spectrum", "write_eigsys_bin", "write_eigenvalues_bin", "read_eigsys_bin",
-           "read_eigenvalues_bin", "autotune", "autotune_search", "LaphError", "lib"]
+           "read_eigenvalues_bin", "autotune", "autotune_search", "solver_footprint",
+           "solver_max_batch", "LaphError", "lib"]
 
 
 def _ptr(a):
@@ -296,6 +297,30 @@ class Context:
 
 def _tune_dict(r):
     return {f: getattr(r, f) for f, _ in r._fields_}
+
+
+def _probs(problems):
+    probs = [(int(L), int(n)) for L, n in problems]
+    return (_lib.laph_problem * len(probs))(*[_lib.laph_problem(L, n) for L, n in probs]), len(probs)
+
+
+def solver_footprint(problems, opts=None, **kw):
+    """Device bytes laph_solver_create would allocate for these problems."""
+    arr, n = _probs(problems)
+    o = opts if opts is not None else solve_opts(**kw)
+    b = ctypes.c_longlong()
+    check(lib.laph_solver_footprint(arr, n, ctypes.byref(o), ctypes.byref(b)), "laph_solver_footprint")
+    return b.value
+
+
+def solver_max_batch(problems, opts=None, device=0, fraction=0.85, **kw):
+    """Largest leading count of problems whose solver fits in `fraction` of the device's free memory."""
+    arr, n = _probs(problems)
+    o = opts if opts is not None else solve_opts(**kw)
+    m = ctypes.c_int()
+    check(lib.laph_solver_max_batch(arr, n, ctypes.byref(o), device, fraction, ctypes.byref(m)),
+          "laph_solver_max_batch")
+    return m.value
 
 
 def autotune_search(deg_c, block_c, guard_c, start, trial):

@@ -107,6 +107,8 @@ _sig("laph_mlp_grad", c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_vo
 _sig("laph_mlp_train", c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, ctypes.c_float, c_void_p, c_int)
 _sig("laph_solver_timings", c_int, c_void_p, P(c_double))
 _sig("laph_solver_counters", c_int, c_void_p, P(c_ll))
+_sig("laph_solver_footprint", c_int, P(laph_problem), c_int, P(laph_solve_opts), P(c_ll))
+_sig("laph_solver_max_batch", c_int, P(laph_problem), c_int, P(laph_solve_opts), c_int, c_double, P(c_int))
 _sig("laph_autotune_search", c_int, P(c_int), c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_int, c_int, TUNE_TRIAL,
      c_void_p, P(laph_tune_result))
 _sig("laph_solver_autotune", c_int, P(laph_problem), c_int, P(c_void_p), c_int, c_int, P(laph_solve_opts), c_void_p,

@@ -739,4 +739,111 @@ int laph_solver_counters(laph_solver* s, long long* c3) {
   return LAPH_OK;
 }
 
+// Device bytes laph_solver_create allocates for probs[0..n): the same pool
+// arithmetic as create (keep the two in step), every allocation rounded up to
+// the 2 MiB the CUDA allocator hands out for large requests.  The CUDA graphs
+// a run captures come on top (small: kernel nodes only).
+int laph_solver_footprint(const laph_problem* probs, int n, const laph_solve_opts* opts, long long* bytes) {
+  if (!probs || n < 1 || !opts || !bytes) {
+    set_error("laph_solver_footprint: bad argument");
+    return LAPH_EINVAL;
+  }
+  const int kb = opts->block > 0 ? opts->block : 32;
+  long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
+  long long max_run = 0, max_v3 = 0;
+  for (int i = 0; i < n; ++i) {
+    const long long L = probs[i].L, V3 = L * L * L, dim = 3 * V3;
+    const int k = round_up(probs[i].nev + opts->guard, kGramTile);
+    if (L < 3 || L > 128 || probs[i].nev < 1 || k > 512 || k > dim / 2) {
+      set_error("laph_solver_footprint: problem %d is not solvable (see laph_solver_create)", i);
+      return LAPH_EINVAL;
+    }
+    const long long nchunk = (dim + 8191) / 8192, T = k / kGramTile, npair = T * (T + 1) / 2;
+    const long long mdeg = opts->deg > 0 ? opts->deg : 16;
+    o_u64 += 27 * V3;
+    o_uf += 27 * V3;
+    o_sc += V3;
+    o_blk += dim * k;
+    o_kk += 5LL * k * k;
+    o_kv += k;
+    o_gp += nchunk * 2 * npair * kGramTile * kGramTile;
+    o_rp += ((V3 + 127) / 128) * k;
+    o_tc += (mdeg + 1) * 3 * k;
+    max_v3 = std::max(max_v3, V3);
+  }
+  for (int i = 0; i < n;) {
+    int j = i;
+    while (j < n && probs[j].L == probs[i].L) ++j;
+    max_run = std::max(max_run, (long long)(j - i) * 27 * probs[i].L * probs[i].L * probs[i].L);
+    i = j;
+  }
+  const long long page = 2LL << 20;
+  long long total = 0;
+  auto add = [&](long long b) { total += (std::max(b, 1LL) + page - 1) / page * page; };
+  add(n * (long long)sizeof(ProbDesc));
+  add(n * (long long)sizeof(ProbState));
+  add(o_u64 * 16);
+  add(o_u64 * 16);
+  add(max_run * 16);
+  add(36 * max_v3 * 16);
+  add(max_run * 2 * 16);
+  add(o_sc * 4);
+  for (int b = 0; b < 3; ++b) add(o_blk * 16);  // V, W, Y
+  for (int b = 0; b < 4; ++b) add(o_blk * 8);   // S, E0..E2
+  add(o_kk * 16);
+  add(o_gp * 16);
+  add(o_rp * 8);
+  for (int b = 0; b < 4; ++b) add(o_kv * 8);  // theta, scol, resid, phases
+  add(o_kv * 8);                              // norms
+  add(o_tc * 8);
+  add(4 * o_kv * 8);                          // dwork
+  add(4);                                     // active count
+  add((long long)(kMlpParams + kMlpNorm) * 4);
+  add((long long)n * kMlpIn * 4);
+  add((long long)n * (kMlpIn + kMlpOut) * 4);
+  add((long long)n * 8);
+  add(4LL * n * 8);
+  add((long long)n * 4);
+  add((long long)n * kSmallPhases * 8);
+  add(o_uf * 8);                              // filter links (FP32, or BF16 + scale in the same pool)
+  for (int t = 0; t < 9; ++t) add((n + 1) * 4LL);  // CTA -> problem prefix tables
+  *bytes = total;
+  return LAPH_OK;
+}
+
+int laph_solver_max_batch(const laph_problem* probs, int n, const laph_solve_opts* opts, int device, double fraction,
+                          int* nmax) {
+  if (!probs || n < 1 || !opts || !nmax || !(fraction > 0.0 && fraction <= 1.0)) {
+    set_error("laph_solver_max_batch: bad argument");
+    return LAPH_EINVAL;
+  }
+  long long need = 0;
+  LAPH_TRY(laph_solver_footprint(probs, 1, opts, &need));  // validates the first problem before the device
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    set_error("laph_solver_max_batch: no CUDA device %d", device);
+    return LAPH_ENODEV;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(device));
+  size_t free_b = 0, total_b = 0;
+  LAPH_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  const double budget = fraction * (double)free_b;
+  // largest m with footprint(probs[0..m)) within the budget (the footprint grows with m)
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    LAPH_TRY(laph_solver_footprint(probs, mid, opts, &need));
+    if ((double)need <= budget) lo = mid;
+    else hi = mid - 1;
+  }
+  *nmax = lo;
+  if (lo == 0) {
+    laph_solver_footprint(probs, 1, opts, &need);
+    set_error("laph_solver_max_batch: one problem needs %lld bytes, %.0f of %zu free allowed", need, budget, free_b);
+    return LAPH_ENOMEM;
+  }
+  return LAPH_OK;
+}
+
 }  // extern "C"

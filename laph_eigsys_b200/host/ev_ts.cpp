@@ -6,8 +6,10 @@
 //   solver = plain (parameters.txt): the reference's loop body -- link map,
 //            smearing, MatShell with the GPU MatMult, EPS Krylov-Schur on
 //            T_DEG(B), fix_phase, recover_spectrum -- one timeslice at a time.
-//   solver = block (default): all timeslices of this process in one batched
-//            device solve (laph_solver), same outputs.
+//   solver = block (default): all timeslices of this process in batched
+//            device solves (laph_solver), in waves of as many timeslices as
+//            fit in the device's free memory (laph_solver_max_batch), same
+//            outputs.
 // Timeslices are split across processes as the reference splits them across
 // MPI ranks (src/ev_ts.cpp:103-119): with LAPH_RANK / LAPH_WORLD_SIZE (or
 // RANK / WORLD_SIZE) set, rank r gets a contiguous block, the first LT % size
@@ -253,33 +255,49 @@ int main(int argc, char** argv) {
                 "\"trials\": %d, \"from_cache\": %d}}\n",
                 tr.deg, tr.block, tr.guard, tr.ms_per_problem, tr.trials, tr.from_cache);
   }
+  // waves of as many timeslices as one solver fits in the device's free memory
+  // (all of them at 32^3 x 64; about 20 at a time at 48^3 x 96, nev 220)
+  int wave = nsolve;
+  st = laph_solver_max_batch(probs.data(), nsolve, &o, device, 0.85, &wave);
+  if (st != LAPH_OK) return die(st, "device memory");
+  if (wave < nsolve)
+    std::printf("{\"waves\": %d, \"timeslices_per_wave\": %d}\n", (nsolve + wave - 1) / wave, wave);
   laph_solver* s = nullptr;
-  st = laph_solver_create(&s, probs.data(), nsolve, &o, device);
-  if (st != LAPH_OK) return die(st, "solver");
-  if (o.window == LAPH_WINDOW_MLP) {
-    st = laph_solver_set_window_model(s, model.data(), (int)model.size());
-    if (st != LAPH_OK) return die(st, "window model");
-  }
-  for (int i = 0; i < nsolve; ++i) {
-    st = laph_solver_set_links(s, i, conf.data() + (size_t)todo[i] * V3 * 72, LAPH_LAYOUT_CONF, 0);
-    if (st != LAPH_OK) return die(st, "links");
-  }
-  std::vector<laph_result> res(nsolve);
-  st = laph_solver_run(s, res.data());
-  if (st != LAPH_OK && st != LAPH_ENOTCONV) return die(st, "solve");
-  double ms[4];
-  laph_solver_timings(s, ms);
-  for (int i = 0; i < nsolve; ++i) {
-    const int ts = todo[i];
-    st = laph_solver_get(s, i, evals.data(), vfix.data(), phases.data(), 0);
-    if (st != LAPH_OK) return die(st, "fetch");
-    st = laph_write_eigsys_bin(P.result_path, "eigenvectors", config, t0 + ts, dim, nev, vfix.data());
-    if (st != LAPH_OK) return die(st, "write eigenvectors");
-    laph_write_eigenvalues_bin(P.result_path, "eigenvalues", config, t0 + ts, nev, evals.data());
-    laph_write_eigenvalues_bin(P.result_path, "phases", config, t0 + ts, nev, phases.data());
-    std::printf("{\"t\": %d, \"solver\": \"block\", \"status\": %d, \"iters\": %d, \"max_resid\": %.3e, "
-                "\"trace_vdv\": %.12f, \"eval0\": %.12f, \"batch_ms\": %.2f}\n",
-                t0 + ts, res[i].status, res[i].iters, res[i].max_resid, res[i].trace_vdv, evals[0], ms[3]);
+  int s_np = 0;
+  std::vector<laph_result> res(wave);
+  for (int w0 = 0; w0 < nsolve; w0 += wave) {
+    const int wn = std::min(wave, nsolve - w0);
+    if (wn != s_np) {  // one solver for every full wave, a smaller one for the last
+      laph_solver_destroy(s);
+      s = nullptr;
+      st = laph_solver_create(&s, probs.data() + w0, wn, &o, device);
+      if (st != LAPH_OK) return die(st, "solver");
+      s_np = wn;
+      if (o.window == LAPH_WINDOW_MLP) {
+        st = laph_solver_set_window_model(s, model.data(), (int)model.size());
+        if (st != LAPH_OK) return die(st, "window model");
+      }
+    }
+    for (int i = 0; i < wn; ++i) {
+      st = laph_solver_set_links(s, i, conf.data() + (size_t)todo[w0 + i] * V3 * 72, LAPH_LAYOUT_CONF, 0);
+      if (st != LAPH_OK) return die(st, "links");
+    }
+    st = laph_solver_run(s, res.data());
+    if (st != LAPH_OK && st != LAPH_ENOTCONV) return die(st, "solve");
+    double ms[4];
+    laph_solver_timings(s, ms);
+    for (int i = 0; i < wn; ++i) {
+      const int ts = todo[w0 + i];
+      st = laph_solver_get(s, i, evals.data(), vfix.data(), phases.data(), 0);
+      if (st != LAPH_OK) return die(st, "fetch");
+      st = laph_write_eigsys_bin(P.result_path, "eigenvectors", config, t0 + ts, dim, nev, vfix.data());
+      if (st != LAPH_OK) return die(st, "write eigenvectors");
+      laph_write_eigenvalues_bin(P.result_path, "eigenvalues", config, t0 + ts, nev, evals.data());
+      laph_write_eigenvalues_bin(P.result_path, "phases", config, t0 + ts, nev, phases.data());
+      std::printf("{\"t\": %d, \"solver\": \"block\", \"status\": %d, \"iters\": %d, \"max_resid\": %.3e, "
+                  "\"trace_vdv\": %.12f, \"eval0\": %.12f, \"batch_ms\": %.2f}\n",
+                  t0 + ts, res[i].status, res[i].iters, res[i].max_resid, res[i].trace_vdv, evals[0], ms[3]);
+    }
   }
   laph_solver_destroy(s);
   return 0;

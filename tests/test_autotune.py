@@ -71,3 +71,29 @@ def test_argument_checks_and_no_device():
 
 def lib_call(f):
     return f()
+
+
+def test_solver_footprint_arithmetic():
+    """The footprint the wave planner uses: additive over equal problems up to the shared buffers, monotone, and
+    the 48^3 x 96, nev 220 batch (about 7 GB per timeslice) does not fit one 180 GB device."""
+    kw = dict(guard=16, deg=48)
+    one = lb.solver_footprint([(48, 220)], **kw)
+    assert 6.5e9 < one < 8e9
+    assert lb.solver_footprint([(48, 220)] * 96, **kw) > 180e9
+    sizes = [lb.solver_footprint([(32, 120)] * m, guard=16, deg=60) for m in (1, 2, 4, 8, 64)]
+    assert all(a < b for a, b in zip(sizes, sizes[1:]))
+    per = (sizes[3] - sizes[2]) / 4
+    assert abs((sizes[4] - sizes[3]) / 56 - per) <= 1e-3 * per  # linear in the number of equal problems
+    assert lb.solver_footprint([(8, 20), (16, 60)]) > lb.solver_footprint([(16, 60)])
+    for bad in ([(2, 1)], [(129, 10)], [(4, 90)]):
+        with pytest.raises(lb.LaphError) as e:
+            lb.solver_footprint(bad)
+        assert e.value.status == _lib.LAPH_EINVAL
+    import torch
+    if not torch.cuda.is_available():
+        with pytest.raises(lb.LaphError) as e:
+            lb.solver_max_batch([(32, 120)] * 4)
+        assert e.value.status == _lib.LAPH_ENODEV
+    with pytest.raises(lb.LaphError) as e:
+        lb.solver_max_batch([(32, 120)], fraction=0.0)
+    assert e.value.status == _lib.LAPH_EINVAL

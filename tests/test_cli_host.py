@@ -110,13 +110,13 @@ def test_ev_ts_resume_detects_incomplete_outputs(tmp_path, damage):
     r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path)
     skipped = [int(ln.split(":")[1].split(",")[0]) for ln in r.stdout.splitlines() if '"skipped"' in ln]
     assert skipped == [0, 2]
-    assert r.returncode == 1 and "laph_ev_ts: solver:" in r.stderr
+    assert r.returncode == 1 and "laph_ev_ts: device memory:" in r.stderr
 
 
 def test_ev_ts_without_device_fails_loudly(tmp_path):
     if _has_device():
         pytest.skip("a device is present")
-    for solver, extra, stage in (("block", "", "solver"), ("plain", "", "context"),
+    for solver, extra, stage in (("block", "", "device memory"), ("plain", "", "context"),
                                  ("block", "autotune = 2\n", "autotune")):
         _setup(tmp_path, solver=solver, extra=extra)
         r = _run(EV_TS, ["--conf", "1227"], tmp_path)

@@ -36,3 +36,21 @@ def test_autotune_picks_cached_settings_that_solve_correctly(gpu, orc, tmp_path)
         assert np.abs(-ev - w[:nev]).max() / w[-1] <= 1e-10
         assert np.abs(V.conj().T @ V - np.eye(nev)).max() <= 1e-10
     s.close()
+
+
+def test_footprint_matches_device_allocation(gpu):
+    """laph_solver_footprint against the free-memory drop of an actual laph_solver_create (two 32^3 timeslices,
+    about 2.7 GB): within the 2 MiB-per-allocation rounding it assumes; laph_solver_max_batch fits them."""
+    import torch
+    probs = [(32, 120)] * 2
+    kw = dict(guard=16, deg=60, link_prec=gpu.LINKS_FP32)
+    fp = gpu.solver_footprint(probs, **kw)
+    assert gpu.solver_max_batch(probs, **kw) == 2
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    s = gpu.Solver(probs, **kw)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    used = free0 - free1
+    s.close()
+    assert 0.85 * fp <= used <= 1.02 * fp + (64 << 20), (used, fp)
