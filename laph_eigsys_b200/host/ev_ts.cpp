@@ -30,6 +30,7 @@
 
 #include "../../include/laph_gpu.h"
 #include "../../include/laph_matshell.h"
+#include "cli_defaults.h"
 
 namespace {
 
@@ -87,12 +88,6 @@ bool outputs_complete(const char* dir, int config, int t, int dim, int nev) {
   double tr = 0.0, sum = 0.0;
   return laph_check_trace(dim, nev, V.data(), &tr, &sum) == 1;
 }
-
-// The block solver's filter degree cap when parameters.txt gives none: the
-// best degree measured for the production lattice sizes (24^3 and 32^3: 60;
-// 48^3: 48); small lattices keep the library default, which they converge
-// with in a few passes.  `autotune = N` measures it for the run's own batch.
-int default_filter_deg(int L, int library_default) { return L >= 40 ? 48 : (L >= 20 ? 60 : library_default); }
 
 double trace_vdv(int dim, int nev, const double* V) {
   double tr = 0.0, sum = 0.0;

@@ -142,7 +142,7 @@ def test_tune_hyp_argument_and_grid_errors(tmp_path):
     if not _has_device():
         (tmp_path / "parameters.txt").write_text((tmp_path / "parameters.txt").read_text() + "alpha_1_f = 0.5\n")
         r = _run(TUNE, ["--ts", "2", "--conf", "1227"], tmp_path)
-        assert r.returncode == 1 and "laph_tune_hyp: solver:" in r.stderr
+        assert r.returncode == 1 and "laph_tune_hyp: device memory:" in r.stderr
 
 
 SHAPE = os.path.join(ROOT, "laph_eigsys_b200", "laph_sourceshape")
