@@ -13,6 +13,7 @@
 #include <vector>
 #ifdef _OPENMP
 #include <errno.h>
+#include <sys/stat.h>
 #include <omp.h>
 #include <unistd.h>
 #endif
@@ -307,14 +308,15 @@ int lime_find_binary(FILE* f, const char* path, uint64_t* len, std::string* xml)
   return LAPH_ENORECORD;
 }
 
-// Timeslices [t_i, t_f] of an ILDG payload with es-byte big-endian reals at the
-// file position, into conf in the LAPH_LAYOUT_CONF order (FP32 widened).
+// Timeslices [t_i, t_f] of an ILDG payload of len bytes with es-byte big-endian
+// reals at the file position, into conf in the LAPH_LAYOUT_CONF order (FP32
+// widened).
 // The file order is t, z, y, x (x fastest), so every (t, z) plane is one
 // contiguous run of L^2 sites; the planes are independent units of work: each
 // OpenMP thread reads whole planes with pread (the FILE position is left as it
 // is) and byte-swaps them into their sites, so the read and the reorder both
 // run on every core and many reads are in flight for a cold file.
-int lime_read_payload(FILE* f, const char* path, int L, int t_i, int t_f, int es, double* conf) {
+int lime_read_payload(FILE* f, const char* path, uint64_t len, int L, int t_i, int t_f, int es, double* conf) {
   const long long V3 = (long long)L * L * L;
   const off_t base = ftello(f);
   if (base < 0) {
@@ -322,6 +324,13 @@ int lime_read_payload(FILE* f, const char* path, int L, int t_i, int t_f, int es
     return LAPH_EIO;
   }
   const int fd = fileno(f);
+  // the whole record must be present, as the reference (which reads all of it)
+  // requires, although only [t_i, t_f] is read
+  struct stat sb;
+  if (fstat(fd, &sb) != 0 || (uint64_t)sb.st_size < (uint64_t)base + len) {
+    set_error("LIME read error while reading file %s (binary record truncated)", path);
+    return LAPH_EIO;
+  }
   const size_t plane = (size_t)L * L * 72 * es;
   const off_t start = base + (off_t)((uint64_t)t_i * V3 * 72 * es);
   const long long nplanes = (long long)(t_f - t_i + 1) * L;
@@ -413,7 +422,7 @@ int laph_lime_read_gauge(const char* path, int T, int L, int t_i, int t_f, doubl
               (unsigned long long)len, path, (unsigned long long)want);
     return LAPH_ESIZE;
   }
-  st = lime_read_payload(f, path, L, t_i, t_f, 8, conf);
+  st = lime_read_payload(f, path, len, L, t_i, t_f, 8, conf);
   std::fclose(f);
   return st;
 }
@@ -448,7 +457,7 @@ int laph_lime_read_gauge_any(const char* path, int T, int L, int t_i, int t_f, d
                 8 * es);
     return LAPH_ESIZE;
   }
-  st = lime_read_payload(f, path, L, t_i, t_f, es, conf);
+  st = lime_read_payload(f, path, len, L, t_i, t_f, es, conf);
   std::fclose(f);
   if (st == LAPH_OK && precision) *precision = 8 * es;
   return st;

@@ -252,3 +252,62 @@ def test_gauge_matrices_file_is_raw_eigen_matrix3cd(tmp_path):
     with pytest.raises(lb.LaphError) as e:
         lb.read_gauge_matrices(tmp_path / "missing", 27)
     assert e.value.status == _lib.LAPH_EIO
+
+
+_STATUS_OF_REF = {0: _lib.LAPH_OK, 500: _lib.LAPH_EIO, 501: _lib.LAPH_ESIZE, 502: _lib.LAPH_ESINGLE,
+                  -2: _lib.LAPH_ENORECORD}
+
+
+def test_lime_reader_fuzz_matches_reference_restatement(tmp_path, orc):
+    """Mutated LIME files (truncations, corrupted header bytes, wrong lengths, extra records before or after the
+    binary one, a second binary record): laph_lime_read_gauge ends with the status the reference's reader ends
+    with (read_lime_gauge_field_doubleprec_timeslices, restated by the oracle: exit codes 500/501/502/-2) and, when
+    both succeed, with the same links, for random timeslice ranges."""
+    L, T = 3, 3
+    conf = lb.gauge_random(L, T, 0.4, 99)
+    good = tmp_path / "good"
+    lb.lime_write_gauge(good, conf, L, T)
+    base = good.read_bytes()
+    i_bin = base.index(b"ildg-binary-data") - 16
+    n_pay = L ** 3 * T * 72 * 8
+    rng = np.random.default_rng(7)
+    p = tmp_path / "mutant"
+    seen = set()
+    for case in range(400):
+        kind = int(rng.integers(0, 7))
+        b = bytearray(base)
+        if kind == 0:    # truncated anywhere
+            b = b[:int(rng.integers(0, len(b)))]
+        elif kind == 1:  # one byte of a record header changed
+            hdr = int(rng.choice([0, i_bin]))
+            k = int(rng.integers(0, 40))
+            b[hdr + k] ^= int(rng.integers(1, 256))
+        elif kind == 2:  # binary record length off by a little, halved or doubled
+            n = int(rng.choice([n_pay - 8, n_pay + 8, n_pay // 2, 2 * n_pay, n_pay - 1]))
+            b[i_bin + 8:i_bin + 16] = n.to_bytes(8, "big")
+        elif kind == 3:  # an extra record of another type first
+            b = bytearray(_lime_record("xlf-info", bytes(rng.integers(0, 256, int(rng.integers(0, 40)), dtype=np.uint8)),
+                                       me=False)) + b
+        elif kind == 4:  # junk after the last record
+            b = b + bytes(rng.integers(0, 256, int(rng.integers(1, 300)), dtype=np.uint8))
+        elif kind == 5:  # a second, different binary record after the first: the first one counts
+            other = bytes(rng.integers(0, 256, n_pay, dtype=np.uint8))
+            b = b + bytearray(_lime_record("ildg-binary-data", other, mb=False))
+        else:            # a binary record of the right size but only part of its payload present
+            b = b[:i_bin + 144 + int(rng.integers(0, n_pay))]
+        p.write_bytes(bytes(b))
+        t0 = int(rng.integers(0, T))
+        t1 = int(rng.integers(t0, T))
+        st_ref, ref = orc.lime_read_gauge(p, T, L, t0, t1)
+        want = _STATUS_OF_REF[st_ref]
+        try:
+            got = lb.lime_read_gauge(p, T, L, t0, t1)
+            st = _lib.LAPH_OK
+        except lb.LaphError as e:
+            st = e.status
+        assert st == want, (case, kind, st, st_ref)
+        if st == _lib.LAPH_OK:
+            assert np.array_equal(got, ref), (case, kind)
+        seen.add((kind, st))
+    assert {s for _, s in seen} >= {_lib.LAPH_OK, _lib.LAPH_EIO, _lib.LAPH_ESIZE, _lib.LAPH_ESINGLE,
+                                    _lib.LAPH_ENORECORD}
