@@ -38,7 +38,8 @@ enum {
   LAPH_ENOTCONV = 8,   /* eigensolver stopped at max_it before nev pairs converged */
   LAPH_ETIMEOUT = 9,   /* a bounded device wait gave up */
   LAPH_ETRACE = 10,    /* tr(V^dag V) / sum(V^dag V) check failed (reference check_trace) */
-  LAPH_EPARSE = 11,    /* parameters.txt line the reference parser cannot read */
+  LAPH_EPARSE = 11,    /* parameters.txt line the reference parser cannot read, or an
+                          ildg-format record without its lattice and precision */
   LAPH_ENODEV = 12     /* no CUDA device */
 };
 const char* laph_strerror(int status);

@@ -140,7 +140,7 @@ const char* laph_strerror(int s) {
     case LAPH_ENOTCONV: return "eigensolver did not converge";
     case LAPH_ETIMEOUT: return "device wait timed out";
     case LAPH_ETRACE: return "tr(V^dag V) check failed";
-    case LAPH_EPARSE: return "parameter file parse error";
+    case LAPH_EPARSE: return "parse error (parameters.txt or ildg-format record)";
     case LAPH_ENODEV: return "no CUDA device";
     default: return "unknown status";
   }

@@ -311,3 +311,38 @@ def test_lime_reader_fuzz_matches_reference_restatement(tmp_path, orc):
         seen.add((kind, st))
     assert {s for _, s in seen} >= {_lib.LAPH_OK, _lib.LAPH_EIO, _lib.LAPH_ESIZE, _lib.LAPH_ESINGLE,
                                     _lib.LAPH_ENORECORD}
+
+
+def test_ildg_format_record_fuzz_never_crashes(tmp_path):
+    """Random and truncated ildg-format payloads in front of a valid FP64 record: lime_info and the any-precision
+    reader return a status (never crash or hang); wherever the XML declares nothing contradicting the data, the
+    links come back exactly."""
+    L, T = 3, 2
+    conf = lb.gauge_random(L, T, 0.4, 5)
+    n64 = L ** 3 * T * 72 * 8
+    payload = bytearray(n64)
+    good = tmp_path / "g"
+    lb.lime_write_gauge(good, conf, L, T)
+    raw = good.read_bytes()
+    data = raw[raw.index(b"ildg-binary-data") - 16:]
+    rng = np.random.default_rng(11)
+    tags = [b"<precision>", b"</precision>", b"<lx>", b"<lt>", b"64", b"32", b"3", b"2", b"<", b">", b"\0", b"x"]
+    p = tmp_path / "f"
+    ok = 0
+    for case in range(300):
+        xml = b"".join(rng.choice(tags, size=int(rng.integers(0, 30))))
+        if rng.random() < 0.3:
+            xml = bytes(rng.integers(0, 256, int(rng.integers(0, 200)), dtype=np.uint8))
+        p.write_bytes(_lime_record("ildg-format", xml, me=False) + data)
+        try:
+            lb.lime_info(p)
+        except lb.LaphError as e:
+            assert e.status in (_lib.LAPH_ESIZE, _lib.LAPH_ENORECORD, _lib.LAPH_EIO, _lib.LAPH_EPARSE)
+        try:
+            got, prec = lb.lime_read_gauge_any(p, T, L, 0, T - 1)
+        except lb.LaphError as e:
+            assert e.status == _lib.LAPH_ESIZE  # the XML declared 32-bit reals over FP64 data
+            continue
+        assert prec == 64 and np.array_equal(got, conf)
+        ok += 1
+    assert ok > 100
