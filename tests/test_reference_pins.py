@@ -163,3 +163,49 @@ def test_parser_fuzz_against_reference(tmp_path):
         for k, rk in zip(KEYS_PATH, ["conf", "res", "in_path", "phase_path"]):
             assert c[k] == r[rk], (k, text)
     assert 0 < threw < 300
+
+
+@pytest.mark.parametrize("L", [4, 6])
+def test_oracle_sourceshape_walks_reference_lookup_tables(tmp_path, orc, L):
+    """source_shape_complete reaches x + r by r_i steps of Nav::get_up in x, then y, then z
+    (get_vectorial_dst_ind, modules/sourceshape_funcs.cpp:9-24): psi(r) built here from the reference's own tables
+    equals the oracle's (and with it the device kernel's, pinned to the oracle elsewhere)."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    up = np.array(ref("nav", p)["up"])
+    V3, nev = L ** 3, 5
+    rng = np.random.default_rng(L)
+    V, _ = np.linalg.qr(rng.normal(size=(3 * V3, nev)) + 1j * rng.normal(size=(3 * V3, nev)))
+    blocks = V.reshape(V3, 3, nev)
+    psi = []
+    for r1 in range(0, L, 2):
+        for r2 in range(0, L, 2):
+            for r3 in range(0, L, 2):
+                dst = np.arange(V3)
+                for d, r in enumerate((r1, r2, r3)):
+                    for _ in range(r):
+                        dst = up[dst, d]
+                M = np.einsum("xan,xbn->xab", blocks[dst], blocks.conj())
+                psi.append(np.sqrt((np.abs(M) ** 2).sum(axis=(1, 2))).sum())
+    ref_psi = np.array(psi)
+    assert np.abs(orc.sourceshape(V, L) - ref_psi).max() <= 1e-12 * ref_psi.max()
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_oracle_displacement_uses_reference_lookup_tables(tmp_path, orc, L):
+    """right_displacement_one_dir (modules/config_utils.cpp:344-382) with the reference's iup / idown tables:
+    W(x) = (U_dir(x) V(iup[x][dir]) - U_dir(idown[x][dir])^dag V(idown[x][dir])) / 2, against the oracle."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    V3, nev = L ** 3, 3
+    U = lb.gauge_random(L, 1, 0.5, 17)[0, :, 1:4]  # (V3, 3, 3, 3): [site][dir][a][b]
+    rng = np.random.default_rng(3)
+    V = rng.normal(size=(3 * V3, nev)) + 1j * rng.normal(size=(3 * V3, nev))
+    blocks = V.reshape(V3, 3, nev)
+    for d in range(3):
+        fw = np.einsum("xab,xbn->xan", U[:, d], blocks[up[:, d]])
+        bw = np.einsum("xba,xbn->xan", U[dn[:, d], d].conj(), blocks[dn[:, d]])
+        W = (0.5 * (fw - bw)).reshape(3 * V3, nev)
+        assert np.abs(orc.displace(U, L, d, V) - W).max() <= 1e-14 * np.abs(W).max()
