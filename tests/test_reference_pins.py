@@ -209,3 +209,36 @@ def test_oracle_displacement_uses_reference_lookup_tables(tmp_path, orc, L):
         bw = np.einsum("xba,xbn->xan", U[dn[:, d], d].conj(), blocks[dn[:, d]])
         W = (0.5 * (fw - bw)).reshape(3 * V3, nev)
         assert np.abs(orc.displace(U, L, d, V) - W).max() <= 1e-14 * np.abs(W).max()
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_oracle_matvec_uses_reference_lookup_tables(tmp_path, orc, L):
+    """tv2 (modules/shell_matop.cpp:16-103) with the reference's get_up / get_dn on random links:
+    B x = c (sum_mu U_mu(k) x(up) + U_mu(dn)^dag x(dn) - 6 x(k)) + a x(k), c = 2 / (LAM_L - LAM_C),
+    a = 1 + c LAM_C; tv_iter's T_deg(B) x by the three-term recurrence, against the oracle for deg 2, 3, 5."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    V3 = L ** 3
+    U = lb.gauge_random(L, 1, 0.5, 23)[0, :, 1:4]
+    lam_l, lam_c = 11.8, 0.6
+    c = 2.0 / (lam_l - lam_c)
+    a = 1.0 + c * lam_c
+
+    def B(v):
+        x = v.reshape(V3, 3)
+        hop = np.zeros_like(x)
+        for mu in range(3):
+            hop += np.einsum("kab,kb->ka", U[:, mu], x[up[:, mu]])
+            hop += np.einsum("kba,kb->ka", U[dn[:, mu], mu].conj(), x[dn[:, mu]])
+        return (c * (hop - 6.0 * x) + a * x).ravel()
+
+    rng = np.random.default_rng(L)
+    x = rng.normal(size=3 * V3) + 1j * rng.normal(size=3 * V3)
+    t_prev, t_cur = x, B(x)
+    for deg in range(2, 6):
+        t_prev, t_cur = t_cur, 2.0 * B(t_cur) - t_prev
+        if deg in (2, 3, 5):
+            got = orc.tv_iter(U, L, lam_l, lam_c, deg, x)
+            assert np.abs(got - t_cur).max() <= 1e-13 * np.abs(t_cur).max(), deg
