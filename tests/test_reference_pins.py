@@ -242,3 +242,126 @@ def test_oracle_matvec_uses_reference_lookup_tables(tmp_path, orc, L):
         if deg in (2, 3, 5):
             got = orc.tv_iter(U, L, lam_l, lam_c, deg, x)
             assert np.abs(got - t_cur).max() <= 1e-13 * np.abs(t_cur).max(), deg
+
+
+def _proj_su3_imp(M):
+    """proj_to_su3_imp (modules/timeslice.cpp:90-104): M ((M^dag M)^{1/2})^{-1}, then times det^{-1/3} with the
+    principal complex cube root, for a stack of 3x3 matrices."""
+    H = np.conj(np.swapaxes(M, -1, -2)) @ M
+    w, Q = np.linalg.eigh(H)
+    inv_sqrt = (Q * (1.0 / np.sqrt(w))[..., None, :]) @ np.conj(np.swapaxes(Q, -1, -2))
+    W = M @ inv_sqrt
+    return W * (1.0 / np.power(np.linalg.det(W).astype(complex), 1.0 / 3.0))[..., None, None]
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_oracle_ape_uses_reference_lookup_tables(tmp_path, orc, L):
+    """Tslice::smearing_ape (modules/timeslice.cpp:196-239) with the reference's get_up / get_dn, including its
+    backward staple U[mu][nd]^dag U[mu][d] U[nu][d] (the quirk: U[nu][d] where U[nu][nd] is meant), two iterations,
+    against the oracle in compat mode."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    U = lb.gauge_random(L, 1, 0.4, 31)[0, :, 1:4].copy()
+    alpha, iters = 0.5, 2
+    dag = lambda m: np.conj(np.swapaxes(m, -1, -2))  # noqa: E731
+    Us = U.copy()
+    for _ in range(iters):
+        new = np.empty_like(Us)
+        for d in range(3):
+            staple = np.zeros_like(Us[:, d])
+            for nd in range(3):
+                if nd == d:
+                    continue
+                mu = up[:, nd]
+                nu = up[mu, d]
+                eta = dn[nu, nd]
+                staple += Us[:, nd] @ (Us[mu, d] @ dag(Us[eta, nd]))
+                mu = dn[:, nd]
+                nu = up[mu, d]
+                staple += dag(Us[mu, nd]) @ (Us[mu, d] @ Us[nu, d])
+            new[:, d] = Us[:, d] * (1.0 - alpha) + staple * (alpha / 4.0)
+        Us = _proj_su3_imp(new)
+    got = orc.smear_ape(U, L, alpha, iters, 1)
+    assert np.abs(got - Us).max() <= 1e-12
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_oracle_stout_uses_reference_lookup_tables(tmp_path, orc, L):
+    """Tslice::smearing_stout (modules/timeslice.cpp:145-193) with the reference's get_up / get_dn and its
+    backward-staple quirk: Omega = (rho / 4) C U^dag, q = (Omega^dag - Omega) / 2 - tr(Omega^dag - Omega) / 6,
+    U' = exp(-q) U, two iterations, against the oracle in compat mode."""
+    from scipy.linalg import expm
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    U = lb.gauge_random(L, 1, 0.4, 37)[0, :, 1:4].copy()
+    rho, iters = 0.1, 2
+    dag = lambda m: np.conj(np.swapaxes(m, -1, -2))  # noqa: E731
+    Us = U.copy()
+    for _ in range(iters):
+        new = np.empty_like(Us)
+        for d in range(3):
+            staple = np.zeros_like(Us[:, d])
+            for nd in range(3):
+                if nd == d:
+                    continue
+                mu = up[:, nd]
+                nu = up[mu, d]
+                eta = dn[nu, nd]
+                staple += Us[:, nd] @ (Us[mu, d] @ dag(Us[eta, nd]))
+                mu = dn[:, nd]
+                nu = up[mu, d]
+                staple += dag(Us[mu, nd]) @ (Us[mu, d] @ Us[nu, d])
+            omega = (staple * (rho / 4.0)) @ dag(Us[:, d])
+            A = dag(omega) - omega
+            q = A * 0.5 - np.trace(A, axis1=1, axis2=2)[:, None, None] * np.eye(3) / 6.0
+            new[:, d] = np.stack([expm(-qq) for qq in q]) @ Us[:, d]
+        Us = new
+    got = orc.smear_stout(U, L, rho, iters, 1)
+    assert np.abs(got - Us).max() <= 1e-12
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_oracle_hyp_uses_reference_lookup_tables(tmp_path, orc, L):
+    """Tslice::smearing_hyp (modules/timeslice.cpp:243-369, get_dirs :106-122, decor :125-140) with the
+    reference's get_up / get_dn: level 1 decorated links in slots dir / dir + 3 (perpendicular directions in
+    get_dirs order), level 2 with plane = ((dir + 1) ^ (not_dir + 1)) - 1 and the decor storage map, two
+    iterations, against the oracle."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    U = lb.gauge_random(L, 1, 0.4, 41)[0, :, 1:4].copy()
+    a1, a2, iters = 0.62, 0.52, 2
+    dag = lambda m: np.conj(np.swapaxes(m, -1, -2))  # noqa: E731
+    dirs = {0: (1, 2), 1: (0, 2), 2: (0, 1)}
+    decor = {(0, 1): 0, (0, 2): 3, (1, 0): 1, (1, 2): 4, (2, 0): 2, (2, 1): 5}
+    Us = U.copy()
+    for _ in range(iters):
+        dec = np.empty((Us.shape[0], 6, 3, 3), dtype=np.complex128)
+        for d in range(3):
+            for n_el, pd in enumerate(dirs[d]):
+                inner = Us[:, pd] @ (Us[up[:, pd], d] @ dag(Us[up[:, d], pd]))
+                m = dn[:, pd]
+                inner = inner + dag(Us[m, pd]) @ (Us[m, d] @ Us[up[m, d], pd])
+                dec[:, d + 3 * n_el] = _proj_su3_imp(Us[:, d] * (1 - a2) + inner * (a2 / 2.0))
+        new = np.empty_like(Us)
+        for d in range(3):
+            outer = np.zeros_like(Us[:, d])
+            for nd in range(3):
+                if nd == d:
+                    continue
+                plane = ((d + 1) ^ (nd + 1)) - 1
+                a, b = decor[(nd, plane)], decor[(d, plane)]
+                mu = up[:, nd]
+                eta = dn[up[mu, d], nd]
+                outer += dec[:, a] @ (dec[mu, b] @ dag(dec[eta, a]))
+                mu = dn[:, nd]
+                outer += dag(dec[mu, a]) @ (dec[mu, b] @ dec[up[mu, d], a])
+            new[:, d] = Us[:, d] * (1.0 - a1) + outer * (a1 / 4.0)
+        Us = _proj_su3_imp(new)
+    got = orc.smear_hyp(U, L, a1, a2, iters)
+    assert np.abs(got - Us).max() <= 1e-12
