@@ -346,3 +346,20 @@ def test_ildg_format_record_fuzz_never_crashes(tmp_path):
         assert prec == 64 and np.array_equal(got, conf)
         ok += 1
     assert ok > 100
+
+
+def test_lime_reorder_transcribes_reference_loop(tmp_path, orc):
+    """read_lime_gauge_field_doubleprec_timeslices' copy loop (modules/io.cpp:84-131), transcribed: file order
+    t, z, y, x with 72 big-endian doubles per site in ILDG mu order x, y, z, t; config position
+    ((t - t_i) LX LY LZ + x LY LZ + y LZ + z) 72, U_x..U_z to slots 1..3 and U_t to slot 0, each 3x3 row-major
+    complex.  Random (not SU(3)) payload, so every number's place is checked."""
+    L, T, ti, tf = 3, 4, 1, 2
+    rng = np.random.default_rng(5)
+    vals = rng.normal(size=L ** 3 * T * 72)
+    p = tmp_path / "conf"
+    p.write_bytes(_lime_record("ildg-binary-data", vals.astype(">f8").tobytes()))
+    filec = (vals[0::2] + 1j * vals[1::2]).reshape(T, L, L, L, 4, 3, 3)  # [t][z][y][x][mu_file][i][j]
+    want = np.transpose(filec, (0, 3, 2, 1, 4, 5, 6)).reshape(T, L ** 3, 4, 3, 3)[:, :, [3, 0, 1, 2]][ti:tf + 1]
+    assert np.array_equal(lb.lime_read_gauge(p, T, L, ti, tf), want)
+    st, ref = orc.lime_read_gauge(p, T, L, ti, tf)
+    assert st == 0 and np.array_equal(ref, want)
