@@ -154,3 +154,31 @@ def test_mlp_forward_rejects_bad_arguments():
     p = ctypes.c_void_p(x.ctypes.data)
     assert lib.laph_mlp_forward(None, p, 1, p, 0) == _lib.LAPH_EINVAL
     assert lib.laph_mlp_forward(p, p, 0, p, 0) == _lib.LAPH_EINVAL
+
+
+def test_last_error_is_per_thread():
+    """Each thread reads back the message of its own failing call, however the calls interleave."""
+    import threading
+    import time
+    errors = {}
+
+    def worker(k):
+        for it in range(200):
+            if k % 2:
+                st = lib.laph_timeslice_split(-k, 1, 0, None, None)
+                want = "laph_timeslice_split"
+            else:
+                st = lib.laph_reset_phase_host(0, 1, None, None, None)
+                want = "laph_reset_phase_host"
+            time.sleep(0)
+            msg = lib.laph_last_error().decode()
+            if st != _lib.LAPH_EINVAL or not msg.startswith(want):
+                errors[k] = (it, st, msg)
+                return
+
+    ts = [threading.Thread(target=worker, args=(k,)) for k in range(8)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errors, errors
