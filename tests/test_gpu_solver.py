@@ -167,3 +167,29 @@ def test_max_it_reached_reports_not_converged(gpu):
     st, res = s.run()
     assert st == 0 and all(r["status"] == 0 for r in res)
     s.close()
+
+
+@pytest.mark.parametrize("nev", [21, 12])
+def test_block_solver_unit_field_degenerate_spectrum(gpu, orc, nev):
+    """The reference's own test input, the unit gauge field: -Delta has the free spectrum sum_i 4 sin^2(pi n_i / L)
+    with 3 colours x momentum multiplicities (6^3: 0 x3, 1 x18, 2 x36, ...).  nev = 21 ends on a cluster boundary,
+    nev = 12 cuts the 18-fold cluster; eigenvalues to 1e-10 of lambda_max either way, the 3 zero modes span the
+    constant colour vectors, and HYP smearing leaves the field unit."""
+    from conftest import unit_links
+    L = 6
+    U = unit_links(L)
+    w = orc.free_spectrum(L)
+    s = gpu.Solver([(L, nev)], guard=16, tol=1e-10, deg=16, max_it=400, smear_kind=gpu.SMEAR_HYP, smear_p1=0.62,
+                   smear_p2=0.52, smear_iters=2, link_prec=gpu.LINKS_FP32, window=gpu.WINDOW_LANCZOS)
+    s.set_links(0, U)
+    st, res = s.run()
+    assert st == 0 and res[0]["max_resid"] <= 1e-10
+    ev, V, _ = s.get(0)
+    assert np.abs(-ev - w[:nev]).max() / 12.0 <= 1e-10
+    assert np.abs(V.conj().T @ V - np.eye(nev)).max() <= 1e-10
+    P0 = V[:, :3] @ V[:, :3].conj().T
+    C = np.zeros((3 * L ** 3, 3))
+    for c in range(3):
+        C[c::3, c] = 1.0 / np.sqrt(L ** 3)
+    assert np.abs(P0 - C @ C.T).max() <= 1e-8
+    s.close()
