@@ -58,3 +58,16 @@ def test_lime_io_measurement_small():
     assert out["matches_written"] and out["oracle_matches"]
     assert out["bytes"] == 4 ** 3 * 3 * 72 * 8 and out["cold_gbs"] > 0 and out["warm_gbs"] > 0
     assert not [p for p in os.listdir(ROOT) if p.startswith("_lime_")]
+
+
+def test_reference_arm_per_core_layout():
+    """The reference's MPI layout (one single-threaded timeslice per core): same line, per-core throughput."""
+    r = subprocess.run([sys.executable] + ARGS + ["--cpu-layout", "per-core"], cwd=ROOT, capture_output=True,
+                       text=True, timeout=900, env=_env())
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1
+    ln = lines[0]
+    cb = ln["cpu_baseline"]
+    assert ln["impl"] == "reference" and ln["value"] > 0 and cb["layout"] == "one timeslice per core"
+    assert cb["cores"] == (os.cpu_count() or 1) and abs(ln["ms_per_step"] * ln["value"] / 1000.0 - cb["cores"]) < 1e-6 * cb["cores"]
