@@ -17,13 +17,11 @@ c_vp, c_int = ctypes.c_void_p, ctypes.c_int
 CB = ctypes.CFUNCTYPE(c_int, c_vp, c_vp, c_vp)
 
 
-def test_shim_eps_solves_matshell_like_slepc(orc):
+def _shim_solve(orc, U, L, nev, deg, lam_l, lam_c, tol):
+    """MatShell (MATOP_MULT = the oracle's tv_iter) + the shim's EPSSolve, as ev_ts drives SLEPc; returns the
+    converged count, the Rayleigh quotients on -Delta and the residual norms of the first nev eigenvectors."""
     shim = ctypes.CDLL(SHIM)
-    L, nev, deg, lam_l = 4, 12, 8, 12.0
-    U = orc.smear_hyp(random_links(L, 0.4, 99), L, 0.62, 0.52, 1)
     A = orc.neglap_dense(U, L)
-    w = np.linalg.eigvalsh(A)
-    lam_c = 0.5 * (w[nev + 2] + w[nev + 3])
     dim = 3 * L ** 3
     calls = [0]
 
@@ -50,19 +48,49 @@ def test_shim_eps_solves_matshell_like_slepc(orc):
     assert shim.EPSSetDimensions(eps, nev, PETSC_DECIDE, PETSC_DECIDE) == 0
     assert shim.EPSSetWhichEigenpairs(eps, EPS_LARGEST_MAGNITUDE) == 0
     shim.EPSSetTolerances.argtypes = [c_vp, ctypes.c_double, c_int]
-    assert shim.EPSSetTolerances(eps, 1e-12, -2) == 0
+    assert shim.EPSSetTolerances(eps, tol, -2) == 0
     assert shim.EPSSolve(eps) == 0
     nconv = c_int()
     shim.EPSGetConverged(eps, ctypes.byref(nconv))
-    assert nconv.value >= nev and calls[0] > 0
+    assert calls[0] > 0
     eig = (ctypes.c_double * 2)()
-    rq = []
+    rq, res = [], []
     for i in range(nev):
         assert shim.EPSGetEigenpair(eps, i, eig, None, xr, xi) == 0
         p = c_vp()
         shim.VecGetArray(xr, ctypes.byref(p))
         v = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), (2 * dim,)).view(np.complex128).copy()
-        rq.append(np.vdot(v, A @ v).real)
-    assert np.abs(np.sort(rq) - w[:nev]).max() / w[-1] < 1e-11
+        lam = np.vdot(v, A @ v).real / np.vdot(v, v).real
+        rq.append(lam)
+        res.append(np.linalg.norm(A @ v - lam * v) / np.linalg.norm(v))
     shim.EPSDestroy(ctypes.byref(eps))
     shim.MatDestroy(ctypes.byref(Am))
+    return nconv.value, np.array(rq), np.array(res)
+
+
+def test_shim_eps_solves_matshell_like_slepc(orc):
+    L, nev, deg, lam_l = 4, 12, 8, 12.0
+    U = orc.smear_hyp(random_links(L, 0.4, 99), L, 0.62, 0.52, 1)
+    w = np.linalg.eigvalsh(orc.neglap_dense(U, L))
+    lam_c = 0.5 * (w[nev + 2] + w[nev + 3])
+    nconv, rq, _ = _shim_solve(orc, U, L, nev, deg, lam_l, lam_c, 1e-12)
+    assert nconv >= nev
+    assert np.abs(np.sort(rq) - w[:nev]).max() / w[-1] < 1e-11
+
+
+def test_shim_eps_on_unit_field_finds_eigenpairs_not_multiplicities(orc):
+    """The reference's own test input, the unit field, has an exactly degenerate spectrum (4^3: 0 x3, 2 x18, ...).
+    Krylov-Schur from one start vector -- SLEPc's method, restated by the plain form -- returns true eigenpairs
+    of -Delta but not the full multiplicities: the 3 zero modes come out at nev = 3, while at nev = 12 the
+    returned set reaches above the 18-fold lambda = 2 cluster.  The block solver's k-column random start has no
+    such limit (tests/test_gpu_solver.py, unit field)."""
+    L, lam_l, deg = 4, 12.0, 8
+    U = np.zeros((L ** 3, 3, 3, 3), dtype=np.complex128)
+    U[:, :] = np.eye(3)
+    w = orc.free_spectrum(L)
+    nconv, rq, res = _shim_solve(orc, U, L, 3, deg, lam_l, 1.0, 1e-12)
+    assert nconv >= 3 and np.abs(rq).max() < 1e-10
+    nconv, rq, res = _shim_solve(orc, U, L, 12, deg, lam_l, 2.3, 1e-12)
+    assert nconv >= 12 and res.max() < 1e-8                       # every returned pair is an eigenpair
+    assert np.abs(rq[:, None] - np.unique(np.round(w, 9))[None, :]).min(axis=1).max() < 1e-8
+    assert np.sort(rq)[-1] > w[11] + 1.0                            # but not the 12 lowest, counted with multiplicity
