@@ -143,6 +143,7 @@ int laph_set_links(laph_ctx* c, const double* links, int layout) {
     return LAPH_EINVAL;
   }
   const int V3 = c->g.V3;
+  LAPH_TRY(check_links_finite(links, layout, V3, "laph_set_links"));
   std::vector<double2> soa(27 * (size_t)V3);
   LAPH_TRY(links_to_soa(links, layout, V3, soa.data()));
   LAPH_CUDA_TRY(cudaMemcpyAsync(c->U, soa.data(), sizeof(double2) * soa.size(), cudaMemcpyHostToDevice, c->st));

@@ -1,4 +1,6 @@
 // links.cu -- boundary link layouts and plaquette reductions.
+#include <cmath>
+
 #include "links.cuh"
 #include "su3.cuh"
 
@@ -19,6 +21,28 @@ int links_to_soa(const double* in, int layout, int V3, double2* soa) {
           }
           soa[(size_t)(d * 9 + 3 * a + b) * V3 + s] = make_double2(p[0], p[1]);
         }
+  return LAPH_OK;
+}
+
+int check_links_finite(const double* in, int layout, int V3, const char* who) {
+  if (layout != LAPH_LAYOUT_ROWMAJOR && layout != LAPH_LAYOUT_EIGEN && layout != LAPH_LAYOUT_CONF) {
+    set_error("%s: unknown link layout %d", who, layout);
+    return LAPH_EINVAL;
+  }
+  // per site: 54 contiguous doubles (ROWMAJOR, EIGEN), or slots 1..3 of 72 (CONF)
+  const size_t stride = layout == LAPH_LAYOUT_CONF ? 72 : 54, first = layout == LAPH_LAYOUT_CONF ? 18 : 0;
+  long long bad = V3;
+#pragma omp parallel for reduction(min : bad) schedule(static)
+  for (long long s = 0; s < V3; ++s) {
+    const double* p = in + (size_t)s * stride + first;
+    bool ok = true;
+    for (int e = 0; e < 54; ++e) ok &= std::isfinite(p[e]);
+    if (!ok && s < bad) bad = s;
+  }
+  if (bad < V3) {
+    set_error("%s: non-finite link value at site %lld", who, bad);
+    return LAPH_EINVAL;
+  }
   return LAPH_OK;
 }
 

@@ -8,6 +8,11 @@ namespace laph {
 // soa[(dir*9 + 3a + b)*V3 + site] (complex128).
 int links_to_soa(const double* links, int layout, int V3, double2* soa);
 int soa_to_links(const double2* soa, int V3, int layout, double* links);
+// Host: LAPH_EINVAL (naming `who` and the first bad site) unless every spatial
+// link entry of the host links in `layout` is finite; the temporal slot of
+// LAPH_LAYOUT_CONF is not read.  NaN or Inf links would only turn into a solve
+// that never converges, so they are refused before any device work.
+int check_links_finite(const double* links, int layout, int V3, const char* who);
 // Device: same reorder for links already in device memory (ROWMAJOR or CONF).
 int links_to_soa_device(const double* links, int layout, int V3, double2* soa, cudaStream_t st);
 // Device: average spatial plaquette of nts timeslices -> out[nts]

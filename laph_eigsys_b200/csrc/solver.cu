@@ -305,6 +305,7 @@ int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout
     set_error("laph_solver_set_links: bad argument");
     return LAPH_EINVAL;
   }
+  if (!on_device) LAPH_TRY(check_links_finite(links, layout, s->hd[i].V3, "laph_solver_set_links"));
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const ProbDesc& d = s->hd[i];
   double2* dst = s->U64raw + d.u64;  // pristine copy; run() smears a working copy
@@ -552,7 +553,8 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
       if (!p.active || !(p.max_resid > kCapResid)) continue;
       const double tb0 = 1.0 + 2.0 * p.lam_cut / (p.lam_max - p.lam_cut);
       // (1e8 after the first pass: 34 instead of 26 in pass 2, same 8 iterations, no faster; 1e10: 42, slower)
-      const int m_safe = (int)std::floor(std::acosh(1e6) / std::acosh(std::max(tb0, 1.0 + 1e-12)));
+      const double ratio = std::acosh(1e6) / std::acosh(std::max(tb0, 1.0 + 1e-12));
+      const int m_safe = std::isfinite(ratio) ? (int)std::min(std::floor(ratio), 1e6) : 2;  // NaN window: degree 2
       m = std::min(m, std::max(2, m_safe));
     }
     for (int i = 0; i < s->np; ++i)

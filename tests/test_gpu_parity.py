@@ -85,3 +85,29 @@ def test_matmult_rejects_bad_window(gpu):
     ctx = gpu.Context(4, 1.0, 2.0, 8)
     with pytest.raises(gpu.LaphError):
         ctx.matmult(np.zeros(3 * 64, dtype=np.complex128))
+
+
+def test_non_finite_links_are_refused_on_the_host(gpu, orc):
+    """NaN or Inf in a spatial link is refused by laph_set_links / laph_solver_set_links before any device work
+    (LAPH_EINVAL naming the site); the context and the solver stay usable with good links."""
+    L = 4
+    U = random_links(L, 0.4, 78)
+    for bad_value, site in ((np.nan, 5), (np.inf, 0), (-np.inf, L ** 3 - 1)):
+        Ub = U.copy()
+        Ub[site, 1, 2, 0] = bad_value
+        ctx = gpu.Context(L)
+        with pytest.raises(gpu.LaphError) as e:
+            ctx.set_links(Ub)
+        assert e.value.status == gpu._lib.LAPH_EINVAL and f"site {site}" in str(e.value)
+        ctx.set_links(U)
+        assert abs(ctx.plaquette() - orc.plaquette(U, L)) < 1e-13
+        ctx.close()
+        s = gpu.Solver([(L, 8)], tol=1e-10, deg=8)
+        with pytest.raises(gpu.LaphError) as e:
+            s.set_links(0, Ub)
+        assert e.value.status == gpu._lib.LAPH_EINVAL
+        s.set_links(0, U)
+        st, _ = s.run()
+        assert st == 0
+        s.close()
+
