@@ -305,7 +305,6 @@ int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout
     set_error("laph_solver_set_links: bad argument");
     return LAPH_EINVAL;
   }
-  if (!on_device) LAPH_TRY(check_links_finite(links, layout, s->hd[i].V3, "laph_solver_set_links"));
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
   const ProbDesc& d = s->hd[i];
   double2* dst = s->U64raw + d.u64;  // pristine copy; run() smears a working copy
@@ -318,11 +317,17 @@ int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout
     // copy to the scratch and transpose with a small kernel
     LAPH_TRY(links_to_soa_device(links, layout, d.V3, dst, s->st));
   } else if (layout == LAPH_LAYOUT_ROWMAJOR || layout == LAPH_LAYOUT_CONF) {
-    // raw copy into the staging area, reorder on the device
+    // raw copy into the staging area, reorder on the device; the finiteness
+    // scan of the host links runs while the copy is in flight
     const size_t n = (layout == LAPH_LAYOUT_CONF ? 36 : 27) * (size_t)d.V3;
     LAPH_CUDA_TRY(cudaMemcpyAsync(s->stage, links, n * sizeof(double2), cudaMemcpyHostToDevice, s->st));
+    if (int e = check_links_finite(links, layout, d.V3, "laph_solver_set_links")) {
+      cudaStreamSynchronize(s->st);  // leave no copy in flight; the stored links are unchanged
+      return e;
+    }
     LAPH_TRY(links_to_soa_device(reinterpret_cast<const double*>(s->stage), layout, d.V3, dst, s->st));
   } else {
+    LAPH_TRY(check_links_finite(links, layout, d.V3, "laph_solver_set_links"));
     std::vector<double2> soa(27 * (size_t)d.V3);
     LAPH_TRY(links_to_soa(links, layout, d.V3, soa.data()));
     LAPH_CUDA_TRY(cudaMemcpyAsync(dst, soa.data(), soa.size() * sizeof(double2), cudaMemcpyHostToDevice, s->st));
