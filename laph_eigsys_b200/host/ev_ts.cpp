@@ -17,6 +17,7 @@
 // Beyond the reference: FP32 ILDG input is read (widened to FP64), and
 // --resume skips timeslices whose three output files are already complete
 // (right sizes, eigenvectors passing check_trace).
+#include <omp.h>
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -123,6 +124,8 @@ int main(int argc, char** argv) {
   laph_config P;
   int st = laph_parse_parameters(params.c_str(), &P);
   if (st != LAPH_OK) return die(st, "parameters");
+  // host threads (LIME reading, checks), as the reference's OMP_THRDS sets them (shell_matop.cpp:26)
+  if (P.OMP_THRDS > 0) omp_set_num_threads(P.OMP_THRDS);
   const int L = P.LX, LT = P.LT, nev = P.NEV;
   const int V3 = L * L * L, dim = 3 * V3;
   const int size = env_int("LAPH_WORLD_SIZE", "WORLD_SIZE", 1), rank = env_int("LAPH_RANK", "RANK", 0);

@@ -11,6 +11,8 @@
 // phases_... files, then the table "#alpha1 alpha2 lowest_ev" on stdout.
 // The reference hard-codes timeslice 10; --ts overrides it.
 #include <algorithm>
+#include <omp.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -67,6 +69,8 @@ int main(int argc, char** argv) {
   laph_config P;
   int st = laph_parse_parameters(params.c_str(), &P);
   if (st != LAPH_OK) return die(st, "parameters");
+  // host threads (LIME reading, checks), as the reference's OMP_THRDS sets them (shell_matop.cpp:26)
+  if (P.OMP_THRDS > 0) omp_set_num_threads(P.OMP_THRDS);
   const int L = P.LX, LT = P.LT, nev = P.NEV, V3 = L * L * L;
   if (ts < 0 || ts >= LT) {
     std::fprintf(stderr, "laph_tune_hyp: timeslice %d outside 0..%d\n", ts, LT - 1);
