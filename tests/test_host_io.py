@@ -363,3 +363,23 @@ def test_lime_reorder_transcribes_reference_loop(tmp_path, orc):
     assert np.array_equal(lb.lime_read_gauge(p, T, L, ti, tf), want)
     st, ref = orc.lime_read_gauge(p, T, L, ti, tf)
     assert st == 0 and np.array_equal(ref, want)
+
+
+def test_reference_quirks_of_the_small_host_functions(orc):
+    """check_trace is one-sided as in read_write.cpp:29-33 (|tr| - nev > eps fails, a shrunken block passes);
+    recover_spectrum gives NaN for theta < 1 (acosh, recover_spec.cpp:24-30), where the eigenvalue lies above
+    LAM_C; fix_phase leaves a column whose first entry is 0 as it is (arg 0 = 0)."""
+    rng = np.random.default_rng(9)
+    Q, _ = np.linalg.qr(rng.normal(size=(60, 5)) + 1j * rng.normal(size=(60, 5)))
+    assert lb.check_trace(Q)[0]
+    assert lb.check_trace(Q * 0.99)[0]          # trace 4.9 < nev: passes, as in the reference
+    assert not lb.check_trace(Q * 1.0001)[0]    # trace above nev by more than 1e-9: fails
+    th = np.array([3.0, 1.0, 0.5])
+    a = lb.recover_spectrum(th, 8, 12.0, 0.6)
+    b = orc.recover_spectrum(th, 8, 12.0, 0.6)
+    assert np.isnan(a[2]) and np.isnan(b[2]) and abs(a[1] + 0.6) < 1e-15 and np.allclose(a[:2], b[:2], rtol=0,
+                                                                                          atol=1e-15)
+    V = Q.copy()
+    V[0, 2] = 0.0
+    Vf, ph = lb.fix_phase(V)
+    assert ph[2] == 0.0 and np.array_equal(Vf[:, 2], V[:, 2])
