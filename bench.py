@@ -5,9 +5,8 @@ Workload (one "step"): every timeslice of a seeded synthetic 32^3 x 64 gauge
 field (U = exp(i*0.3*H), stout-smeared 5 x rho=0.1 on the device in FP64),
 solved for the lowest nev = 120 eigenpairs of -Delta to a residual
 ||(-Delta)v - lambda v|| / (||v|| lambda_max) <= 1e-9 by the batched block
-solver (FP32 filter matvecs with BF16 links + per-site scale, FP64 Gram /
-Cholesky / Rayleigh-Ritz / residuals), phase-fixed.  All 64 timeslices run as
-one batch.
+solver (FP32 filter matvecs on FP32 links, FP64 Gram / Cholesky /
+Rayleigh-Ritz / residuals), phase-fixed.  All 64 timeslices run as one batch.
 
 value : timeslices/s with links resident in HBM (device-timed, CUDA events on
         the solver's stream, K steps between barriers, max over ranks).
@@ -18,8 +17,12 @@ roofline: lap_cheb_mrhs (the FP32 multi-RHS Chebyshev stencil), algorithmic
 cpu_baseline: the CPU FP64 oracle (restated reference ev_ts path: stout
         smearing + Krylov-Schur on T_DEG(B)) on one timeslice of the same
         workload, all host cores.
+Also reported: the plain GPU form (MatShell + Krylov-Schur), the source shape
+and displacement kernels on the solved eigenvectors, the LIME reader's
+throughput (lime_io), and with --autotune N the autotuner's choice.
 
---impl reference runs that CPU path as the reference arm.
+--impl reference runs that CPU path as the reference arm (--cpu-layout
+per-core: one single-threaded timeslice per core, the reference's MPI layout).
 Multi-GPU (torchrun): timeslices are independent; each rank solves its own
 64-timeslice batch (weak scaling), no collective on the data path.
 """
