@@ -194,7 +194,10 @@ int laph_solver_destroy(laph_solver* s);
 /* Links of problem i: FP64, layout as above; host (on_device = 0) or device pointer. */
 int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout, int on_device);
 /* Run: smear + solve all problems.  Results stay on the device; results (may be
- * NULL) receives one laph_result per problem. */
+ * NULL) receives one laph_result per problem.  With the environment variable
+ * LAPH_TRACE=1 each outer iteration prints one line to stderr: active, locked
+ * and converged counts, the largest wanted residual, the filter degree and the
+ * phase times of the small dense step. */
 int laph_solver_run(laph_solver* s, laph_result* results);
 /* Fetch problem i: evals[nev] (reference convention, see top), evecs column-major
  * complex128 [3*V3][nev] (may be NULL), phases[nev] (may be NULL). */
