@@ -365,3 +365,23 @@ def test_oracle_hyp_uses_reference_lookup_tables(tmp_path, orc, L):
         Us = _proj_su3_imp(new)
     got = orc.smear_hyp(U, L, a1, a2, iters)
     assert np.abs(got - Us).max() <= 1e-12
+
+
+REF_PARAMS = os.environ.get("LAPH_REFERENCE", "/root/reference") + "/src/parameters.txt"
+
+
+@pytest.mark.skipif(not os.path.isfile(REF_PARAMS), reason="the reference checkout is not on this machine")
+def test_reference_shipped_parameters_file(tmp_path):
+    """The parameters.txt the reference ships (src/parameters.txt, with its trailing spaces after values) parses
+    to what IO::set_values stores (the command-line programs read their settings through this parser)."""
+    p = tmp_path / "parameters.txt"
+    p.write_bytes(open(REF_PARAMS, "rb").read())
+    r = ref("params", p)
+    assert not r["threw"]
+    c = lb.parse_parameters(p)
+    assert (c["LT"], c["LX"], c["NEV"], c["iter"], c["DEG"], c["OMP_THRDS"]) == (r["LT"], r["LX"], r["NEV"], r["iter"],
+                                                                                 r["DEG"], r["OMP_THRDS"])
+    for k, rk in (("alpha_1", "alpha_1"), ("alpha_2", "alpha_2"), ("alpha_1_i", "alpha_1_i"), ("alpha_1_f", "alpha_1_f"),
+                  ("alpha_2_i", "alpha_2_i"), ("alpha_2_f", "alpha_2_f"), ("LAM_L", "lambda_l"), ("LAM_C", "lambda_c")):
+        assert c[k] == r[rk], k
+    assert (c["config_path"], c["result_path"], c["in_path"]) == (r["conf"], r["res"], r["in_path"])
