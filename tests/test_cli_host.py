@@ -184,3 +184,26 @@ def test_sourceshape_cli_errors(tmp_path):
         r = _run(SHAPE, ["1227", "3", "8"], tmp_path)
         assert r.returncode == 1 and "laph_sourceshape: sourceshape:" in r.stderr
         assert not list(tmp_path.glob("sourceshape_nev*"))
+
+
+def test_window_model_file_and_ev_ts_loading(tmp_path):
+    """The shipped learned-window model (data/window_mlp.bin: "LAPHMLP1", int32 nparams, int32 nnorm, float32
+    values, then the training record as JSON) has the shape the library expects and finite values; laph_ev_ts with
+    window = mlp loads it (from beside the executable) and, without a device, stops at its first device step, not
+    at the model."""
+    import json
+    from laph_eigsys_b200 import window as lw
+    raw = open(lw.MODEL_PATH, "rb").read()
+    assert raw[:8] == b"LAPHMLP1"
+    npar, nnorm = (int(v) for v in np.frombuffer(raw[8:16], dtype="<i4"))
+    end = 16 + 4 * (npar + nnorm)
+    assert npar == lb.lib.laph_mlp_nparams() and len(raw) >= end
+    meta = json.loads(raw[end:].decode()) if len(raw) > end else {}
+    assert "val_cut_rel_err_median" in meta
+    m = lw.load_model()
+    assert m.size == npar + nnorm and np.all(np.isfinite(m))
+    if _has_device():
+        pytest.skip("a device is present")
+    _setup(tmp_path, extra="window = mlp\n")
+    r = _run(EV_TS, ["--conf", "1227"], tmp_path)
+    assert r.returncode == 1 and "laph_ev_ts: device memory:" in r.stderr and "window" not in r.stderr
