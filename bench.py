@@ -49,7 +49,8 @@ CONFIGS = {
                guard=16, link_prec="fp32", tol=1e-9, deg=60),
     # 8^3 x 16, eps 0.4, stout 3 x 0.1, nev 60
     "c1": dict(L=8, T=16, eps=0.4, seed=1227, smear="stout", p1=0.1, p2=0.0, iters=3, compat=1, nev=60,
-               guard=16, link_prec="fp32", tol=1e-9, deg=32),
+               guard=16, link_prec="fp32", tol=1e-9, deg=32,
+               lam_c_ref=2.07),  # the reference's window must lie above lambda_60 (1.88 here); 0.65 suits the rest
     # one launch mixing 16^3 x 32 (nev 60), 24^3 x 48 (nev 120), 32^3 x 64 (nev 180), APE 0.5 x 10
     "c4": dict(mixed=[(16, 32, 60, 1230), (24, 48, 120, 1231), (32, 64, 180, 1232)], eps=0.3, smear="ape", p1=0.5,
                p2=0.0, iters=10, compat=1, guard=16, link_prec="fp32", tol=1e-9, deg=48, L=32, T=144, nev=180),
