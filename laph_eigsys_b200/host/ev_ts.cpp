@@ -90,6 +90,25 @@ bool outputs_complete(const char* dir, int config, int t, int dim, int nev) {
   return laph_check_trace(dim, nev, V.data(), &tr, &sum) == 1;
 }
 
+// The run's settings on stdout before any work, as the reference's rank 0
+// prints them (IO::print_summary, modules/par_io.cpp:138-154), plus this
+// program's own keys; every line starts with '#' so that the JSON lines that
+// follow stay easy to pick out.
+void print_summary(const laph_config& P) {
+  const long long V3 = (long long)P.LX * P.LX * P.LX;
+  static const char* smear[] = {"none", "hyp", "stout", "ape"};
+  static const char* window[] = {"fixed", "lanczos", "mlp"};
+  std::printf("# lattice %d x %d x %d x %d, nev %d\n", P.LT, P.LX, P.LX, P.LX, P.NEV);
+  std::printf("# smearing %s: alpha_1 %g alpha_2 %g rho %g alpha %g, %d iterations\n",
+              smear[P.smear >= 0 && P.smear < 4 ? P.smear : 0], P.alpha_1, P.alpha_2, P.rho, P.alpha, P.iter);
+  std::printf("# Chebyshev (plain form): LAM_L %g LAM_C %g DEG %d\n", P.LAM_L, P.LAM_C, P.DEG);
+  std::printf("# solver %s, tol %g, guard %d, window %s, filter_deg %d, autotune %d\n", P.solver ? "plain" : "block",
+              P.tol, P.guard, window[P.window >= 0 && P.window < 3 ? P.window : 1], P.filter_deg, P.autotune);
+  std::printf("# configurations from %s, results to %s\n", P.config_path, P.result_path);
+  std::printf("# MAT_ENTRIES %lld, V3 %lld, doubles per configuration %lld, OMP_THRDS %d\n", 3 * V3, V3,
+              72 * V3 * P.LT, P.OMP_THRDS);
+}
+
 double trace_vdv(int dim, int nev, const double* V) {
   double tr = 0.0, sum = 0.0;
   laph_check_trace(dim, nev, V, &tr, &sum);
@@ -121,6 +140,7 @@ int main(int argc, char** argv) {
     usage();
     return 2;
   }
+  std::printf("Working on configuration %d\n", config);
   laph_config P;
   int st = laph_parse_parameters(params.c_str(), &P);
   if (st != LAPH_OK) return die(st, "parameters");
@@ -129,6 +149,10 @@ int main(int argc, char** argv) {
   const int L = P.LX, LT = P.LT, nev = P.NEV;
   const int V3 = L * L * L, dim = 3 * V3;
   const int size = env_int("LAPH_WORLD_SIZE", "WORLD_SIZE", 1), rank = env_int("LAPH_RANK", "RANK", 0);
+  if (rank == 0) {
+    print_summary(P);
+    std::printf("calculating config %d\n", config);
+  }
   int t0, ntodo;
   st = laph_timeslice_split(LT, size, rank, &t0, &ntodo);
   if (st != LAPH_OK) return die(st, "timeslice split");
