@@ -10,6 +10,11 @@
  * are staged through the context's stream; "device" pointers are CUDA global
  * memory of the context's device and are used in place.
  *
+ * Threads: a context (laph_ctx) or a solver (laph_solver) is used by one thread
+ * at a time; separate contexts and solvers, on one device or several, may be
+ * driven from separate threads at once, each on its own CUDA stream.  The
+ * host-only functions (file I/O, parsing, fix_phase, ...) are reentrant.
+ *
  * Conventions (identical to the reference):
  *   site      = x*L*L + y*L + z                     (modules/navigation.cpp:27-88)
  *   vector    = complex128[3*V3], index 3*site+colour (modules/shell_matop.cpp:33-38)
