@@ -2,9 +2,11 @@
 
 TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the CPU
 baseline leg of bench.py as the checker / timed CPU baseline, never by the
-product path.  Parity status: unpinned against reference outputs (the
-reference cannot be built here and ships no golden vectors); pinned by
-analytic known answers (see laph_oracle.h).
+product path.  Parity status: arithmetic unpinned against reference outputs
+(the reference cannot be built here as a whole and ships no golden vectors);
+site indexing and formulas checked on the reference's compiled parameter parser
+and lookup tables (oracle/_ref/ref_dump), and pinned by analytic known answers
+(see laph_oracle.h).
 """
 import ctypes
 import os

@@ -1,8 +1,10 @@
 /*
  * laph_oracle.cpp -- CPU FP64 oracle (TEST INFRASTRUCTURE, see laph_oracle.h).
  *
- * Parity status: unpinned against reference outputs (the reference cannot be
- * built here and has no golden vectors); pinned by analytic known answers.
+ * Parity status: arithmetic unpinned against reference outputs (the reference
+ * cannot be built here as a whole and has no golden vectors); site indexing and
+ * formulas checked on the reference's compiled lookup tables, and pinned by
+ * analytic known answers (laph_oracle.h).
  * Each function cites the reference file:line it restates.  Third-party
  * arithmetic the reference delegates to libraries is restated from the
  * mathematics:

@@ -7,14 +7,19 @@
  * and bench.py's CPU-baseline leg may load it, and only as the checker or the
  * timed CPU baseline -- never as a product code path.
  *
- * Parity status: UNPINNED against reference outputs.  The reference cannot be
- * built on this machine (Eigen, PETSc, SLEPc, c-lime, Boost and MPI are
- * absent) and it ships no golden vectors, stored eigenvalues or fixtures.  The
- * oracle is instead pinned by analytic known answers that follow from the
- * reference's own checks: the unit gauge field (free spectrum
- * sum_i 4 sin^2(pi n_i / L) with its degeneracies), pure-gauge fields
- * (gauge-covariant spectrum), SU(3) unitarity/determinant, tr(V^dag V) = nev,
- * and a dense eigendecomposition of the assembled operator for small L.
+ * Parity status: the arithmetic is UNPINNED against reference outputs.  The
+ * reference cannot be built here as a whole (Eigen, PETSc, SLEPc, c-lime,
+ * Boost and MPI are absent) and it ships no golden vectors, stored eigenvalues
+ * or fixtures.  Its parameter parser and lookup tables (modules/par_io.cpp,
+ * modules/navigation.cpp) need only the standard library; the tests compile
+ * them unchanged into a driver (oracle/_ref/ref_dump) and check this oracle's
+ * site indexing, matvec, smearings, source shape and displacement against the
+ * reference's formulas evaluated on those compiled tables.  Beyond that the
+ * oracle is pinned by analytic known answers that follow from the reference's
+ * own checks: the unit gauge field (free spectrum sum_i 4 sin^2(pi n_i / L)
+ * with its degeneracies), pure-gauge fields (gauge-covariant spectrum), SU(3)
+ * unitarity/determinant, tr(V^dag V) = nev, and a dense eigendecomposition of
+ * the assembled operator for small L.
  *
  * Conventions (all follow the reference):
  *   site   = x*L*L + y*L + z                         (modules/navigation.cpp:27-88)
