@@ -144,3 +144,26 @@ def test_plaquette_unit_and_random(orc):
     p0 = orc.plaquette(U, 4)
     p1 = orc.plaquette(orc.smear_hyp(U, 4, 0.62, 0.62, 1), 4)
     assert p1 > p0  # smearing raises the plaquette
+
+
+@pytest.mark.parametrize("cond", [1e2, 1e4, 1e6])
+def test_proj_su3_ill_conditioned(orc, cond):
+    """The projection's Jacobi route (the one the device kernel shares) on matrices with singular values spread
+    over `cond`, and on near-unitary ones (what smearing produces).  The reference's formula M (M^dag M)^{-1/2}
+    squares the condition number, so its polar factor is good to ~cond^2 eps (numpy's eigh on the same formula does
+    no better), and so is the unitarity of the result; near-unitary inputs come out at rounding level."""
+    rng = np.random.default_rng(int(np.log10(cond)))
+    for _ in range(20):
+        u, _ = np.linalg.qr(rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3)))
+        v, _ = np.linalg.qr(rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3)))
+        M = u @ np.diag([1.0, cond ** -0.5, 1.0 / cond]) @ v
+        W = orc.proj_su3(M)
+        P = u @ v
+        P = P / np.linalg.det(P) ** (1.0 / 3.0)
+        bound = 100 * cond ** 2 * 2.2e-16 + 1e-12
+        assert np.abs(W - P).max() < bound and su3_err(W) < bound
+        N = P + 1e-3 * (rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3)))  # near-unitary
+        u2, s2, vh2 = np.linalg.svd(N)
+        Q = u2 @ vh2
+        Q = Q / np.linalg.det(Q) ** (1.0 / 3.0)
+        assert np.abs(orc.proj_su3(N) - Q).max() < 1e-13
