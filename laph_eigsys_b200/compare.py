@@ -9,6 +9,9 @@ same for U^dag U and V^dag V) and adds the numbers that decide parity:
             columns contain completely (gap < 1e-6 * 12 inside a cluster), from
             the principal angles between the two subspaces
   phase     max |arg U(0, n)| and |arg V(0, n)|: 0 for phase-fixed vectors
+  col       max |u_n - v_n| over the columns of non-degenerate eigenvalues (with
+            --eigenvalues): phase-fixed vectors of a simple eigenvalue agree
+            entry by entry
 
 Usage: python -m laph_eigsys_b200.compare DIR_U DIR_V --conf N --lx L --nev K [--timeslices 0 1 ...]
        [--eigenvalues] (also read eigenvalues.%04d.%03d from both) [--json]
@@ -55,6 +58,12 @@ def compare_timeslice(U, V, lam_u=None, lam_v=None, gap=1e-6 * 12.0):
             worst = max(worst, sin_max_angle(U[:, order_u[:end]], V[:, order_v[:end]]))
         out["proj"] = worst
         out["clusters_checked"] = len(ends)
+        col, start = 0.0, 0
+        for end in ends:
+            if end - start == 1:  # a simple eigenvalue: the phase-fixed vector is unique
+                col = max(col, float(np.abs(U[:, order_u[start]] - V[:, order_v[start]]).max()))
+            start = end
+        out["col"] = col
     else:
         out["proj"] = sin_max_angle(U, V)
     return out
@@ -79,7 +88,7 @@ def main(argv=None):
     ap.add_argument("--json", action="store_true")
     a = ap.parse_args(argv)
     dim = 3 * a.lx ** 3
-    worst = {"dlam": 0.0, "proj": 0.0}
+    worst = {"dlam": 0.0, "proj": 0.0, "col": 0.0}
     for t in a.timeslices:
         U = read_eigsys_bin(a.dir_u, "eigenvectors", a.conf, t, dim, a.nev)
         V = read_eigsys_bin(a.dir_v, "eigenvectors", a.conf, t, dim, a.nev)
@@ -97,7 +106,7 @@ def main(argv=None):
             print(f"ts {t}: tr(U^dag V) = {r['tr_uv']:.12g}  sum(U^dag V) = {r['sum_uv']:.6g}  "
                   f"sum|U^dag V|^2 = {r['sum_abs2_uv']:.12g}  tr(U^dag U) = {r['tr_uu']:.12g}  "
                   f"tr(V^dag V) = {r['tr_vv']:.12g}  proj = {r['proj']:.3e}"
-                  + (f"  dlam = {r['dlam']:.3e}" if "dlam" in r else ""))
+                  + (f"  dlam = {r['dlam']:.3e}  col = {r['col']:.3e}" if "dlam" in r else ""))
     print(json.dumps({"worst": worst}) if a.json else f"worst: {worst}")
     return 0
 

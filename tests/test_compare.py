@@ -37,6 +37,11 @@ def test_compare_equal_up_to_phases_and_cluster_rotation(tmp_path):
     V = V * np.exp(1j * rng.uniform(-np.pi, np.pi, 6))[None, :]  # column phases
     r = compare_timeslice(U, V, ev, ev)
     assert r["proj"] < 1e-12 and r["dlam"] == 0.0 and r["clusters_checked"] == 3
+    assert r["col"] > 0.1                                     # column 5 (simple) carries a different phase in V
+    Uf, _ = lb.fix_phase(U)
+    Vf, _ = lb.fix_phase(V)
+    r = compare_timeslice(Uf, Vf, ev, ev)
+    assert r["col"] < 1e-14 and r["phase"] < 1e-14            # phase-fixed: the simple column agrees
     W = U.copy()
     W[:, 5] = Q[:, 7]                                         # a vector of another eigenvalue
     r = compare_timeslice(U, W, ev, ev)
