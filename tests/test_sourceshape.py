@@ -115,3 +115,24 @@ def test_sourceshape_rejects_odd_L():
     with pytest.raises(lb.LaphError) as e:
         lb.sourceshape_avg(5, np.ones(27))
     assert e.value.status == lb._lib.LAPH_EINVAL
+
+
+def test_ascii_writer_matches_ostream_setprecision_12(tmp_path):
+    """write_sourceshape_ascii formats with std::ostream << setprecision(12) (modules/read_write.cpp:205-220);
+    the library's %.12g writer must give the same bytes, exponents and trailing-zero trimming included."""
+    vals = [0.0, 2.0, 2.8284271247461903, 1e-5, 123456789012.5, 1.5e-300, 7.0e20, 0.1, 3.4641016151377544,
+            12.000000000000002]
+    r = np.array(vals)
+    psi = np.array(vals[::-1])
+    lb.write_sourceshape(tmp_path, 7, 3, 11, r, psi)
+    got = open(tmp_path / "sourceshape_nev11.7.3").read()
+    src = tmp_path / "fmt.cpp"
+    src.write_text(
+        "#include <fstream>\n#include <iomanip>\n#include <iostream>\nint main(){double a;double b;\n"
+        "std::cout << \"#r\\tpsi(r)\" << std::endl;\n"
+        "while (std::cin >> a >> b) std::cout << std::setprecision(12) << a << \" \" << b << std::endl;}\n")
+    exe = tmp_path / "fmt"
+    subprocess.run(["g++", "-O1", "-o", str(exe), str(src)], check=True, timeout=120)
+    feed = "".join(f"{float(a)!r} {float(b)!r}\n" for a, b in zip(r, psi))
+    want = subprocess.run([str(exe)], input=feed, capture_output=True, text=True, check=True).stdout
+    assert got == want
