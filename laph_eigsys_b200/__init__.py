@@ -39,12 +39,14 @@ def gauge_random(L, nt, eps, seed):
 
 
 def lime_write_gauge(path, conf, L, T, precision=64):
+    """ILDG/LIME file of conf (T, L^3, 4, 3, 3) complex128 (laph_lime_write_gauge_prec), FP64 or FP32 payload."""
     conf = _c128(conf)
     check(lib.laph_lime_write_gauge_prec(str(path).encode(), _ptr(conf), L, T, precision),
           "laph_lime_write_gauge_prec")
 
 
 def lime_read_gauge(path, T, L, t_i, t_f):
+    """Timeslices t_i..t_f of an FP64 ILDG file (read_lime_gauge_field_doubleprec_timeslices, modules/io.cpp:22-146)."""
     conf = np.empty((t_f - t_i + 1, L ** 3, 4, 3, 3), dtype=np.complex128)
     check(lib.laph_lime_read_gauge(str(path).encode(), T, L, t_i, t_f, _ptr(conf)), "laph_lime_read_gauge")
     return conf
@@ -87,6 +89,7 @@ def sourceshape_avg(L, psi):
 
 
 def write_sourceshape(dirname, config, t, nev, r, psi):
+    """write_sourceshape_ascii / _bin (modules/read_write.cpp:205-234): the radius-averaged psi(r) files."""
     r = np.ascontiguousarray(r, dtype=np.float64)
     psi = np.ascontiguousarray(psi, dtype=np.float64)
     check(lib.laph_write_sourceshape(str(dirname).encode() if dirname else None, config, t, nev, len(r), _ptr(r),
@@ -106,6 +109,7 @@ def timeslice_split(LT, size, rank):
 
 
 def parse_parameters(path):
+    """parameters.txt as IO::set_values reads it (modules/par_io.cpp:8-136), plus this library's keys; a dict."""
     cfg = _lib.laph_config()
     check(lib.laph_parse_parameters(str(path).encode(), ctypes.byref(cfg)), "laph_parse_parameters")
     out = {}
@@ -116,6 +120,7 @@ def parse_parameters(path):
 
 
 def check_trace(V):
+    """check_trace (modules/read_write.cpp:20-35): (passes, tr(V^dag V), sum(V^dag V))."""
     V = np.asfortranarray(V, dtype=np.complex128)
     dim, nev = V.shape
     tr, sm = ctypes.c_double(), ctypes.c_double()
@@ -124,6 +129,7 @@ def check_trace(V):
 
 
 def fix_phase(V):
+    """fix_phase (modules/eigensystem.cpp:4-30): (V with every first entry real >= 0, the removed phases)."""
     V = np.asfortranarray(V, dtype=np.complex128)
     dim, nev = V.shape
     Vf = np.empty_like(V, order="F")
@@ -167,6 +173,7 @@ def read_gauge_matrices(path, V3):
 
 
 def recover_spectrum(theta, deg, lam_l, lam_c):
+    """recover_spectrum (modules/recover_spec.cpp:13-54): stored eigenvalues (of Delta, <= 0) from T_deg(B) ones."""
     theta = np.ascontiguousarray(theta, dtype=np.float64)
     out = np.empty_like(theta)
     check(lib.laph_recover_spectrum(len(theta), _ptr(theta), deg, lam_l, lam_c, _ptr(out)), "laph_recover_spectrum")
@@ -174,18 +181,21 @@ def recover_spectrum(theta, deg, lam_l, lam_c):
 
 
 def write_eigsys_bin(dirname, prefix, config, t, V):
+    """write_eig_sys_bin (modules/read_write.cpp:176-201): "<dir>/<prefix>.%04d.%03d", check_trace first."""
     V = np.asfortranarray(V, dtype=np.complex128)
     check(lib.laph_write_eigsys_bin(str(dirname).encode(), prefix.encode(), config, t, V.shape[0], V.shape[1],
                                     ctypes.c_void_p(V.ctypes.data)), "laph_write_eigsys_bin")
 
 
 def write_eigenvalues_bin(dirname, prefix, config, t, ev):
+    """write_eigenvalues_bin (modules/read_write.cpp:237-250): raw doubles to "<dir>/<prefix>.%04d.%03d"."""
     ev = np.ascontiguousarray(ev, dtype=np.float64)
     check(lib.laph_write_eigenvalues_bin(str(dirname).encode(), prefix.encode(), config, t, len(ev), _ptr(ev)),
           "laph_write_eigenvalues_bin")
 
 
 def read_eigsys_bin(dirname, prefix, config, t, dim, nev):
+    """read_evectors_bin_ts (modules/read_write.cpp:70-97): [dim][nev] column-major block, check_trace applied."""
     V = np.empty((dim, nev), dtype=np.complex128, order="F")
     check(lib.laph_read_eigsys_bin(str(dirname).encode(), prefix.encode(), config, t, dim, nev,
                                    ctypes.c_void_p(V.ctypes.data)), "laph_read_eigsys_bin")
@@ -193,6 +203,7 @@ def read_eigsys_bin(dirname, prefix, config, t, dim, nev):
 
 
 def read_eigenvalues_bin(dirname, prefix, config, t, nev):
+    """read_eigenvalues_bin (modules/read_write.cpp:135-152): nev raw doubles."""
     ev = np.empty(nev)
     check(lib.laph_read_eigenvalues_bin(str(dirname).encode(), prefix.encode(), config, t, nev, _ptr(ev)),
           "laph_read_eigenvalues_bin")
@@ -211,6 +222,7 @@ class Context:
         self.deg = deg
 
     def close(self):
+        """Free the context's device memory and stream (laph_ctx_destroy)."""
         if self._h:
             lib.laph_ctx_destroy(self._h)
             self._h = None
@@ -222,48 +234,59 @@ class Context:
             pass
 
     def set_window(self, lam_l, lam_c, deg):
+        """LAM_L, LAM_C and DEG of the MatShell product (laph_ctx_set_window)."""
         check(lib.laph_ctx_set_window(self._h, lam_l, lam_c, deg), "laph_ctx_set_window")
         self.deg = deg
 
     def set_links(self, links, layout=LAYOUT_ROWMAJOR):
+        """Host links of the timeslice (laph_set_links; map_timeslice_to_eigen for LAYOUT_CONF)."""
         links = _c128(links)
         check(lib.laph_set_links(self._h, _ptr(links), layout), "laph_set_links")
 
     def get_links(self, layout=LAYOUT_ROWMAJOR):
+        """The (smeared) links back on the host (laph_get_links; Tslice::get_gauge)."""
         shape = (self.V3, 4, 3, 3) if layout == LAYOUT_CONF else (self.V3, 3, 3, 3)
         out = np.empty(shape, dtype=np.complex128)
         check(lib.laph_get_links(self._h, _ptr(out), layout), "laph_get_links")
         return out
 
     def smear(self, kind, p1, p2, iters, compat=1):
+        """FP64 smearing on the device (laph_smear): kind SMEAR_HYP / SMEAR_STOUT / SMEAR_APE."""
         check(lib.laph_smear(self._h, kind, p1, p2, iters, compat), "laph_smear")
 
     def smearing_hyp(self, alpha_1, alpha_2, iters):
+        """Tslice::smearing_hyp (modules/timeslice.cpp:243-369) on the device."""
         self.smear(SMEAR_HYP, alpha_1, alpha_2, iters, 0)
 
     def smearing_stout(self, rho, iters, compat=1):
+        """Tslice::smearing_stout (modules/timeslice.cpp:145-193); compat keeps its backward-staple factor."""
         self.smear(SMEAR_STOUT, rho, 0.0, iters, compat)
 
     def smearing_ape(self, alpha, iters, compat=1):
+        """Tslice::smearing_ape (modules/timeslice.cpp:196-239); compat keeps its backward-staple factor."""
         self.smear(SMEAR_APE, alpha, 0.0, iters, compat)
 
     def matmult(self, x, deg=None):
+        """y = T_deg(B) x in FP64, the MatShell product (MatMult_Laplacian2D / tv_iter), host vectors."""
         x = _c128(x)
         y = np.empty_like(x)
         check(lib.laph_matmult(self._h, _ptr(x), _ptr(y), self.deg if deg is None else deg, 0), "laph_matmult")
         return y
 
     def matmult_device(self, x_ptr, y_ptr, deg=None):
+        """As matmult on device pointers (complex128[3 V3] each)."""
         check(lib.laph_matmult(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
                                self.deg if deg is None else deg, 1), "laph_matmult")
 
     def apply_neglap(self, x):
+        """(-Delta) x = 6 x - hop(x) in FP64 (laph_apply_neglap)."""
         x = _c128(x)
         y = np.empty_like(x)
         check(lib.laph_apply_neglap(self._h, _ptr(x), _ptr(y), 0), "laph_apply_neglap")
         return y
 
     def get_diagonal(self):
+        """MatGetDiagonal_Laplacian2D (modules/shell_matop.cpp:248-255): the constant -6."""
         d = np.empty(self.dim, dtype=np.complex128)
         check(lib.laph_get_diagonal(self._h, _ptr(d), 0), "laph_get_diagonal")
         return d
@@ -290,6 +313,7 @@ class Context:
         return W
 
     def plaquette(self):
+        """Average spatial plaquette (plaque_timeslice, modules/config_utils.cpp:388-426)."""
         p = ctypes.c_double()
         check(lib.laph_plaquette(self._h, ctypes.byref(p)), "laph_plaquette")
         return p.value
@@ -375,6 +399,7 @@ class Solver:
         self._h = h
 
     def close(self):
+        """Free the solver's device memory, graphs and stream (laph_solver_destroy)."""
         if self._h:
             lib.laph_solver_destroy(self._h)
             self._h = None
@@ -386,13 +411,16 @@ class Solver:
             pass
 
     def set_links(self, i, links, layout=LAYOUT_ROWMAJOR):
+        """Host links of problem i (laph_solver_set_links); non-finite entries are refused."""
         links = _c128(links)
         check(lib.laph_solver_set_links(self._h, i, _ptr(links), layout, 0), "laph_solver_set_links")
 
     def set_links_device(self, i, ptr, layout=LAYOUT_ROWMAJOR):
+        """Links of problem i from device memory at ptr (ROWMAJOR or CONF)."""
         check(lib.laph_solver_set_links(self._h, i, ctypes.c_void_p(ptr), layout, 1), "laph_solver_set_links")
 
     def run(self):
+        """(status, per-problem result dicts) of one smear + solve of every problem (laph_solver_run)."""
         res = (_lib.laph_result * len(self.problems))()
         st = lib.laph_solver_run(self._h, res)
         if st not in (_lib.LAPH_OK, _lib.LAPH_ENOTCONV):
@@ -400,6 +428,7 @@ class Solver:
         return st, [dict((f, getattr(r, f)) for f, _ in r._fields_) for r in res]
 
     def get(self, i, vectors=True):
+        """(eigenvalues as stored by the reference, phase-fixed eigenvectors [3 V3][nev] or None, phases) of problem i."""
         L, nev = self.problems[i]
         ev = np.empty(nev)
         V = np.empty((3 * L ** 3, nev), dtype=np.complex128, order="F") if vectors else None
@@ -409,6 +438,7 @@ class Solver:
         return ev, V, ph
 
     def stream(self):
+        """The solver's CUDA stream handle (an int), for timing or ordering work around run()."""
         h = ctypes.c_void_p()
         check(lib.laph_solver_stream(self._h, ctypes.byref(h)), "laph_solver_stream")
         return h.value
@@ -419,6 +449,7 @@ class Solver:
                                   else None, _ptr(phases), 0), "laph_solver_get")
 
     def timings(self):
+        """Device ms of the last run: smearing + setup, filter, dense + FP64 stencils, total."""
         t = (ctypes.c_double * 4)()
         check(lib.laph_solver_timings(self._h, t), "laph_solver_timings")
         return list(t)
@@ -447,6 +478,7 @@ class Solver:
         return psi
 
     def counters(self):
+        """Filter site-vector-steps, filter launches and all kernel launches of the last run."""
         c = (ctypes.c_longlong * 3)()
         check(lib.laph_solver_counters(self._h, c), "laph_solver_counters")
         return list(c)

@@ -142,6 +142,7 @@ _sig("laph_timeslice_split", c_int, c_int, c_int, c_int, P(c_int), P(c_int))
 
 
 class LaphError(RuntimeError):
+    """A LAPH_E* status from the library: .status is the code, the message carries laph_last_error()."""
     def __init__(self, status, where):
         self.status = status
         msg = lib.laph_last_error().decode(errors="replace")
