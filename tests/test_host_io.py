@@ -383,3 +383,16 @@ def test_reference_quirks_of_the_small_host_functions(orc):
     V[0, 2] = 0.0
     Vf, ph = lb.fix_phase(V)
     assert ph[2] == 0.0 and np.array_equal(Vf[:, 2], V[:, 2])
+
+
+def test_fp32_reader_refuses_truncated_record(tmp_path):
+    """The any-precision reader applies the same whole-record rule to FP32 files."""
+    L, T = 3, 3
+    conf = lb.gauge_random(L, T, 0.3, 8)
+    p = tmp_path / "c32"
+    lb.lime_write_gauge(p, conf, L, T, precision=32)
+    raw = p.read_bytes()
+    p.write_bytes(raw[:len(raw) - 100])
+    with pytest.raises(lb.LaphError) as e:
+        lb.lime_read_gauge_any(p, T, L, 0, 0)  # the first timeslice is all there, the record is not
+    assert e.value.status == _lib.LAPH_EIO
