@@ -702,9 +702,10 @@ def main():
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
-                "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-                "sourceshape": shape, "displacement": disp, "lime_io": lime_io, "autotune": tune,
-                "detail": {"outer_iterations": iters, "max_resid": max_resid, "filter_ms_per_step": filt_ms / args.steps,
+                "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk, "sourceshape": shape, "displacement": disp, "lime_io": lime_io, "autotune": tune,
+                "detail": {"outer_iterations": iters, "max_resid": max_resid,
+                           "filter_ms_per_step": filt_ms / args.steps,
                            "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
                                                        solver.timings()))}}
         print(json.dumps(line), flush=True)

@@ -90,7 +90,8 @@ _sig("laph_matmult_noalloc", c_int, c_void_p, c_int, c_double, c_double, c_int, 
 _sig("laph_apply_neglap", c_int, c_void_p, c_void_p, c_void_p, c_int)
 _sig("laph_get_diagonal", c_int, c_void_p, c_void_p, c_int)
 _sig("laph_plaquette", c_int, c_void_p, P(c_double))
-_sig("laph_eps_solve", c_int, c_void_p, c_int, c_int, c_double, c_int, c_int, c_u64, c_void_p, c_void_p, P(c_int), P(c_int), P(c_ll))
+_sig("laph_eps_solve", c_int, c_void_p, c_int, c_int, c_double, c_int, c_int, c_u64, c_void_p, c_void_p, P(c_int),
+     P(c_int), P(c_ll))
 _sig("laph_solve_opts_default", None, P(laph_solve_opts))
 _sig("laph_solver_create", c_int, P(c_void_p), P(laph_problem), c_int, P(laph_solve_opts), c_int)
 _sig("laph_solver_destroy", c_int, c_void_p)
