@@ -428,7 +428,8 @@ class Solver:
         return st, [dict((f, getattr(r, f)) for f, _ in r._fields_) for r in res]
 
     def get(self, i, vectors=True):
-        """(eigenvalues as stored by the reference, phase-fixed eigenvectors [3 V3][nev] or None, phases) of problem i."""
+        """(eigenvalues as the reference stores them, phase-fixed eigenvectors [3 V3][nev] or None, phases) of
+        problem i."""
         L, nev = self.problems[i]
         ev = np.empty(nev)
         V = np.empty((3 * L ** 3, nev), dtype=np.complex128, order="F") if vectors else None

@@ -70,4 +70,5 @@ def test_reference_arm_per_core_layout():
     ln = lines[0]
     cb = ln["cpu_baseline"]
     assert ln["impl"] == "reference" and ln["value"] > 0 and cb["layout"] == "one timeslice per core"
-    assert cb["cores"] == (os.cpu_count() or 1) and abs(ln["ms_per_step"] * ln["value"] / 1000.0 - cb["cores"]) < 1e-6 * cb["cores"]
+    assert cb["cores"] == (os.cpu_count() or 1)
+    assert abs(ln["ms_per_step"] * ln["value"] / 1000.0 - cb["cores"]) < 1e-6 * cb["cores"]

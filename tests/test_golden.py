@@ -52,7 +52,8 @@ def test_cuda_path_reproduces_fixtures(gpu):
     assert np.linalg.norm(y - g["tv_iter_deg8_hyp"]) / np.linalg.norm(g["tv_iter_deg8_hyp"]) <= 1e-13
     assert abs(ctx.plaquette() - float(g["plaquette_hyp"])) < 1e-13
     ctx.close()
-    s = gpu.Solver([(L, 20)], guard=16, tol=1e-10, deg=8, max_it=300, smear_kind=gpu.SMEAR_HYP, smear_p1=0.62, smear_p2=0.52,
+    s = gpu.Solver([(L, 20)], guard=16, tol=1e-10, deg=8, max_it=300, smear_kind=gpu.SMEAR_HYP, smear_p1=0.62,
+                   smear_p2=0.52,
                    smear_iters=3, link_prec=gpu.LINKS_FP32)
     s.set_links(0, U)
     st, res = s.run()

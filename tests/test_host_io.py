@@ -286,8 +286,8 @@ def test_lime_reader_fuzz_matches_reference_restatement(tmp_path, orc):
             n = int(rng.choice([n_pay - 8, n_pay + 8, n_pay // 2, 2 * n_pay, n_pay - 1]))
             b[i_bin + 8:i_bin + 16] = n.to_bytes(8, "big")
         elif kind == 3:  # an extra record of another type first
-            b = bytearray(_lime_record("xlf-info", bytes(rng.integers(0, 256, int(rng.integers(0, 40)), dtype=np.uint8)),
-                                       me=False)) + b
+            junk = bytes(rng.integers(0, 256, int(rng.integers(0, 40)), dtype=np.uint8))
+            b = bytearray(_lime_record("xlf-info", junk, me=False)) + b
         elif kind == 4:  # junk after the last record
             b = b + bytes(rng.integers(0, 256, int(rng.integers(1, 300)), dtype=np.uint8))
         elif kind == 5:  # a second, different binary record after the first: the first one counts

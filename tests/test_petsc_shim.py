@@ -59,7 +59,8 @@ def _shim_solve(orc, U, L, nev, deg, lam_l, lam_c, tol):
         assert shim.EPSGetEigenpair(eps, i, eig, None, xr, xi) == 0
         p = c_vp()
         shim.VecGetArray(xr, ctypes.byref(p))
-        v = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), (2 * dim,)).view(np.complex128).copy()
+        v = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), (2 * dim,))
+        v = v.view(np.complex128).copy()
         lam = np.vdot(v, A @ v).real / np.vdot(v, v).real
         rq.append(lam)
         res.append(np.linalg.norm(A @ v - lam * v) / np.linalg.norm(v))

@@ -381,7 +381,8 @@ def test_reference_shipped_parameters_file(tmp_path):
     c = lb.parse_parameters(p)
     assert (c["LT"], c["LX"], c["NEV"], c["iter"], c["DEG"], c["OMP_THRDS"]) == (r["LT"], r["LX"], r["NEV"], r["iter"],
                                                                                  r["DEG"], r["OMP_THRDS"])
-    for k, rk in (("alpha_1", "alpha_1"), ("alpha_2", "alpha_2"), ("alpha_1_i", "alpha_1_i"), ("alpha_1_f", "alpha_1_f"),
+    for k, rk in (("alpha_1", "alpha_1"), ("alpha_2", "alpha_2"), ("alpha_1_i", "alpha_1_i"),
+                  ("alpha_1_f", "alpha_1_f"),
                   ("alpha_2_i", "alpha_2_i"), ("alpha_2_f", "alpha_2_f"), ("LAM_L", "lambda_l"), ("LAM_C", "lambda_c")):
         assert c[k] == r[rk], k
     assert (c["config_path"], c["result_path"], c["in_path"]) == (r["conf"], r["res"], r["in_path"])
