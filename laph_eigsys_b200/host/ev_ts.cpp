@@ -11,9 +11,9 @@
 //            fit in the device's free memory (laph_solver_max_batch), same
 //            outputs.
 // Timeslices are split across processes as the reference splits them across
-// MPI ranks (src/ev_ts.cpp:103-119): with LAPH_RANK / LAPH_WORLD_SIZE (or
-// RANK / WORLD_SIZE) set, rank r gets a contiguous block, the first LT % size
-// ranks one extra.  One JSON line per timeslice goes to stdout.
+// MPI ranks (src/ev_ts.cpp:103-119): with the rank and size of the launcher
+// (LAPH_RANK / LAPH_WORLD_SIZE, torchrun, mpirun, srun) rank r gets a
+// contiguous block, the first LT % size ranks one extra.  One JSON line per timeslice goes to stdout.
 // Beyond the reference: FP32 ILDG input is read (widened to FP64), and
 // --resume skips timeslices whose three output files are already complete
 // (right sizes, eigenvectors passing check_trace).
@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -42,10 +43,14 @@ void usage() {
                "  window, solver, autotune)\n");
 }
 
-int env_int(const char* a, const char* b, int def) {
-  const char* v = std::getenv(a);
-  if (!v) v = std::getenv(b);
-  return v ? std::atoi(v) : def;
+// The first of the named environment variables that is set, as an int: this
+// library's own name, then torchrun's, Open MPI's, MPICH / Intel MPI's
+// (PMI) and Slurm's, so that the launchers the reference is run with
+// (mpirun, srun) give each process its rank and device.
+int env_int(std::initializer_list<const char*> names, int def) {
+  for (const char* n : names)
+    if (const char* v = std::getenv(n)) return std::atoi(v);
+  return def;
 }
 
 int die(int st, const char* what) {
@@ -148,7 +153,8 @@ int main(int argc, char** argv) {
   if (P.OMP_THRDS > 0) omp_set_num_threads(P.OMP_THRDS);
   const int L = P.LX, LT = P.LT, nev = P.NEV;
   const int V3 = L * L * L, dim = 3 * V3;
-  const int size = env_int("LAPH_WORLD_SIZE", "WORLD_SIZE", 1), rank = env_int("LAPH_RANK", "RANK", 0);
+  const int size = env_int({"LAPH_WORLD_SIZE", "WORLD_SIZE", "OMPI_COMM_WORLD_SIZE", "PMI_SIZE", "SLURM_NTASKS"}, 1);
+  const int rank = env_int({"LAPH_RANK", "RANK", "OMPI_COMM_WORLD_RANK", "PMI_RANK", "SLURM_PROCID"}, 0);
   if (rank == 0) {
     print_summary(P);
     std::printf("calculating config %d\n", config);
@@ -156,7 +162,8 @@ int main(int argc, char** argv) {
   int t0, ntodo;
   st = laph_timeslice_split(LT, size, rank, &t0, &ntodo);
   if (st != LAPH_OK) return die(st, "timeslice split");
-  const int device = env_int("LAPH_DEVICE", "LOCAL_RANK", 0);
+  const int device =
+      env_int({"LAPH_DEVICE", "LOCAL_RANK", "OMPI_COMM_WORLD_LOCAL_RANK", "MPI_LOCALRANKID", "SLURM_LOCALID"}, 0);
   char conf_name[1100];
   std::snprintf(conf_name, sizeof conf_name, "%s/conf.%04d", P.config_path, config);
   std::vector<double> conf((size_t)std::max(ntodo, 1) * V3 * 72);

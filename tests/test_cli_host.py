@@ -16,9 +16,15 @@ EV_TS = os.path.join(ROOT, "laph_eigsys_b200", "laph_ev_ts")
 TUNE = os.path.join(ROOT, "laph_eigsys_b200", "laph_tune_hyp")
 
 
+# rank / size / device variables of the launchers laph_ev_ts understands
+LAUNCHER_VARS = ("LAPH_RANK", "LAPH_WORLD_SIZE", "LAPH_DEVICE", "RANK", "WORLD_SIZE", "LOCAL_RANK",
+                 "OMPI_COMM_WORLD_RANK", "OMPI_COMM_WORLD_SIZE", "OMPI_COMM_WORLD_LOCAL_RANK", "PMI_RANK", "PMI_SIZE",
+                 "MPI_LOCALRANKID", "SLURM_PROCID", "SLURM_NTASKS", "SLURM_LOCALID")
+
+
 def _run(exe, args, cwd, env=None):
     e = dict(os.environ)
-    for k in ("LAPH_RANK", "LAPH_WORLD_SIZE", "RANK", "WORLD_SIZE"):
+    for k in LAUNCHER_VARS:
         e.pop(k, None)
     e.update(env or {})
     return subprocess.run([exe] + args, cwd=cwd, capture_output=True, text=True, timeout=120, env=e)
@@ -84,10 +90,17 @@ def test_ev_ts_resume_over_complete_outputs_needs_no_solve(tmp_path):
     skipped = [ln for ln in r.stdout.splitlines() if '"skipped"' in ln]
     assert [int(ln.split(":")[1].split(",")[0]) for ln in skipped] == list(range(T))
     assert {p.name: p.read_bytes() for p in out.iterdir()} == before
-    # the reference's MPI split: rank 1 of 2 owns timeslices 3, 4 (rank 0 takes the extra one)
-    r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path, {"LAPH_WORLD_SIZE": "2", "LAPH_RANK": "1"})
-    assert r.returncode == 0, r.stderr
-    assert [ln for ln in r.stdout.splitlines() if '"skipped"' in ln] == skipped[3:]
+    # the reference's MPI split: rank 1 of 2 owns timeslices 3, 4 (rank 0 takes the extra one), whichever
+    # launcher sets the rank and size
+    for env in ({"LAPH_WORLD_SIZE": "2", "LAPH_RANK": "1"}, {"WORLD_SIZE": "2", "RANK": "1"},
+                {"OMPI_COMM_WORLD_SIZE": "2", "OMPI_COMM_WORLD_RANK": "1"}, {"PMI_SIZE": "2", "PMI_RANK": "1"},
+                {"SLURM_NTASKS": "2", "SLURM_PROCID": "1"}):
+        r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path, env)
+        assert r.returncode == 0, r.stderr
+        assert [ln for ln in r.stdout.splitlines() if '"skipped"' in ln] == skipped[3:], env
+    # rank 0 of 3 under srun: timeslices 0, 1
+    r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path, {"SLURM_NTASKS": "3", "SLURM_PROCID": "0"})
+    assert [ln for ln in r.stdout.splitlines() if '"skipped"' in ln] == skipped[:2]
 
 
 @pytest.mark.parametrize("damage", ["short_phases", "bad_trace", "missing_eigenvalues"])

@@ -13,6 +13,11 @@ import laph_eigsys_b200 as lb
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EXE = os.path.join(ROOT, "laph_eigsys_b200", "laph_ev_ts")
+# one process, device 0: no launcher's rank, size or device variables reach the programs
+ENV = {k: v for k, v in os.environ.items()
+       if k not in ("LAPH_RANK", "LAPH_WORLD_SIZE", "LAPH_DEVICE", "RANK", "WORLD_SIZE", "LOCAL_RANK",
+                    "OMPI_COMM_WORLD_RANK", "OMPI_COMM_WORLD_SIZE", "OMPI_COMM_WORLD_LOCAL_RANK", "PMI_RANK",
+                    "PMI_SIZE", "MPI_LOCALRANKID", "SLURM_PROCID", "SLURM_NTASKS", "SLURM_LOCALID")}
 
 
 @pytest.mark.parametrize("solver", ["block", "plain"])
@@ -34,7 +39,7 @@ def test_ev_ts_cli(gpu, orc, tmp_path, solver):
         f"config_path = {gdir}\nresult_path = {out}\nLT = {T}\nLX = {L}\nNEV = {nev}\n"
         f"alpha_1 = 0.62\nalpha_2 = 0.52\niter = 2\nLAM_L = 12.0\nLAM_C = {lam_c}\nDEG = 8\nOMP_THRDS = 2\n"
         f"tol = 1e-11\nsolver = {solver}\n")
-    r = subprocess.run([EXE, "--conf", str(cfgno)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    r = subprocess.run([EXE, "--conf", str(cfgno)], cwd=tmp_path, capture_output=True, text=True, timeout=600, env=ENV)
     assert r.returncode == 0, r.stderr
     assert len([ln for ln in r.stdout.splitlines() if ln.startswith("{")]) == T
     for t in range(T):
@@ -66,7 +71,7 @@ def test_ev_ts_cli_fp32_input_and_resume(gpu, orc, tmp_path):
         f"config_path = {gdir}\nresult_path = {out}\nLT = {T}\nLX = {L}\nNEV = {nev}\n"
         f"alpha_1 = 0.62\nalpha_2 = 0.52\niter = 2\nLAM_L = 12.0\nLAM_C = 1.0\nDEG = 8\nOMP_THRDS = 2\n"
         f"tol = 1e-11\nsolver = block\n")
-    r = subprocess.run([EXE, "--conf", str(cfgno)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    r = subprocess.run([EXE, "--conf", str(cfgno)], cwd=tmp_path, capture_output=True, text=True, timeout=600, env=ENV)
     assert r.returncode == 0, r.stderr
     assert "single-precision" in r.stdout
     for t in range(T):
@@ -75,7 +80,7 @@ def test_ev_ts_cli_fp32_input_and_resume(gpu, orc, tmp_path):
     before = lb.read_eigenvalues_bin(out, "eigenvalues", cfgno, 1, nev)
     # damage timeslice 1's phases file; resume must redo exactly that timeslice
     (out / f"phases.{cfgno:04d}.001").write_bytes(b"\0" * 8)
-    r = subprocess.run([EXE, "--conf", str(cfgno), "--resume"], cwd=tmp_path, capture_output=True, text=True,
+    r = subprocess.run([EXE, "--conf", str(cfgno), "--resume"], cwd=tmp_path, capture_output=True, text=True, env=ENV,
                        timeout=600)
     assert r.returncode == 0, r.stderr
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
@@ -103,7 +108,7 @@ def test_sourceshape_cli(gpu, orc, tmp_path, weighted):
     lb.write_eigenvalues_bin(ind, "eigenvalues", cfgno, t, ev)
     exe = os.path.join(ROOT, "laph_eigsys_b200", "laph_sourceshape")
     args = (["--weighted"] if weighted else []) + [str(cfgno), str(t), str(nev)]
-    r = subprocess.run([exe] + args, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    r = subprocess.run([exe] + args, cwd=tmp_path, capture_output=True, text=True, timeout=300, env=ENV)
     assert r.returncode == 0, r.stderr
     Vw = Q * np.sqrt(np.abs(ev))[None, :] if weighted else Q
     rr, aa = orc.sourceshape_avg(L, orc.sourceshape(Vw, L))
