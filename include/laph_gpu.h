@@ -169,7 +169,8 @@ typedef struct {
   int window;           /* LAPH_WINDOW_*                                          */
   double lam_cut;       /* fixed window: cut (<= 0: from the first Rayleigh-Ritz) */
   double lam_max;       /* fixed window: upper end (<= 0: Lanczos bound)          */
-  int deg;              /* filter degree (<= 0: default)                          */
+  int deg;              /* filter degree cap, 2..64 (default 16; 48-60 measured
+                           best at 24^3-48^3; laph_solver_autotune picks it)     */
   int phase_fix;        /* apply fix_phase to the output eigenvectors             */
   uint64_t seed;        /* start block                                            */
   int block;            /* columns per CTA of the filter kernel, 8..64 (0: 32)     */
