@@ -173,7 +173,8 @@ typedef struct {
                            best at 24^3-48^3; laph_solver_autotune picks it)     */
   int phase_fix;        /* apply fix_phase to the output eigenvectors             */
   uint64_t seed;        /* start block                                            */
-  int block;            /* columns per CTA of the filter kernel, 8..64 (0: 32)     */
+  int block;            /* columns per CTA of the filter kernel, 1..512 (0: 32);
+                           above 64 the filter runs as variant 0               */
   int filter_kernel;    /* filter variant, both with register-resident links and L2
                            bulk prefetch: 0 FP64 coefficients per thread; 1 FP32
                            coefficients staged per CTA (default; block <= 64)    */
