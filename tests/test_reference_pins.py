@@ -386,3 +386,28 @@ def test_reference_shipped_parameters_file(tmp_path):
                   ("alpha_2_i", "alpha_2_i"), ("alpha_2_f", "alpha_2_f"), ("LAM_L", "lambda_l"), ("LAM_C", "lambda_c")):
         assert c[k] == r[rk], k
     assert (c["config_path"], c["result_path"], c["in_path"]) == (r["conf"], r["res"], r["in_path"])
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_oracle_plaquette_uses_reference_lookup_tables(tmp_path, orc, L):
+    """plaque_timeslice / get_plaque_nx_ny (modules/config_utils.cpp:388-426) with the reference's iup / idown:
+    the mean over sites and ordered direction pairs x != y of Re tr(U_x(i) U_y(i+x) U_x(i+y)^dag U_y(i)^dag) / 3
+    (l = idown[iup[iup[i][x]][y]][x] = i + y), against the oracle."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    U = lb.gauge_random(L, 1, 0.6, 53)[0, :, 1:4]
+    dag = lambda m: np.conj(np.swapaxes(m, -1, -2))  # noqa: E731
+    tot, cnt = 0.0, 0
+    for x in range(3):
+        for y in range(3):
+            if x == y:
+                continue
+            j = up[:, x]
+            k = up[j, y]
+            l_ = dn[k, x]
+            P = U[:, x] @ (U[j, y] @ (dag(U[l_, x]) @ dag(U[:, y])))
+            tot += np.trace(P, axis1=1, axis2=2).real.sum() / 3.0
+            cnt += L ** 3
+    assert abs(orc.plaquette(U, L) - tot / cnt) < 1e-14
