@@ -411,3 +411,25 @@ def test_oracle_plaquette_uses_reference_lookup_tables(tmp_path, orc, L):
             tot += np.trace(P, axis1=1, axis2=2).real.sum() / 3.0
             cnt += L ** 3
     assert abs(orc.plaquette(U, L) - tot / cnt) < 1e-14
+
+
+@pytest.mark.parametrize("L", [3, 4])
+def test_oracle_assembled_operator_is_buildlaplacian(tmp_path, orc, L):
+    """BuildLaplacian (modules/config_utils.cpp:18-58) with the reference's get_up / get_dn on random links:
+    6 on the diagonal, -U_mu(i)(a, b) at (3i + a, 3 up + b), -U_mu(down)^dag(a, b) at (3i + a, 3 down + b), with
+    its INSERT_VALUES (for L >= 3 no entry is set twice) -- the oracle's dense -Delta used by every spectrum test."""
+    p = tmp_path / "parameters.txt"
+    p.write_text(f"LT = 4\nLX = {L}\nNEV = 4\n")
+    nav = ref("nav", p)
+    up, dn = np.array(nav["up"]), np.array(nav["dn"])
+    V3 = L ** 3
+    U = lb.gauge_random(L, 1, 0.5, 59)[0, :, 1:4]
+    A = np.zeros((3 * V3, 3 * V3), dtype=np.complex128)
+    for i in range(V3):
+        for c in range(3):
+            A[3 * i + c, 3 * i + c] = 6.0
+        for mu in range(3):
+            u, d = up[i, mu], dn[i, mu]
+            A[3 * i:3 * i + 3, 3 * u:3 * u + 3] = -U[i, mu]
+            A[3 * i:3 * i + 3, 3 * d:3 * d + 3] = -U[d, mu].conj().T
+    assert np.abs(orc.neglap_dense(U, L) - A).max() < 1e-15
