@@ -396,3 +396,14 @@ def test_fp32_reader_refuses_truncated_record(tmp_path):
     with pytest.raises(lb.LaphError) as e:
         lb.lime_read_gauge_any(p, T, L, 0, 0)  # the first timeslice is all there, the record is not
     assert e.value.status == _lib.LAPH_EIO
+
+
+def test_recover_spectrum_transcribes_reference():
+    """invert_Tn then invert_B (modules/recover_spec.cpp:13-30, applied in recover_spectrum :45-54):
+    b = cosh(acosh(theta) / DEG), lambda_stored = (LAM_L - LAM_C) (b - 1) / 2 - LAM_C."""
+    theta = np.array([1e6, 123.4, 2.5, 1.0 + 1e-9])
+    for deg, lam_l, lam_c in ((8, 11.8, 0.6), (12, 12.0, 0.65), (3, 10.0, 1.5)):
+        b = np.cosh(np.arccosh(theta) / deg)
+        want = (lam_l - lam_c) * (b - 1) * 0.5 - lam_c
+        got = lb.recover_spectrum(theta, deg, lam_l, lam_c)
+        assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
