@@ -50,6 +50,9 @@ enum {
 const char* laph_strerror(int status);
 const char* laph_last_error(void);
 int laph_version(void);
+/* The device architecture the library's kernels were built for, as the CUDA
+ * runtime reports it (cudaFuncAttributes::binaryVersion: 100 = sm_100a). */
+int laph_binary_version(int* version);
 
 /* ---- link layouts accepted at the boundary -------------------------------- */
 enum {
@@ -78,6 +81,9 @@ typedef struct {
 int laph_ctx_create(laph_ctx** ctx, const laph_params* p);
 int laph_ctx_destroy(laph_ctx* ctx);
 int laph_ctx_set_window(laph_ctx* ctx, double lam_l, double lam_c, int deg);
+/* The context's CUDA stream (a cudaStream_t): every device call of the
+ * context runs on it, so callers can time the products with their own events. */
+int laph_ctx_stream(laph_ctx* ctx, void** stream);
 
 /* Load one timeslice of links (host pointer, FP64).  Replaces
  * Tslice::map_timeslice_to_eigen (modules/timeslice.cpp:34-79) for
@@ -97,20 +103,22 @@ int laph_smear(laph_ctx* ctx, int kind, double p1, double p2, int iters, int com
 /* y = T_deg(B) x in FP64, B = c(hop - 6) + a, c = 2/(LAM_L - LAM_C),
  * a = 1 + c LAM_C: the body of MatMult_Laplacian2D (shell_matop.cpp:136-168,
  * :226-244).  deg >= 1 (deg = 1 gives B x).  x, y: complex128[3*V3];
- * on_device = 0 for host pointers (staged), 1 for device pointers. */
+ * on_device = 0 for host pointers (staged), 1 for device pointers, which must
+ * not overlap (LAPH_EINVAL).  The whole recurrence is one cooperative launch. */
 int laph_matmult(laph_ctx* ctx, const double* x, double* y, int deg, int on_device);
 /* laph_matmult_noalloc: the same y = T_deg(B) x in FP64 without any device
- * allocation, for callers that cannot call cudaMalloc (inside another
- * library's stream capture, under a framework that owns the device memory
- * budget, or after a service's start-up).  No counterpart in the reference.
+ * allocation, for callers that may not call cudaMalloc where they need the
+ * product (a framework that owns the device memory budget through its own
+ * pool, a service that allocates only at start-up, a loop that cannot take
+ * cudaMalloc's implicit synchronisation).  No counterpart in the reference.
  * links: device pointer, LAPH_LAYOUT_ROWMAJOR, one timeslice of L^3 sites;
- * x, y: device pointers, complex128[3*L^3]; work is queued on `stream`
- * (a cudaStream_t, 0 = legacy default) and the call returns without waiting.
- * The two Chebyshev temporaries live in a fixed file-scope device array of
- * 3 MiB that holds timeslices up to L = 32; larger L returns LAPH_EINVAL.
- * The first call on each device resolves that array's address (make it
- * before any stream capture).  Calls that overlap on the GPU share the array
- * and race: serialise them on one stream. */
+ * x, y: device pointers, complex128[3*L^3], not overlapping (LAPH_EINVAL);
+ * work is queued on `stream` (a cudaStream_t, 0 = legacy default) and the
+ * call returns without waiting.  The two Chebyshev temporaries live in a
+ * fixed file-scope device array of 3 MiB that holds timeslices up to L = 32;
+ * larger L returns LAPH_EINVAL.  The first call in each CUDA context resolves
+ * that array's address (make it before any stream capture).  Calls that
+ * overlap on the GPU share the array and race: serialise them on one stream. */
 int laph_matmult_noalloc(const double* links, int L, double lam_l, double lam_c, int deg, const double* x,
                          double* y, void* stream);
 /* y = (-Delta) x = 6x - hop(x) in FP64 (for residuals). */

@@ -273,6 +273,12 @@ class Context:
         check(lib.laph_matmult(self._h, _ptr(x), _ptr(y), self.deg if deg is None else deg, 0), "laph_matmult")
         return y
 
+    def stream(self):
+        """The context's CUDA stream handle (laph_ctx_stream), for timing its products with events."""
+        h = ctypes.c_void_p()
+        check(lib.laph_ctx_stream(self._h, ctypes.byref(h)), "laph_ctx_stream")
+        return h.value or 0
+
     def matmult_device(self, x_ptr, y_ptr, deg=None):
         """As matmult on device pointers (complex128[3 V3] each)."""
         check(lib.laph_matmult(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),

@@ -21,6 +21,8 @@ struct laph_ctx {
   double2* vec = nullptr;   // 4 vectors of dim: x, y, tmp0, tmp1
   double2* h_stage = nullptr;  // pinned staging, 2 vectors
   double* d_scalar = nullptr;
+  laph::GridBar* bar = nullptr;  // grid barrier of the fused MatMult
+  int* h_err = nullptr;          // pinned: that barrier's error flag after a product
 };
 
 using namespace laph;
@@ -91,6 +93,8 @@ int laph_ctx_create(laph_ctx** out, const laph_params* p) {
       cudaMalloc(&c->dec, sizeof(double2) * 54 * V3) != cudaSuccess ||
       cudaMalloc(&c->vec, sizeof(double2) * 4 * dim) != cudaSuccess ||
       cudaMalloc(&c->d_scalar, sizeof(double) * 64) != cudaSuccess ||
+      cudaMalloc(&c->bar, sizeof(GridBar)) != cudaSuccess || cudaMemset(c->bar, 0, sizeof(GridBar)) != cudaSuccess ||
+      cudaMallocHost(&c->h_err, sizeof(int)) != cudaSuccess ||
       cudaMallocHost(&c->h_stage, sizeof(double2) * 2 * dim) != cudaSuccess) {
     cudaGetLastError();
     set_error("laph_ctx_create: allocation failed for L=%d", p->L);
@@ -118,9 +122,20 @@ int laph_ctx_destroy(laph_ctx* c) {
   cudaFree(c->dec);
   cudaFree(c->vec);
   cudaFree(c->d_scalar);
+  cudaFree(c->bar);
+  if (c->h_err) cudaFreeHost(c->h_err);
   if (c->h_stage) cudaFreeHost(c->h_stage);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
+  return LAPH_OK;
+}
+
+int laph_ctx_stream(laph_ctx* c, void** stream) {
+  if (!c || !stream) {
+    set_error("laph_ctx_stream: bad argument");
+    return LAPH_EINVAL;
+  }
+  *stream = static_cast<void*>(c->st);
   return LAPH_OK;
 }
 
@@ -210,11 +225,24 @@ int laph_matmult(laph_ctx* c, const double* x, double* y, int deg, int on_device
     return LAPH_EINVAL;
   }
   const size_t dim = 3 * (size_t)c->g.V3;
+  if (on_device && ranges_overlap(x, y, sizeof(double2) * dim)) {
+    set_error("laph_matmult: x and y overlap (the product reads x while it writes y)");
+    return LAPH_EINVAL;
+  }
   const double2* dx;
   LAPH_TRY(stage_in(c, x, on_device, &dx));
   double2* dy = on_device ? reinterpret_cast<double2*>(y) : c->vec + dim;
-  LAPH_TRY(cheb64(c->U, c->g.L, c->lam_l, c->lam_c, deg, dx, dy, c->vec + 2 * dim, dim, 1, c->st));
-  return stage_out(c, y, on_device);
+  // the whole recurrence in one launch (tv_iter, shell_matop.cpp:136-168)
+  LAPH_TRY(cheb64_fused(c->U, c->g.L, c->lam_l, c->lam_c, deg, dx, dy, c->vec + 2 * dim, dim, c->bar, c->st));
+  LAPH_CUDA_TRY(cudaMemcpyAsync(c->h_err, &c->bar->err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  LAPH_TRY(stage_out(c, y, on_device));
+  if (*c->h_err) {
+    cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->st);
+    cudaStreamSynchronize(c->st);
+    set_error("laph_matmult: a grid barrier of the fused product gave up waiting; y is not valid");
+    return LAPH_ECUDA;
+  }
+  return LAPH_OK;
 }
 
 int laph_apply_neglap(laph_ctx* c, const double* x, double* y, int on_device) {
@@ -224,6 +252,10 @@ int laph_apply_neglap(laph_ctx* c, const double* x, double* y, int on_device) {
     return LAPH_EINVAL;
   }
   const size_t dim = 3 * (size_t)c->g.V3;
+  if (on_device && ranges_overlap(x, y, sizeof(double2) * dim)) {
+    set_error("laph_apply_neglap: x and y overlap (the stencil reads x while it writes y)");
+    return LAPH_EINVAL;
+  }
   const double2* dx;
   LAPH_TRY(stage_in(c, x, on_device, &dx));
   double2* dy = on_device ? reinterpret_cast<double2*>(y) : c->vec + dim;

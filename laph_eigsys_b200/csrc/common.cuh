@@ -119,4 +119,10 @@ inline Lat make_lat(int L) { return Lat{L, L * L, L * L * L}; }
 
 inline unsigned ceil_div(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
+// [a, a + bytes) and [b, b + bytes) share a byte
+inline bool ranges_overlap(const void* a, const void* b, size_t bytes) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + bytes && y < x + bytes;
+}
+
 }  // namespace laph

@@ -285,6 +285,7 @@ struct DeviceBasis : Basis {
   cudaStream_t st = nullptr;
   cublasHandle_t hb = nullptr;
   double2 *V = nullptr, *w = nullptr, *tmp = nullptr, *h = nullptr, *Zd = nullptr;
+  GridBar* bar = nullptr;  // grid barrier of the fused T_deg(B) product
   int ok = 0;
   DeviceBasis(laph_ctx* c, long dim, int m) : ctx(c) {
     n = dim;
@@ -293,7 +294,8 @@ struct DeviceBasis : Basis {
     if (ctx_device_links(ctx, &U, &L, &lam_l, &lam_c, &dg, &st, &dev) != LAPH_OK) return;
     if (cudaMalloc(&V, sizeof(double2) * n * (cap + 1)) != cudaSuccess || cudaMalloc(&w, sizeof(double2) * n) != cudaSuccess ||
         cudaMalloc(&tmp, sizeof(double2) * n * 2) != cudaSuccess || cudaMalloc(&h, sizeof(double2) * 2 * cap) != cudaSuccess ||
-        cudaMalloc(&Zd, sizeof(double2) * cap * cap) != cudaSuccess) {
+        cudaMalloc(&Zd, sizeof(double2) * cap * cap) != cudaSuccess || cudaMalloc(&bar, sizeof(GridBar)) != cudaSuccess ||
+        cudaMemset(bar, 0, sizeof(GridBar)) != cudaSuccess) {
       cudaGetLastError();
       return;
     }
@@ -308,6 +310,13 @@ struct DeviceBasis : Basis {
     cudaFree(tmp);
     cudaFree(h);
     cudaFree(Zd);
+    cudaFree(bar);
+  }
+  // nonzero if a grid barrier of any product so far gave up (sticky)
+  int barrier_failed() {
+    int e = 0;
+    if (cudaMemcpy(&e, &bar->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+    return e;
   }
   double2* col(int j) { return V + (size_t)j * n; }
   int start(const std::vector<cd>& v0) override {
@@ -316,7 +325,7 @@ struct DeviceBasis : Basis {
   }
   int op(int j) override {
     ++nmatvec;
-    return cheb64(U, L, lam_l, lam_c, deg, col(j), w, tmp, n, 1, st);
+    return cheb64_fused(U, L, lam_l, lam_c, deg, col(j), w, tmp, n, bar, st);
   }
   int orth(int j, std::vector<cd>& hh, double* beta) override {
     const cuDoubleComplex one = {1.0, 0.0}, zero = {0.0, 0.0}, mone = {-1.0, 0.0};
@@ -492,7 +501,11 @@ extern "C" int laph_eps_solve(laph_ctx* ctx, int nev, int ncv, double tol, int m
   } else {
     B = new HostBasis(ctx, dim, m, deg);
   }
-  const int rc = krylov_schur(B, dim, nev, m, tol, max_it, seed, theta_out, V_out, nconv_out, its_out, nmatvec_out);
+  int rc = krylov_schur(B, dim, nev, m, tol, max_it, seed, theta_out, V_out, nconv_out, its_out, nmatvec_out);
+  if (device_basis && static_cast<DeviceBasis*>(B)->barrier_failed()) {
+    set_error("laph_eps_solve: a grid barrier of the fused product gave up waiting; the result is not valid");
+    rc = LAPH_ECUDA;
+  }
   delete B;
   return rc;
 }

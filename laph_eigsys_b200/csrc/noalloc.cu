@@ -1,29 +1,36 @@
 // noalloc.cu -- laph_matmult_noalloc: the FP64 MatShell product
 // y = T_deg(B) x for callers that must not allocate device memory.
 //
-// Who needs it: code that runs where cudaMalloc is off limits -- inside
-// another library's stream capture (a cudaMalloc there breaks the capture),
-// under a host framework that owns the whole device memory budget through its
-// own pool, or in a long-running service that forbids allocation after
-// start-up.  Such a caller owns its links, x and y on the device and only
-// needs somewhere to keep the two Chebyshev temporaries of tv_iter
+// Who needs it: callers that cannot call cudaMalloc at the point where they
+// need the product -- a host framework that owns the whole device memory
+// budget through its own pool and forbids other allocations, a long-running
+// service that allocates only at start-up, or a real-time loop that cannot
+// afford the implicit synchronisation of cudaMalloc / cudaFree.  Such a
+// caller owns its links, x and y on the device and only needs somewhere to
+// keep the two Chebyshev temporaries of tv_iter
 // (modules/shell_matop.cpp:136-168).
 //
 // Those temporaries live in g_noalloc_scratch below: a file-scope device
 // array sized for timeslices up to kNoAllocMaxL^3 (3 MiB).  Every GPU that
 // loads this library keeps that array until the process exits.  Host code
 // cannot pass g_noalloc_scratch to a kernel directly (on the host the name is
-// only a stand-in, not a device address), so the first call on each device
-// looks the address up with cudaGetSymbolAddress while that device is
-// current, checks it, and caches it.  Make that first call before any stream
-// capture begins.
+// only a stand-in, not a device address), so the first call in each CUDA
+// context looks the address up with cudaGetSymbolAddress while that context
+// is current, checks it, and caches it under the context's unique ID
+// (cuCtxGetId: never reused in a process, so a context created after
+// cudaDeviceReset or cuCtxDestroy gets a fresh lookup).  Make that first call
+// before any stream capture begins.
 //
 // Every call shares the one array and it keeps the previous call's contents.
 // Nothing in it has to start at zero: each Chebyshev step writes every
 // element of its output before any later step reads it.  Calls whose work
 // overlaps on the GPU (different streams, or different host threads, on the
 // same device) race on the array; serialise them on one stream.
+#include <cuda.h>
+
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 
@@ -31,26 +38,72 @@ namespace laph {
 
 constexpr int kNoAllocMaxL = 32;
 constexpr size_t kNoAllocMaxDim = 3ull * kNoAllocMaxL * kNoAllocMaxL * kNoAllocMaxL;
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double2 g_noalloc_scratch[2 * kNoAllocMaxDim];
 
 namespace {
-std::mutex g_noalloc_mu;
-double2* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+using CtxGetId = CUresult (*)(CUcontext, unsigned long long*);
 
-int noalloc_scratch(int dev, double2** out) {
+std::mutex g_noalloc_mu;
+std::vector<std::pair<unsigned long long, double2*>> g_noalloc_ptr;  // (context ID, scratch address)
+CtxGetCurrent g_get_current = nullptr;
+CtxGetId g_get_id = nullptr;
+
+// Unique ID of the calling thread's current context (0: none current).
+int current_ctx_id(unsigned long long* id) {
+  *id = 0;
+  CUcontext c = nullptr;
+  if (g_get_current(&c) != CUDA_SUCCESS) {
+    set_error("laph_matmult_noalloc: cuCtxGetCurrent failed");
+    return LAPH_ECUDA;
+  }
+  if (c && g_get_id(c, id) != CUDA_SUCCESS) {
+    set_error("laph_matmult_noalloc: cuCtxGetId failed");
+    return LAPH_ECUDA;
+  }
+  return LAPH_OK;
+}
+
+int noalloc_scratch(double2** out) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      set_error("laph_matmult_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(e));
+  if (!g_get_current || !g_get_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      cudaGetLastError();
+      set_error("laph_matmult_noalloc: the driver does not provide cuCtxGetCurrent / cuCtxGetId");
       return LAPH_ECUDA;
     }
-    g_noalloc_ptr[dev] = static_cast<double2*>(p);
+    g_get_current = reinterpret_cast<CtxGetCurrent>(f1);
+    g_get_id = reinterpret_cast<CtxGetId>(f2);
   }
-  *out = g_noalloc_ptr[dev];
+  unsigned long long id = 0;
+  LAPH_TRY(current_ctx_id(&id));
+  if (id != 0)
+    for (const auto& e : g_noalloc_ptr)
+      if (e.first == id) {
+        *out = e.second;
+        return LAPH_OK;
+      }
+  // first call in this context: resolve the array's device address (this also
+  // makes the device's primary context current if no context was)
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    cudaGetLastError();
+    set_error("laph_matmult_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+    return LAPH_ECUDA;
+  }
+  LAPH_TRY(current_ctx_id(&id));
+  if (id == 0) {
+    set_error("laph_matmult_noalloc: no CUDA context is current");
+    return LAPH_ECUDA;
+  }
+  g_noalloc_ptr.emplace_back(id, static_cast<double2*>(p));
+  *out = static_cast<double2*>(p);
   return LAPH_OK;
 }
 }  // namespace
@@ -112,14 +165,13 @@ extern "C" int laph_matmult_noalloc(const double* links, int L, double lam_l, do
     set_error("laph_matmult_noalloc: need deg >= 1 and lam_l > lam_c");
     return LAPH_EINVAL;
   }
-  int dev = -1;
-  LAPH_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocMaxDevices) {
-    set_error("laph_matmult_noalloc: device ordinal %d not supported", dev);
+  const size_t vbytes = sizeof(double2) * 3 * (size_t)L * L * L;
+  if (ranges_overlap(x, y, vbytes)) {
+    set_error("laph_matmult_noalloc: x and y overlap (the product reads x while it writes y)");
     return LAPH_EINVAL;
   }
   double2* scratch = nullptr;
-  LAPH_TRY(noalloc_scratch(dev, &scratch));
+  LAPH_TRY(noalloc_scratch(&scratch));
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   const Lat g = make_lat(L);
   const size_t dim = 3 * (size_t)g.V3;

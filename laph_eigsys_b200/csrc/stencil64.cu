@@ -11,6 +11,9 @@
 // block of ncol vectors is column-major with column stride ld.  One thread per
 // (site, column); consecutive threads take consecutive sites so every
 // 48-byte site vector and every link element is read coalesced.
+#include <algorithm>
+#include <mutex>
+
 #include "stencil64.cuh"
 #include "su3.cuh"
 
@@ -89,4 +92,220 @@ int cheb64(const double2* U, int L, double lam_l, double lam_c, int deg, const d
   return LAPH_OK;
 }
 
+
+// ------------------------------------------- fused T_deg(B) x, one launch ---
+// The plain form's MatMult in ONE cooperative launch: every thread keeps its
+// site for the whole recurrence, so the links are read from HBM once per
+// product (forward links in 108 registers, backward links U_mu(s - mu) in
+// shared memory, as the block stencils keep them) instead of once per step,
+// and the deg steps are separated by a grid barrier instead of kernel
+// boundaries.  At 32^3 the whole product (links 14 MB, three vectors of
+// 1.5 MB) then runs from L2.  The T_n written inside the launch are read
+// with ld.global.cg (L2, never a stale L1 line); only x, read-only for the
+// launch, goes through the non-coherent path.  Used when one site per thread
+// fits the device's co-resident CTAs (up to 296 CTAs of 128 sites on a
+// B200: L <= 33); otherwise a grid-stride variant reads the links per step.
+
+// Grid barrier with a bounded wait: a CTA that waits longer than
+// kBarSpinLimit polls sets `err` and every CTA leaves at its next barrier.
+// Cooperative launches guarantee co-residency, so the limit is a safety net.
+constexpr unsigned kBarSpinLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblk) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned gen = ld_acquire_gpu(&b->gen);
+    __threadfence();  // this CTA's writes before its arrival
+    if (atomicAdd(&b->count, 1u) == nblk - 1) {
+      atomicExch(&b->count, 0u);
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      unsigned it = 0;
+      while (ld_acquire_gpu(&b->gen) == gen) {
+        if (++it > kBarSpinLimit || *reinterpret_cast<volatile int*>(&b->err)) {
+          atomicExch(&b->err, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    s_ok = *reinterpret_cast<volatile int*>(&b->err) == 0;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+constexpr int kFusedSmem = 27 * 128 * (int)sizeof(double2);
+
+template <bool RESIDENT>
+__global__ void __launch_bounds__(128, 2)
+    k_cheb64_fused(const double2* __restrict__ U, Lat g, const double2* __restrict__ x, double2* y, double2* t0,
+                   double2* t1, int deg, double c, double a, GridBar* bar) {
+  extern __shared__ double2 s_ub[];  // [27][128] backward links (RESIDENT only)
+  double2 (*sUb)[128] = reinterpret_cast<double2 (*)[128]>(s_ub);
+  const unsigned nblk = gridDim.x;
+  // T_n lives in buffer (2 - (deg - n)) mod 3 of {t0, t1, y}: T_deg lands in y
+  auto buf = [=](int n) {
+    const int i = (((2 - (deg - n)) % 3) + 3) % 3;
+    return i == 0 ? t0 : (i == 1 ? t1 : y);
+  };
+  const double cd = a - 6.0 * c;
+  int s = blockIdx.x * 128 + threadIdx.x;
+  double2 uf[3][9];
+  int up[3], dn[3];
+  if (RESIDENT) {
+    if (s < g.V3) {
+      int sx, sy, sz;
+      site_xyz(g, s, sx, sy, sz);
+#pragma unroll
+      for (int mu = 0; mu < 3; ++mu) {
+        up[mu] = nb_up(g, sx, sy, sz, mu);
+        dn[mu] = nb_dn(g, sx, sy, sz, mu);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+          uf[mu][e] = __ldg(U + (size_t)(mu * 9 + e) * g.V3 + s);
+          sUb[mu * 9 + e][threadIdx.x] = __ldg(U + (size_t)(mu * 9 + e) * g.V3 + dn[mu]);
+        }
+      }
+    }
+  }
+  for (int n = 1; n <= deg; ++n) {
+    const double2* X = n == 1 ? x : buf(n - 1);
+    const double2* Z = n == 2 ? x : (n > 2 ? buf(n - 2) : nullptr);
+    double2* Y = buf(n);
+    const double ch = n == 1 ? c : 2.0 * c, cdiag = n == 1 ? cd : 2.0 * cd;
+    for (int si = s; si < g.V3; si += (RESIDENT ? g.V3 : (int)nblk * 128)) {
+      if (!RESIDENT) {
+        int sx, sy, sz;
+        site_xyz(g, si, sx, sy, sz);
+#pragma unroll
+        for (int mu = 0; mu < 3; ++mu) {
+          up[mu] = nb_up(g, sx, sy, sz, mu);
+          dn[mu] = nb_dn(g, sx, sy, sz, mu);
+        }
+      }
+      double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+#pragma unroll
+      for (int mu = 0; mu < 3; ++mu) {
+        double2 xu[3], xd[3];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          xu[b] = n == 1 ? __ldg(X + 3 * (size_t)up[mu] + b) : __ldcg(X + 3 * (size_t)up[mu] + b);
+          xd[b] = n == 1 ? __ldg(X + 3 * (size_t)dn[mu] + b) : __ldcg(X + 3 * (size_t)dn[mu] + b);
+        }
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            if (RESIDENT) {
+              cfma(acc[aa], uf[mu][3 * aa + b], xu[b]);
+              cfmac(acc[aa], sUb[mu * 9 + 3 * b + aa][threadIdx.x], xd[b]);
+            } else {
+              cfma(acc[aa], __ldg(U + (size_t)(mu * 9 + 3 * aa + b) * g.V3 + si), xu[b]);
+              cfmac(acc[aa], __ldg(U + (size_t)(mu * 9 + 3 * b + aa) * g.V3 + dn[mu]), xd[b]);
+            }
+          }
+      }
+#pragma unroll
+      for (int aa = 0; aa < 3; ++aa) {
+        const double2 xs = n == 1 ? __ldg(X + 3 * (size_t)si + aa) : __ldcg(X + 3 * (size_t)si + aa);
+        double2 r = make_double2(ch * acc[aa].x + cdiag * xs.x, ch * acc[aa].y + cdiag * xs.y);
+        if (Z) {
+          const double2 zz = n == 2 ? __ldg(Z + 3 * (size_t)si + aa) : __ldcg(Z + 3 * (size_t)si + aa);
+          r.x -= zz.x;
+          r.y -= zz.y;
+        }
+        __stcg(Y + 3 * (size_t)si + aa, r);
+      }
+    }
+    if (n < deg && !grid_barrier(bar, nblk)) return;
+  }
+}
+
+namespace {
+struct FusedOcc {
+  int sms = 0, res = 0, nonres = 0;
+};
+std::mutex g_fused_mu;
+FusedOcc g_fused_occ[64];
+
+int fused_occupancy(FusedOcc* out) {
+  int dev = 0;
+  LAPH_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("device ordinal %d not supported", dev);
+    return LAPH_EINVAL;
+  }
+  std::lock_guard<std::mutex> lk(g_fused_mu);
+  FusedOcc& o = g_fused_occ[dev];
+  if (o.sms == 0) {
+    LAPH_CUDA_TRY(cudaFuncSetAttribute(k_cheb64_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kFusedSmem));
+    LAPH_CUDA_TRY(cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev));
+    LAPH_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.res, k_cheb64_fused<true>, 128, kFusedSmem));
+    LAPH_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.nonres, k_cheb64_fused<false>, 128, 0));
+  }
+  *out = o;
+  return LAPH_OK;
+}
+}  // namespace
+
+int cheb64_fused(const double2* U, int L, double lam_l, double lam_c, int deg, const double2* x, double2* y,
+                 double2* tmp, size_t ld, GridBar* bar, cudaStream_t st) {
+  const double c = 2.0 / (lam_l - lam_c);
+  const double a = 1.0 + c * lam_c;
+  const Lat g = make_lat(L);
+  if (deg <= 1) return hop64(U, L, x, nullptr, y, ld, 1, c, a - 6.0 * c, 0.0, st);
+  FusedOcc o;
+  LAPH_TRY(fused_occupancy(&o));
+  const int need = (int)ceil_div(g.V3, 128);
+  const bool resident = need <= o.res * o.sms;
+  const int grid = resident ? need : std::max(1, std::min(need, o.nonres * o.sms));
+  if (grid < 1 || (!resident && o.nonres < 1)) {
+    set_error("cheb64_fused: no co-resident grid for L = %d", L);
+    return LAPH_ECUDA;
+  }
+  // count and generation back to zero; err is sticky until the owner reads it
+  LAPH_CUDA_TRY(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
+  double2* t0 = tmp;
+  double2* t1 = tmp + ld;
+  Lat gg = g;
+  void* args[] = {(void*)&U, (void*)&gg, (void*)&x, (void*)&y, (void*)&t0, (void*)&t1, (void*)&deg, (void*)&c,
+                  (void*)&a, (void*)&bar};
+  if (resident)
+    LAPH_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_cheb64_fused<true>, dim3(grid), dim3(128), args,
+                                              kFusedSmem, st));
+  else
+    LAPH_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_cheb64_fused<false>, dim3(grid), dim3(128), args, 0, st));
+  return LAPH_OK;
+}
+
 }  // namespace laph
+
+// The architecture the library's device code was built for, as the CUDA
+// runtime reports it for one of its kernels (cudaFuncAttributes::binaryVersion,
+// major * 10 + minor: 100 for sm_100a).
+extern "C" int laph_binary_version(int* version) {
+  if (!version) {
+    laph::set_error("laph_binary_version: null pointer");
+    return LAPH_EINVAL;
+  }
+  cudaFuncAttributes fa;
+  const cudaError_t e = cudaFuncGetAttributes(&fa, laph::k_hop64<false>);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    laph::set_error("laph_binary_version: %s", cudaGetErrorString(e));
+    return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? LAPH_ENODEV : LAPH_ECUDA;
+  }
+  *version = fa.binaryVersion;
+  return LAPH_OK;
+}

@@ -43,14 +43,41 @@ void usage() {
                "  window, solver, autotune)\n");
 }
 
-// The first of the named environment variables that is set, as an int: this
-// library's own name, then torchrun's, Open MPI's, MPICH / Intel MPI's
-// (PMI) and Slurm's, so that the launchers the reference is run with
-// (mpirun, srun) give each process its rank and device.
+// The first of the named environment variables that is set, as an int.
 int env_int(std::initializer_list<const char*> names, int def) {
   for (const char* n : names)
     if (const char* v = std::getenv(n)) return std::atoi(v);
   return def;
+}
+
+// Rank, size and node-local rank of this process, all three taken from ONE
+// launcher's variables: this program's own (LAPH_RANK / LAPH_WORLD_SIZE /
+// LAPH_DEVICE), torchrun's, Open MPI's, MPICH / Intel MPI's (PMI) or Slurm's,
+// the first launcher whose rank and size are both set.  Slurm counts only
+// inside an srun step (SLURM_STEP_ID set; size SLURM_STEP_NUM_TASKS): a plain
+// process in an sbatch allocation also sees SLURM_NTASKS / SLURM_PROCID, which
+// describe the allocation, not this run.  Without a launcher: rank 0 of 1.
+struct Launch {
+  const char* name;
+  int rank, size, local;
+};
+Launch launcher() {
+  struct Vars {
+    const char *name, *rank, *size, *local, *needs;
+  };
+  static const Vars kLaunchers[] = {
+      {"laph", "LAPH_RANK", "LAPH_WORLD_SIZE", "LAPH_DEVICE", nullptr},
+      {"torchrun", "RANK", "WORLD_SIZE", "LOCAL_RANK", nullptr},
+      {"openmpi", "OMPI_COMM_WORLD_RANK", "OMPI_COMM_WORLD_SIZE", "OMPI_COMM_WORLD_LOCAL_RANK", nullptr},
+      {"pmi", "PMI_RANK", "PMI_SIZE", "MPI_LOCALRANKID", nullptr},
+      {"srun", "SLURM_PROCID", "SLURM_STEP_NUM_TASKS", "SLURM_LOCALID", "SLURM_STEP_ID"},
+  };
+  for (const Vars& v : kLaunchers) {
+    if (!std::getenv(v.rank) || !std::getenv(v.size) || (v.needs && !std::getenv(v.needs))) continue;
+    // LAPH_DEVICE picks the GPU under any launcher
+    return Launch{v.name, env_int({v.rank}, 0), env_int({v.size}, 1), env_int({"LAPH_DEVICE", v.local}, 0)};
+  }
+  return Launch{"none", 0, 1, env_int({"LAPH_DEVICE"}, 0)};
 }
 
 int die(int st, const char* what) {
@@ -153,8 +180,8 @@ int main(int argc, char** argv) {
   if (P.OMP_THRDS > 0) omp_set_num_threads(P.OMP_THRDS);
   const int L = P.LX, LT = P.LT, nev = P.NEV;
   const int V3 = L * L * L, dim = 3 * V3;
-  const int size = env_int({"LAPH_WORLD_SIZE", "WORLD_SIZE", "OMPI_COMM_WORLD_SIZE", "PMI_SIZE", "SLURM_NTASKS"}, 1);
-  const int rank = env_int({"LAPH_RANK", "RANK", "OMPI_COMM_WORLD_RANK", "PMI_RANK", "SLURM_PROCID"}, 0);
+  const Launch ln = launcher();
+  const int size = ln.size, rank = ln.rank, device = ln.local;
   if (rank == 0) {
     print_summary(P);
     std::printf("calculating config %d\n", config);
@@ -162,8 +189,9 @@ int main(int argc, char** argv) {
   int t0, ntodo;
   st = laph_timeslice_split(LT, size, rank, &t0, &ntodo);
   if (st != LAPH_OK) return die(st, "timeslice split");
-  const int device =
-      env_int({"LAPH_DEVICE", "LOCAL_RANK", "OMPI_COMM_WORLD_LOCAL_RANK", "MPI_LOCALRANKID", "SLURM_LOCALID"}, 0);
+  // every rank says which part it took, so a wrong launcher guess shows at once
+  std::printf("{\"launcher\": \"%s\", \"rank\": %d, \"size\": %d, \"device\": %d, \"t0\": %d, \"t1\": %d}\n", ln.name,
+              rank, size, device, t0, t0 + ntodo - 1);
   char conf_name[1100];
   std::snprintf(conf_name, sizeof conf_name, "%s/conf.%04d", P.config_path, config);
   std::vector<double> conf((size_t)std::max(ntodo, 1) * V3 * 72);

@@ -1,8 +1,11 @@
 """The C-ABI library loads on a CPU-only host and exports every entry point
-that include/laph_gpu.h declares (no compute calls)."""
+that include/laph_gpu.h declares (no compute calls); on a GPU the runtime
+reports its kernels as sm_100 code."""
 import os
 import re
 import subprocess
+
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -30,9 +33,22 @@ def test_version_and_errors():
     assert lb.lib.laph_strerror(0) == b"ok"
 
 
-def test_sm100a_only():
-    """The shipped cubin targets sm_100a."""
+@pytest.mark.gpu
+def test_kernels_are_built_for_sm100():
+    """The CUDA runtime reports the library's kernels as sm_100 code (cudaFuncGetAttributes binaryVersion)."""
+    import ctypes
     import laph_eigsys_b200 as lb
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", lb._lib.LIB_PATH],
-                         capture_output=True, text=True)
-    assert "sm_100a" in out.stdout
+    v = ctypes.c_int(0)
+    assert lb.lib.laph_binary_version(ctypes.byref(v)) == 0, lb.lib.laph_last_error()
+    assert v.value == 100
+
+
+def test_binary_version_without_a_device_is_an_error_not_a_guess():
+    import ctypes
+    import torch
+    import laph_eigsys_b200 as lb
+    if torch.cuda.is_available():
+        pytest.skip("a device is visible")
+    v = ctypes.c_int(-1)
+    assert lb.lib.laph_binary_version(ctypes.byref(v)) != 0
+    assert v.value == -1

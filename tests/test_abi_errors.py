@@ -182,3 +182,21 @@ def test_last_error_is_per_thread():
     for t in ts:
         t.join()
     assert not errors, errors
+
+
+def test_noalloc_refuses_overlapping_vectors_before_the_device():
+    """laph_matmult_noalloc reads x while it writes y, so overlapping x and y are refused with LAPH_EINVAL before
+    any CUDA call (the pointers below are never dereferenced)."""
+    L = 4
+    vb = 16 * 3 * L ** 3
+    base = 1 << 40
+    for dx, dy in ((base, base), (base, base + vb - 16), (base + 32, base)):
+        st = lib.laph_matmult_noalloc(ctypes.c_void_p(base), L, 12.0, 0.5, 4, ctypes.c_void_p(dx),
+                                      ctypes.c_void_p(dy), None)
+        assert st == _lib.LAPH_EINVAL, (dx, dy)
+        assert "overlap" in _err()
+    # L beyond the fixed array, deg < 1 and a reversed window are refused the same way
+    for L_, deg, ll, lc in ((33, 4, 12.0, 0.5), (8, 0, 12.0, 0.5), (8, 4, 0.5, 12.0)):
+        st = lib.laph_matmult_noalloc(ctypes.c_void_p(base), L_, ll, lc, deg, ctypes.c_void_p(base),
+                                      ctypes.c_void_p(base + (1 << 30)), None)
+        assert st == _lib.LAPH_EINVAL

@@ -19,7 +19,8 @@ TUNE = os.path.join(ROOT, "laph_eigsys_b200", "laph_tune_hyp")
 # rank / size / device variables of the launchers laph_ev_ts understands
 LAUNCHER_VARS = ("LAPH_RANK", "LAPH_WORLD_SIZE", "LAPH_DEVICE", "RANK", "WORLD_SIZE", "LOCAL_RANK",
                  "OMPI_COMM_WORLD_RANK", "OMPI_COMM_WORLD_SIZE", "OMPI_COMM_WORLD_LOCAL_RANK", "PMI_RANK", "PMI_SIZE",
-                 "MPI_LOCALRANKID", "SLURM_PROCID", "SLURM_NTASKS", "SLURM_LOCALID")
+                 "MPI_LOCALRANKID", "SLURM_PROCID", "SLURM_NTASKS", "SLURM_LOCALID", "SLURM_STEP_ID",
+                 "SLURM_STEP_NUM_TASKS")
 
 
 def _run(exe, args, cwd, env=None):
@@ -94,13 +95,31 @@ def test_ev_ts_resume_over_complete_outputs_needs_no_solve(tmp_path):
     # launcher sets the rank and size
     for env in ({"LAPH_WORLD_SIZE": "2", "LAPH_RANK": "1"}, {"WORLD_SIZE": "2", "RANK": "1"},
                 {"OMPI_COMM_WORLD_SIZE": "2", "OMPI_COMM_WORLD_RANK": "1"}, {"PMI_SIZE": "2", "PMI_RANK": "1"},
-                {"SLURM_NTASKS": "2", "SLURM_PROCID": "1"}):
+                {"SLURM_STEP_ID": "0", "SLURM_STEP_NUM_TASKS": "2", "SLURM_PROCID": "1"}):
         r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path, env)
         assert r.returncode == 0, r.stderr
         assert [ln for ln in r.stdout.splitlines() if '"skipped"' in ln] == skipped[3:], env
     # rank 0 of 3 under srun: timeslices 0, 1
-    r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path, {"SLURM_NTASKS": "3", "SLURM_PROCID": "0"})
+    r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path,
+             {"SLURM_STEP_ID": "0", "SLURM_STEP_NUM_TASKS": "3", "SLURM_PROCID": "0", "SLURM_NTASKS": "8"})
     assert [ln for ln in r.stdout.splitlines() if '"skipped"' in ln] == skipped[:2]
+    assert '"launcher": "srun", "rank": 0, "size": 3' in r.stdout
+
+
+def test_ev_ts_plain_process_in_a_slurm_allocation_takes_every_timeslice(tmp_path):
+    """A process started inside an sbatch allocation of 8 tasks, but not by srun, sees SLURM_NTASKS = 8 and
+    SLURM_PROCID = 0; those describe the allocation, so laph_ev_ts must run as rank 0 of 1 and take all
+    timeslices.  Rank and size never mix launchers either (torchrun's rank with Slurm's size)."""
+    L, T, nev, cfgno = 4, 5, 6, 1227
+    out = _setup(tmp_path, L, T, nev, cfgno)
+    for t in range(T):
+        _write_complete_outputs(out, cfgno, t, 3 * L ** 3, nev, t)
+    for env in ({"SLURM_NTASKS": "8", "SLURM_PROCID": "0", "SLURM_LOCALID": "0"},
+                {"SLURM_NTASKS": "8", "SLURM_PROCID": "0", "RANK": "3"}):
+        r = _run(EV_TS, ["--conf", str(cfgno), "--resume"], tmp_path, env)
+        assert r.returncode == 0, r.stderr
+        assert '"launcher": "none", "rank": 0, "size": 1, "device": 0, "t0": 0, "t1": 4' in r.stdout, (env, r.stdout)
+        assert len([ln for ln in r.stdout.splitlines() if '"skipped"' in ln]) == T
 
 
 @pytest.mark.parametrize("damage", ["short_phases", "bad_trace", "missing_eigenvalues"])

@@ -367,7 +367,17 @@ def test_oracle_hyp_uses_reference_lookup_tables(tmp_path, orc, L):
     assert np.abs(got - Us).max() <= 1e-12
 
 
-REF_PARAMS = os.environ.get("LAPH_REFERENCE", "/root/reference") + "/src/parameters.txt"
+def _refdir():
+    """The reference checkout's directory as oracle/Makefile knows it ($LAPH_REFERENCE or the build machine's)."""
+    try:
+        out = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "refdir"], capture_output=True,
+                             text=True, timeout=30)
+        return out.stdout.strip()
+    except Exception:
+        return ""
+
+
+REF_PARAMS = os.path.join(_refdir(), "src", "parameters.txt")
 
 
 @pytest.mark.skipif(not os.path.isfile(REF_PARAMS), reason="the reference checkout is not on this machine")
