@@ -141,32 +141,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def filter_bytes(m, kb, link_bytes):
-    """Algorithmic bytes of one filter pass (m-1 launches) per site-vector, and
-    the link bytes per site per column block per launch.
-    step 1 : read S, write E2                     (FP32 complex, 24 B each)
-    step 2 : read E2, S, write E3
-    step n : read E_n, E_{n-1}, S, write E_{n+1}
-    final  : as its step, but reads V (FP64) and writes W (FP64) instead of E_m."""
-    per = 0
-    for n in range(1, m):
-        reads = 1 if n == 1 else (2 if n == 2 else 3)
-        if n == m - 1:
-            per += reads * 24 + 48 + 48
-        else:
-            per += reads * 24 + 24
-    return per, link_bytes
-
-
-def generate_links(cfg, seed_offset=0):
-    """Spatial links of one batch: list of (L, nev, links (V3, 3, 3, 3))."""
-    import laph_eigsys_b200 as lb
+def generate_links(cfg, seed_offset=0, oracle_generator=False):
+    """Spatial links of one batch: list of (L, nev, links (V3, 3, 3, 3)).  oracle_generator: the oracle's
+    restatement of the seeded generator (same field to rounding), for the reference arm, which must not load the
+    library."""
+    if oracle_generator:
+        import oracle as gen
+    else:
+        import laph_eigsys_b200 as gen
     out = []
     if cfg.get("scan"):
-        conf = lb.gauge_random(cfg["L"], 1, cfg["eps"], cfg["seed"] + seed_offset)
+        conf = gen.gauge_random(cfg["L"], 1, cfg["eps"], cfg["seed"] + seed_offset)
         return [(cfg["L"], cfg["nev"], np.ascontiguousarray(conf[0, :, 1:4])) for _ in cfg["scan"]]
     for L, T, nev, seed in cfg.get("mixed") or [(cfg["L"], cfg.get("wave") or cfg["T"], cfg["nev"], cfg["seed"])]:
-        conf = lb.gauge_random(L, T, cfg["eps"], seed + seed_offset)
+        conf = gen.gauge_random(L, T, cfg["eps"], seed + seed_offset)
         for t in range(T):
             out.append((L, nev, np.ascontiguousarray(conf[t, :, 1:4])))
     return out
@@ -212,7 +200,7 @@ def make_solver(cfg, device, batch):
     return s
 
 
-def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads, L=None, nev=None):
+def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads, L=None, nev=None, keep=False):
     """One timeslice of the reference ev_ts path on the CPU oracle: smear + Krylov-Schur on T_DEG(B)."""
     import oracle as orc
     orc.set_threads(threads)
@@ -230,7 +218,10 @@ def cpu_reference_step(cfg, links_ts, lam_c, deg_ref, threads, L=None, nev=None)
     st, theta, V, nconv, its, nmv = orc.eps_solve(Us, L, 12.0, lam_c, deg_ref, nev, tol=1e-10, max_it=100)
     Vf, ph = orc.fix_phase(V)
     dt = time.perf_counter() - t0
-    return dt, dict(status=st, nconv=nconv, restarts=its, matvecs=nmv)
+    info = dict(status=st, nconv=nconv, restarts=its, matvecs=nmv)
+    if keep:
+        info["_solution"] = (Us, Vf)
+    return dt, info
 
 
 def plain_gpu(cfg, batch, lam_c, ntimeslices, device, deg_ref=12):
@@ -293,7 +284,7 @@ def run_reference(args, cfg):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    batch = generate_links(cfg)
+    batch = generate_links(cfg, oracle_generator=True)
     lam_c = cfg.get("lam_c_ref", 0.65)
     deg_ref = 12
     if args.cpu_layout == "per-core":
@@ -320,12 +311,28 @@ def run_reference(args, cfg):
     value = args.steps / tot
     sample = (f"1 timeslice per step ({batch[0][0]}^3, nev {batch[0][1]}, smear + Krylov-Schur on T_{deg_ref}(B), "
               f"LAM_L 12, LAM_C {lam_c}, tol 1e-10)")
+    cpu = {"value": value, "unit": "timeslices/s", "cores": threads, "kind": "port",
+           "layout": "OpenMP inside one timeslice", "sample": sample, "last": info,
+           "inputs": "seeded field from the oracle's generator (the library is not loaded in this arm)"}
+    if not args.no_per_core:
+        # the reference's MPI layout (src/ev_ts.cpp:103-119): one round of one single-threaded timeslice per core,
+        # wall clock around the round, no warm-up round (a round is minutes at 32^3)
+        import multiprocessing as mp
+        jobs = [(cfg, batch[i % len(batch)][2], lam_c, deg_ref, batch[0][0], batch[0][1]) for i in range(threads)]
+        with mp.get_context("spawn").Pool(threads) as pool:
+            t0 = time.perf_counter()
+            out = pool.map(_per_core_step, jobs)
+            wall = time.perf_counter() - t0
+        cpu["per_core"] = {"value": threads / wall, "unit": "timeslices/s", "cores": threads,
+                           "layout": "one single-threaded timeslice per core (the reference's MPI layout)",
+                           "sample": f"one round of {threads} timeslices, wall clock", "seconds": wall,
+                           "last": out[0][1]}
+        cpu["value_best_layout"] = max(value, threads / wall)
     line = {"impl": "reference", "metric": "timeslices/s to nev pairs @resid<=1e-9", "value": value,
             "unit": "timeslices/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": workload_config(cfg),
-            "cpu_baseline": {"value": value, "unit": "timeslices/s", "cores": threads, "kind": "port",
-                             "layout": "OpenMP inside one timeslice", "sample": sample, "last": info},
+            "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": "timeslices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -386,7 +393,7 @@ def measure_displacement(solver, stream, batch, reps=4):
 
 def measure_matvec_fp64(cfg, batch, device, deg=12, reps=20):
     """The plain form's MatShell MatMult y = T_deg(B) x (FP64, one vector, device pointers), CUDA events around
-    `reps` products on the context's stream.  Algorithmic bytes per site and B application: the 6 links a site
+    each of `reps` products on the context's stream.  Algorithmic bytes per site and B application: the 6 links a site
     reads once (its 3 forward links; the backward ones are other sites' forward links) = 432, plus x read,
     z read, y written = 3 x 48."""
     import torch
@@ -397,20 +404,28 @@ def measure_matvec_fp64(cfg, batch, device, deg=12, reps=20):
     dim = 3 * L ** 3
     x = torch.randn(dim, dtype=torch.complex128, device="cuda")
     y = torch.empty_like(x)
-    ctx.matmult_device(x.data_ptr(), y.data_ptr(), deg)  # warm-up
+    for _ in range(3):
+        ctx.matmult_device(x.data_ptr(), y.data_ptr(), deg)  # warm-up
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(reps):
+    for a, b in evs:
+        a.record(stream)
         ctx.matmult_device(x.data_ptr(), y.data_ptr(), deg)
+        b.record(stream)
     torch.cuda.synchronize()
-    ms = (time.perf_counter() - t0) * 1e3 / reps
+    host_ms = (time.perf_counter() - t0) * 1e3 / reps
+    ms = sum(a.elapsed_time(b) for a, b in evs) / reps
     ctx.close()
     byts = deg * L ** 3 * (432.0 + 3 * 48.0)
     hbm, src = peaks()
     return {"workload": f"T_{deg}(B) x on one {L}^3 vector, FP64 (laph_matmult, device pointers)",
             "ms_per_matmult": ms, "bytes_per_matmult": byts, "achieved_gbs": byts / (ms / 1e3) / 1e9,
             "peak_gbs": hbm, "peak_source": src, "frac": byts / (ms / 1e3) / 1e9 / hbm,
-            "timing": "host clock around synchronised device-pointer calls (each call synchronises its stream)"}
+            "kernel": "k_cheb64_fused (one cooperative launch per product)",
+            "timing": "CUDA events on the context's stream around each call (device time of the product and its "
+                      "error-flag read), mean of the calls", "host_ms_per_matmult": host_ms}
 
 
 def measure_lime_io(L=32, T=16, no_cpu=False):
@@ -527,6 +542,8 @@ def main():
                     help="reference arm: OpenMP inside one timeslice (default) or one single-threaded timeslice per "
                          "core (the reference's MPI layout; a step is one round over all cores, minutes at 32^3)")
     ap.add_argument("--plain-timeslices", type=int, default=2)
+    ap.add_argument("--no-per-core", action="store_true",
+                    help="reference arm: skip the extra per-core round recorded beside the OpenMP figure")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
@@ -593,6 +610,7 @@ def main():
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     filt_ms, fsv, flaunch, launches, iters = 0.0, 0, 0, 0, []
+    fbytes_tot = [0.0, 0.0]
     e0.record(stream)
     for _ in range(args.steps):
         st, results = solver.run()
@@ -602,6 +620,9 @@ def main():
         cn = solver.counters()
         filt_ms += tm[1]
         fsv += cn[0]
+        fb = solver.filter_bytes()
+        fbytes_tot[0] += fb[0]
+        fbytes_tot[1] += fb[1]
         flaunch += cn[1]
         launches += cn[2]
         iters.append(max(r["iters"] for r in results))
@@ -614,15 +635,15 @@ def main():
     max_resid = max(r["max_resid"] for r in results)
 
     # ---- roofline of lap_cheb_mrhs -----------------------------------------
-    m = cfg["deg"]
+    # algorithmic bytes of the timed filter passes, counted by the solver pass by pass (each pass's own degree,
+    # its unlocked columns and column blocks): what the correction-form recurrence moves, and the survey's unit
+    # of one step Y = 2BX - Z (72 B per site-vector-step + links once per column block)
     kb = cfg["block"] or 32
-    per_sv, _ = filter_bytes(m, kb, 0)
     link_b = 112 if cfg["link_prec"] == "bf16" else 216
-    sv_iter = fsv / (m - 1)  # site-vectors per filter pass, summed over passes
-    site_blocks = sv_iter / kb  # site x column-block pairs per pass
-    alg_bytes = sv_iter * per_sv + site_blocks * (m - 1) * link_b
+    alg_bytes, alg_s8d = fbytes_tot
     hbm, src = peaks()
     achieved = alg_bytes / (filt_ms / 1000.0) / 1e9 if filt_ms > 0 else None
+    achieved_s8d = alg_s8d / (filt_ms / 1000.0) / 1e9 if filt_ms > 0 else None
     kname = "k_cheb_mrhs2" if cfg.get("filter_kernel", 1) == 1 and kb <= 64 else "k_cheb_mrhs"
     roofline = {"kernel": f"{kname} (lap_cheb_mrhs)", "bound": "hbm", "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm if achieved else None, "peak_source": src,
@@ -630,7 +651,9 @@ def main():
                 "traffic_source": "ncu capture of 32^3 x 4, scaled by site-vectors",
                 "avg_launch_ms": filt_ms / max(flaunch, 1),
                 "bytes_per_launch": alg_bytes / max(flaunch, 1),
-                "filter_share_of_step": filt_ms / ms if ms > 0 else None}
+                "filter_share_of_step": filt_ms / ms if ms > 0 else None,
+                "achieved_s8d": achieved_s8d, "frac_s8d": achieved_s8d / hbm if achieved_s8d else None,
+                "bytes_model_s8d": f"72 + {link_b}/{kb} B per site-vector-step"}
 
     # ---- e2e through the public API with host buffers ----------------------
     e2e = None
@@ -685,24 +708,34 @@ def main():
             lime_io = {"error": f"{type(e).__name__}: {e}"}
 
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         ev0, _, _ = solver.get(0, vectors=False)
         lam = -ev0
         lam_c = float(1.1 * lam[-1])
         threads = os.cpu_count() or 1
-        dt, info = cpu_reference_step(cfg, batch[0][2], lam_c, 12, threads, batch[0][0], batch[0][1])
+        dt, info = cpu_reference_step(cfg, batch[0][2], lam_c, 12, threads, batch[0][0], batch[0][1], keep=True)
+        Us_orc, V_orc = info.pop("_solution")
         cpu = {"value": 1.0 / dt, "unit": "timeslices/s", "cores": threads, "kind": "port",
                "sample": f"timeslice 0 of the workload: {cfg['smear']} smearing + Krylov-Schur on T_12(B), "
                          f"LAM_L 12, LAM_C {lam_c:.4f} (1.1 x lambda_nev from this run), tol 1e-10",
                "seconds": dt, "detail": info}
+        # parity of the timed run's timeslice-0 eigenpairs against that FP64 oracle run (outside every timed region)
+        import oracle as orc
+        _, V_gpu, _ = solver.get(0)
+        parity = orc.compare_eigensystems(Us_orc, batch[0][0], V_gpu, V_orc)
+        parity["what"] = ("timeslice 0 of the timed batch (FP32 filter, FP64 Rayleigh-Ritz, tol 1e-9) against the "
+                          "oracle's FP64 smearing + Krylov-Schur on T_12(B) (tol 1e-10), both phase-fixed; "
+                          "eigenvalues as FP64 Rayleigh quotients on -Delta")
+        del V_gpu, V_orc
 
     if rank == 0:
         line = {"metric": "timeslices/s to nev pairs @resid<=1e-9", "value": value, "unit": "timeslices/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 filter / fp64 RR",
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
-                "roofline": roofline, "cpu_baseline": cpu, "plain_gpu": plain, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "plain_gpu": plain, "e2e": e2e,
+                "gpu_launches": launches,
                 "clocks": clk, "sourceshape": shape, "displacement": disp, "lime_io": lime_io, "autotune": tune,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid,
                            "filter_ms_per_step": filt_ms / args.steps,

@@ -225,6 +225,13 @@ int laph_solver_timings(laph_solver* s, double* ms4);
 /* Counters of the last run for roofline accounting: filter site-vector-steps,
  * number of filter kernel launches, total device kernel launches. */
 int laph_solver_counters(laph_solver* s, long long* c3);
+/* Algorithmic bytes of the last run's filter passes (lap_cheb_mrhs): b2[0] =
+ * what the correction-form recurrence must move (per unlocked site-vector and
+ * step 24 B for each of X, Z, S read and Y written, the last step FP64 V read
+ * and W written, W = V for locked columns, the links once per column block),
+ * b2[1] = the plain recurrence's unit, 72 B per site-vector-step (X, Z read, Y
+ * written) plus the links once per column block. */
+int laph_solver_filter_bytes(laph_solver* s, double* b2);
 
 /* Device memory a solver for probs[0..n) with opts allocates (bytes, each
  * allocation rounded up to 2 MiB), without touching a device. */

@@ -489,3 +489,10 @@ class Solver:
         c = (ctypes.c_longlong * 3)()
         check(lib.laph_solver_counters(self._h, c), "laph_solver_counters")
         return list(c)
+
+    def filter_bytes(self):
+        """Algorithmic bytes of the last run's filter passes (laph_solver_filter_bytes): (correction form as
+        run, 72 B + links per site-vector-step)."""
+        c = (ctypes.c_double * 2)()
+        check(lib.laph_solver_filter_bytes(self._h, c), "laph_solver_filter_bytes")
+        return list(c)

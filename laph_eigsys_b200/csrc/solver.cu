@@ -79,6 +79,11 @@ struct laph_solver {
   std::vector<int> degs;  // filter degree of each pass of the last run
   double ms[4] = {0, 0, 0, 0};
   long long cnt[3] = {0, 0, 0};
+  // algorithmic bytes of the filter passes of the last run: [0] what the
+  // kernels must move (X, Z, S read, Y written, FP64 V / W in the last step,
+  // W = V for locked columns, links once per column block), [1] the unit
+  // 72 B + links / block per unlocked site-vector-step (X, Z read, Y written)
+  double fbytes[2] = {0, 0};
   std::vector<cudaEvent_t> evf;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   int ran = 0;
@@ -497,6 +502,7 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     nlaunch += 2 + 7;  // pack, random block, first Rayleigh-Ritz
   }
   s->cnt[0] = s->cnt[1] = s->cnt[2] = 0;
+  s->fbytes[0] = s->fbytes[1] = 0.0;
   s->degs.clear();
   double filt_ms = 0.0;
   if (s->evf.empty()) {
@@ -562,8 +568,21 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
       const int m_safe = std::isfinite(ratio) ? (int)std::min(std::floor(ratio), 1e6) : 2;  // NaN window: degree 2
       m = std::min(m, std::max(2, m_safe));
     }
-    for (int i = 0; i < s->np; ++i)
-      if (s->hps[i].active) s->cnt[0] += (long long)s->hd[i].V3 * (s->hd[i].k - s->hps[i].nlock) * (m - 1);
+    const double lbytes = s->o.link_prec == LAPH_LINKS_BF16 ? 112.0 : 216.0;  // per site per column block
+    for (int i = 0; i < s->np; ++i) {
+      if (!s->hps[i].active) continue;
+      const ProbDesc& d = s->hd[i];
+      const int nl = s->hps[i].nlock, nact = d.k - nl;
+      s->cnt[0] += (long long)d.V3 * nact * (m - 1);
+      const int nblk = (d.k + s->kb - 1) / s->kb - nl / s->kb;  // column blocks with an unlocked column
+      double per = 0.0;  // bytes per unlocked site-vector over the pass
+      for (int n = 1; n < m; ++n) {
+        const int reads = n == 1 ? 1 : (n == 2 ? 2 : 3);
+        per += reads * 24.0 + (n == m - 1 ? 96.0 : 24.0);
+      }
+      s->fbytes[0] += (double)d.V3 * (nact * per + nl * 96.0 + (double)nblk * (m - 1) * lbytes);
+      s->fbytes[1] += (double)d.V3 * (m - 1) * (nact * 72.0 + (double)nblk * lbytes);
+    }
     s->cnt[1] += m - 1;
     s->degs.push_back(m);
     if (trace) std::fprintf(stderr, "laph_trace it %d filter degree %d\n", it, m);
@@ -737,6 +756,16 @@ int laph_solver_displace(laph_solver* s, int i, int dir, double* W, int on_devic
   if (!on_device)
     LAPH_CUDA_TRY(cudaMemcpyAsync(W, out, sizeof(double2) * d.dim * d.nev, cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return LAPH_OK;
+}
+
+int laph_solver_filter_bytes(laph_solver* s, double* b2) {
+  if (!s || !b2) {
+    set_error("laph_solver_filter_bytes: bad argument");
+    return LAPH_EINVAL;
+  }
+  b2[0] = s->fbytes[0];
+  b2[1] = s->fbytes[1];
   return LAPH_OK;
 }
 

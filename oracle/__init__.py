@@ -40,6 +40,7 @@ _sig("orc_lime_read_gauge", _i, ctypes.c_char_p, _i, _i, _i, _i, _vp)
 _sig("orc_map_timeslice", None, _vp, _i, _vp)
 _sig("orc_proj_su3", None, _vp)
 _sig("orc_expiH", None, _vp, _vp)
+_sig("orc_gauge_random", None, _vp, _i, _i, _d, ctypes.c_uint64)
 _sig("orc_smear_stout", None, _vp, _i, _d, _i, _i)
 _sig("orc_smear_ape", None, _vp, _i, _d, _i, _i)
 _sig("orc_smear_hyp", None, _vp, _i, _d, _d, _i)
@@ -95,6 +96,13 @@ def expiH(h):
     out = np.empty((3, 3), dtype=np.complex128)
     _lib.orc_expiH(_p(h), _p(out))
     return out
+
+
+def gauge_random(L, nt, eps, seed):
+    """Seeded synthetic gauge field (nt, V3, 4, 3, 3) complex128, U = exp(i eps H) (orc_gauge_random)."""
+    conf = np.empty((nt, L ** 3, 4, 3, 3), dtype=np.complex128)
+    _lib.orc_gauge_random(_p(conf), L, nt, eps, seed)
+    return conf
 
 
 def smear_stout(U, L, rho, iters, compat=1):
@@ -232,3 +240,72 @@ def mlp_loss_grad(params, X, Y):
     g = np.zeros_like(P)
     loss = _lib.orc_mlp_loss_grad(_p(P), _p(X), _p(Y), X.shape[0], _p(g))
     return loss, g
+
+
+def rayleigh(U, L, V):
+    """FP64 Rayleigh quotients lambda_j = v_j^H (-Delta) v_j / v_j^H v_j of the columns of V on links U, and their
+    residual norms ||(-Delta) v_j - lambda_j v_j|| / ||v_j|| (the oracle's stencil)."""
+    V = np.asarray(V)
+    lam = np.empty(V.shape[1])
+    res = np.empty(V.shape[1])
+    for j in range(V.shape[1]):
+        v = np.ascontiguousarray(V[:, j])
+        y = neglap(U, L, v)
+        n2 = np.vdot(v, v).real
+        lam[j] = np.vdot(v, y).real / n2
+        res[j] = np.linalg.norm(y - lam[j] * v) / np.sqrt(n2)
+    return lam, res
+
+
+def _subspace_distance(A, B):
+    """sin of the largest principal angle between span(A) and span(B) (orthonormal columns): ||A - B (B^H A)||_2."""
+    return float(np.linalg.norm(A - B @ (B.conj().T @ A), 2))
+
+
+def compare_eigensystems(U, L, Va, Vb, lam_max=12.0, gap=1e-3):
+    """Eigenpair parity of two eigensystems Va (the one checked) and Vb (the oracle's) of -Delta on links U, both
+    (dim, nev) column-major with the reference's phase fix applied (fix_phase).  Eigenvalues are compared as FP64
+    Rayleigh quotients on -Delta, each relative to itself (where lambda > 1e-12 lambda_max) and relative to
+    lambda_max; eigenvectors one by one where the eigenvalue is isolated (no neighbour within `gap`, absolute, in
+    units of lambda), and by subspace distance (sin of the largest principal angle) on clusters of eigenvalues
+    closer than `gap`.  `gap_min` is the smallest separation of an isolated eigenvalue: an eigenvector with residual
+    r is determined to about r / gap_min, which bounds what any two solvers can agree to."""
+    la, ra = rayleigh(U, L, Va)
+    lb, rb = rayleigh(U, L, Vb)
+    ia, ib = np.argsort(la), np.argsort(lb)
+    la, ra, lb, rb = la[ia], ra[ia], lb[ib], rb[ib]
+    Va, Vb = np.asarray(Va)[:, ia], np.asarray(Vb)[:, ib]
+    pos = lb > 1e-12 * lam_max
+    out = {"nev": int(len(lb)),
+           "max_rel_eig": float(np.max(np.abs(la - lb)[pos] / lb[pos])) if pos.any() else 0.0,
+           "max_eig_over_lam_max": float(np.max(np.abs(la - lb)) / lam_max),
+           "max_resid_checked": float(ra.max() / lam_max), "max_resid_oracle": float(rb.max() / lam_max),
+           "trace_vdv_checked": float(np.sum(np.abs(Va) ** 2)), "trace_vdv_oracle": float(np.sum(np.abs(Vb) ** 2))}
+    # clusters on the oracle's eigenvalues
+    cl, cur = [], [0]
+    for j in range(1, len(lb)):
+        if lb[j] - lb[j - 1] < gap:
+            cur.append(j)
+        else:
+            cl.append(cur)
+            cur = [j]
+    cl.append(cur)
+    vec, vec_al, proj, gmin = 0.0, 0.0, 0.0, np.inf
+    for c in cl:
+        if len(c) == 1:
+            j = c[0]
+            g = lb[j] - lb[j - 1] if j > 0 else np.inf
+            if j + 1 < len(lb):
+                g = min(g, lb[j + 1] - lb[j])
+            gmin = min(gmin, g)
+            a, b = Va[:, j], Vb[:, j]
+            vec = max(vec, float(np.linalg.norm(a - b)))
+            ph = np.vdot(a, b)
+            vec_al = max(vec_al, float(np.linalg.norm(a * (ph / abs(ph)) - b)))
+        else:
+            proj = max(proj, _subspace_distance(Va[:, c], Vb[:, c]))
+    out.update({"clusters": int(sum(len(c) > 1 for c in cl)), "in_clusters": int(sum(len(c) for c in cl if len(c) > 1)),
+                "max_vec_phase_fixed": vec, "max_vec_aligned": vec_al, "max_cluster_proj": proj,
+                "gap_min_isolated": float(gmin) if np.isfinite(gmin) else None,
+                "block_proj": _subspace_distance(Va, Vb), "cluster_gap": gap})
+    return out

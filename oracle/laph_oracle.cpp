@@ -366,6 +366,51 @@ void orc_proj_su3(double* m18) { store(m18, proj_su3(load(m18))); }
 
 void orc_expiH(const double* h18, double* out18) { store(out18, expiH(load(h18))); }
 
+/* The seeded synthetic gauge field of the benchmark configurations (no
+ * reference function: the reference reads its fields from ILDG files):
+ * U = exp(i eps H), H = sum_a c_a lambda_a over the Gell-Mann matrices, c_a
+ * i.i.d. N(0, 1), for all 4 links of every site of nt timeslices, conf laid
+ * out [t][site][mu][3][3] complex128 as the ILDG slice (slot 0 = U_t).  The
+ * normals come from the same counter-based SplitMix64 stream as the
+ * library's laph_gauge_random (link n: 4 Box-Muller pairs), so the two agree
+ * to rounding; exp(i eps H) goes through this oracle's own Hermitian
+ * eigensolver.  Lets CPU-only runs build their inputs without the library. */
+static inline uint64_t orc_mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+void orc_gauge_random(double* conf, int L, int nt, double eps, uint64_t seed) {
+  const long long nlinks = (long long)L * L * L * nt * 4;
+  const double is3 = 1.0 / std::sqrt(3.0);
+#pragma omp parallel for schedule(static)
+  for (long long n = 0; n < nlinks; ++n) {
+    uint64_t st = seed * 0x9E3779B97F4A7C15ULL + (uint64_t)n * 0xD1B54A32D192ED03ULL + 0x632BE59BD9B4E019ULL;
+    double c[8];
+    for (int k = 0; k < 4; ++k) {
+      st += 0x9E3779B97F4A7C15ULL;
+      const double u1 = ((orc_mix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+      st += 0x9E3779B97F4A7C15ULL;
+      const double u2 = ((orc_mix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+      const double r = std::sqrt(-2.0 * std::log(u1));
+      c[2 * k] = r * std::cos(2.0 * M_PI * u2);
+      c[2 * k + 1] = r * std::sin(2.0 * M_PI * u2);
+    }
+    M3 H = m3_zero();
+    H.m[0] = eps * (c[2] + c[7] * is3);
+    H.m[4] = eps * (-c[2] + c[7] * is3);
+    H.m[8] = eps * (-2.0 * c[7] * is3);
+    H.m[1] = eps * cd(c[0], -c[1]);
+    H.m[3] = eps * cd(c[0], c[1]);
+    H.m[2] = eps * cd(c[3], -c[4]);
+    H.m[6] = eps * cd(c[3], c[4]);
+    H.m[5] = eps * cd(c[5], -c[6]);
+    H.m[7] = eps * cd(c[5], c[6]);
+    store(conf + n * 18, expiH(H));
+  }
+}
+
 /* Tslice::smearing_stout, modules/timeslice.cpp:145-193 */
 void orc_smear_stout(double* U, int L, double rho, int iter, int compat) {
   Geo g(L);

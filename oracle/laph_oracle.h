@@ -104,6 +104,11 @@ void orc_sourceshape(const double* V, int L, int nev, double* psi);
 /* avg_radii (sourceshape_funcs.cpp:100-135); returns the number of radii. */
 int orc_sourceshape_avg(int L, const double* psi, double* r_out, double* psi_out);
 
+/* Seeded synthetic gauge field U = exp(i eps H) of the benchmark inputs, all 4
+ * links of nt timeslices, [t][site][mu][3][3] complex128 (the ILDG slice
+ * layout); same normal stream as the library's laph_gauge_random. */
+void orc_gauge_random(double* conf, int L, int nt, double eps, uint64_t seed);
+
 /* Window MLP (16->64->64->3, tanh) mean-squared loss and gradient, FP64. */
 double orc_mlp_loss_grad(const double* params, const double* X, const double* Y, int n, double* grad);
 

@@ -65,6 +65,35 @@ def test_matmult_parity(gpu, orc, L, deg):
     ctx.close()
 
 
+@pytest.mark.parametrize("L,deg", [(32, 12), (36, 5), (5, 7)])
+def test_matmult_fused_launch_shapes(gpu, orc, L, deg):
+    """The one-launch product at the largest lattice whose sites all fit the device's co-resident CTAs one per
+    thread (32^3: 256 CTAs, links held in registers and shared memory), beyond it (36^3: grid-stride, links read
+    per step) and at a ragged last CTA (5^3 = 125 sites), against the oracle's tv_iter, through host and device
+    pointers, twice in a row on one context."""
+    import torch
+    U = random_links(L, 0.3, 1500 + L)
+    lam_l, lam_c = 12.0, 0.7
+    ctx = gpu.Context(L, lam_l, lam_c, deg)
+    ctx.set_links(U)
+    rng = np.random.default_rng(L)
+    for rep in range(2):
+        x = rng.normal(size=3 * L ** 3) + 1j * rng.normal(size=3 * L ** 3)
+        ref = orc.tv_iter(U, L, lam_l, lam_c, deg, x)
+        y = ctx.matmult(x)
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) <= 1e-13, (rep, "host")
+        dx = torch.from_numpy(x.copy()).cuda()
+        dy = torch.empty_like(dx)
+        ctx.matmult_device(dx.data_ptr(), dy.data_ptr())
+        yd = dy.cpu().numpy()
+        assert np.linalg.norm(yd - ref) / np.linalg.norm(ref) <= 1e-13, (rep, "device")
+    # overlapping device vectors are refused: the product reads x while it writes y
+    with pytest.raises(gpu.LaphError) as e:
+        ctx.matmult_device(dx.data_ptr(), dx.data_ptr())
+    assert e.value.status == gpu._lib.LAPH_EINVAL
+    ctx.close()
+
+
 def test_neglap_diag_plaquette(gpu, orc):
     L = 6
     U = random_links(L, 0.4, 77)

@@ -167,3 +167,15 @@ def test_proj_su3_ill_conditioned(orc, cond):
         Q = u2 @ vh2
         Q = Q / np.linalg.det(Q) ** (1.0 / 3.0)
         assert np.abs(orc.proj_su3(N) - Q).max() < 1e-13
+
+
+def test_oracle_gauge_generator_matches_the_library(orc):
+    """The oracle's restatement of the seeded field generator (used where the library must not be loaded, such as
+    the CPU reference arm) gives the library's field to rounding, SU(3) link by link."""
+    import laph_eigsys_b200 as lb
+    a = orc.gauge_random(5, 3, 0.3, 1229)
+    b = lb.gauge_random(5, 3, 0.3, 1229)
+    assert np.abs(a - b).max() < 1e-13
+    U = a.reshape(-1, 3, 3)
+    assert np.abs(U @ np.conj(np.transpose(U, (0, 2, 1))) - np.eye(3)).max() < 1e-13
+    assert np.abs(np.linalg.det(U) - 1.0).max() < 1e-13
