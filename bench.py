@@ -338,6 +338,98 @@ def run_reference(args, cfg):
     return 0
 
 
+def solve_config(cfg, device, reps=1, window=None, link_prec=None, wave=None, parity=None, no_cpu=False):
+    """One configuration of the survey as a compact sub-record: its batch (or one memory-bounded wave of it) solved
+    once untimed (graph capture) and `reps` times timed with CUDA events on the solver's stream, with iterations,
+    residual, the filter's algorithmic bandwidth and, where asked, parity of timeslice 0 (or all timeslices of a
+    small lattice) against the oracle.  Everything here runs outside the headline's timed region."""
+    import torch
+    import laph_eigsys_b200 as lb
+    cfg = dict(cfg)
+    if window:
+        cfg["window"] = window
+    if link_prec:
+        cfg["link_prec"] = link_prec
+    if wave:
+        if cfg.get("mixed"):
+            cfg["mixed"] = [(L, wave[i], nev, seed) for i, (L, T, nev, seed) in enumerate(cfg["mixed"])]
+        else:
+            cfg["wave"] = wave
+    batch = generate_links(cfg)
+    solver = make_solver(cfg, device, batch)
+    if cfg.get("window", "mlp") == "mlp":
+        from laph_eigsys_b200 import window as lw
+        lw.set_model(solver, lw.load_model())
+    for i, (_, _, U) in enumerate(batch):
+        solver.set_links(i, U)
+    stream = torch.cuda.ExternalStream(solver.stream())
+    st, res = solver.run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    filt_ms, fb = 0.0, [0.0, 0.0]
+    e0.record(stream)
+    for _ in range(reps):
+        st, res = solver.run()
+        filt_ms += solver.timings()[1]
+        b = solver.filter_bytes()
+        fb[0] += b[0]
+        fb[1] += b[1]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    hbm, src = peaks()
+    kb = cfg.get("block") or 32
+    out = {"workload": workload_config(cfg)["workload"], "timeslices": len(batch), "status": st,
+           "value": len(batch) / (ms / 1e3), "unit": "timeslices/s", "ms_per_solve": ms,
+           "outer_iterations": max(r["iters"] for r in res), "max_resid": max(r["max_resid"] for r in res),
+           "window": cfg.get("window", "mlp"), "links": cfg["link_prec"], "deg": cfg["deg"],
+           "window_fallbacks": sum(r["window_fallback"] for r in res),
+           "filter": {"ms_per_solve": filt_ms / reps, "achieved_gbs": fb[0] / (filt_ms / 1e3) / 1e9,
+                      "frac": fb[0] / (filt_ms / 1e3) / 1e9 / hbm,
+                      "frac_s8d": fb[1] / (filt_ms / 1e3) / 1e9 / hbm, "peak_gbs": hbm, "peak_source": src,
+                      "bytes_model_s8d": f"72 + {112 if cfg['link_prec'] == 'bf16' else 216}/{kb} B"}}
+    if parity and not no_cpu:
+        import oracle as orc
+        orc.set_threads(os.cpu_count() or 1)
+        worst = {}
+        for t in parity["timeslices"]:
+            L, nev, U = batch[t]
+            Us = smear_oracle(cfg, U, L)
+            if parity["kind"] == "dense":
+                w, Vd = np.linalg.eigh(orc.neglap_dense(Us, L))
+                Vo, _ = orc.fix_phase(Vd[:, :nev])
+            else:
+                lam = -solver.get(t, vectors=False)[0]
+                sto, _, Vk, _, _, _ = orc.eps_solve(Us, L, 12.0, float(1.1 * lam[-1]), 12, nev, tol=1e-12,
+                                                     max_it=200)
+                Vo, _ = orc.fix_phase(Vk)
+            r = orc.compare_eigensystems(Us, L, solver.get(t)[1], Vo)
+            for k_, v in r.items():
+                if isinstance(v, float) and (k_.startswith("max") or k_ == "block_proj"):
+                    worst[k_] = max(worst.get(k_, 0.0), v)
+            g = r["gap_min_isolated"]
+            if g is not None:
+                worst["gap_min_isolated"] = min(worst.get("gap_min_isolated", g), g)
+        worst["against"] = ("oracle smearing + dense eigh of the assembled -Delta" if parity["kind"] == "dense" else
+                            "oracle smearing + FP64 Krylov-Schur on T_12(B), tol 1e-12")
+        worst["timeslices"] = list(parity["timeslices"])
+        out["parity"] = worst
+    solver.close()
+    del batch
+    return out
+
+
+def smear_oracle(cfg, U, L):
+    import oracle as orc
+    if cfg["smear"] == "stout":
+        return orc.smear_stout(U, L, cfg["p1"], cfg["iters"], cfg["compat"])
+    if cfg["smear"] == "ape":
+        return orc.smear_ape(U, L, cfg["p1"], cfg["iters"], cfg["compat"])
+    if cfg["smear"] == "hyp":
+        return orc.smear_hyp(U, L, cfg["p1"], cfg["p2"], cfg["iters"])
+    return U
+
+
 def workload_config(cfg):
     if cfg.get("mixed"):
         shape = " + ".join(f"{L}^3x{T} (nev {nev})" for L, T, nev, _ in cfg["mixed"]) + " in one batch"
@@ -535,6 +627,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-shape", action="store_true")
     ap.add_argument("--no-io", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the learned-window A/B and the sub-records of the other survey configurations")
     ap.add_argument("--autotune", type=int, default=0, metavar="NSAMPLE",
                     help="tune deg / block / guard on the first NSAMPLE timeslices before measuring (0: off)")
     ap.add_argument("--tune-cache", default=None, help="autotuner cache file")
@@ -611,6 +705,7 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     filt_ms, fsv, flaunch, launches, iters = 0.0, 0, 0, 0, []
     fbytes_tot = [0.0, 0.0]
+    window_fallbacks = 0
     e0.record(stream)
     for _ in range(args.steps):
         st, results = solver.run()
@@ -626,6 +721,7 @@ def main():
         flaunch += cn[1]
         launches += cn[2]
         iters.append(max(r["iters"] for r in results))
+        window_fallbacks = sum(r["window_fallback"] for r in results)
     e1.record(stream)
     barrier()
     clk = clocks.stop()
@@ -729,6 +825,28 @@ def main():
                           "eigenvalues as FP64 Rayleigh quotients on -Delta")
         del V_gpu, V_orc
 
+    solver.close()
+    # ---- learned window A/B and the survey's other configurations (rank 0, N = 1, untimed for the headline) --
+    window_ab = configs = None
+    if rank == 0 and world == 1 and not args.no_configs and args.config == "c3":
+        torch.cuda.synchronize()
+        lanc = solve_config(cfg, local, reps=1, window="lanczos")
+        window_ab = {"workload": "the headline batch", "mlp": {"value": value, "outer_iterations": max(iters),
+                                                              "window_fallbacks": window_fallbacks},
+                     "lanczos": {k: lanc[k] for k in ("value", "outer_iterations", "ms_per_solve", "status")},
+                     "gain": value / lanc["value"] if lanc["value"] else None}
+        configs = {}
+        for name, kw in (("c1", dict(parity={"kind": "dense", "timeslices": range(16)})),
+                         ("c2", dict(wave=16, parity={"kind": "ks", "timeslices": [0]})),
+                         ("c3_bf16", dict(link_prec="bf16")),
+                         ("c4_wave", dict(wave=[8, 12, 16])),
+                         ("c5_wave", dict(wave=16))):
+            base = CONFIGS[name.split("_")[0]]
+            try:
+                configs[name] = solve_config(base, local, no_cpu=args.no_cpu, **kw)
+            except Exception as e:  # one configuration's failure must not cost the headline line
+                configs[name] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.synchronize()
     if rank == 0:
         line = {"metric": "timeslices/s to nev pairs @resid<=1e-9", "value": value, "unit": "timeslices/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -737,12 +855,12 @@ def main():
                 "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "plain_gpu": plain, "e2e": e2e,
                 "gpu_launches": launches,
                 "clocks": clk, "sourceshape": shape, "displacement": disp, "lime_io": lime_io, "autotune": tune,
+                "window_ab": window_ab, "configs": configs,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid,
                            "filter_ms_per_step": filt_ms / args.steps,
                            "timings_last_ms": dict(zip(["smear+setup", "filter", "dense+stencil64", "total"],
                                                        solver.timings()))}}
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -189,6 +189,14 @@ typedef struct {
   int jacobi_sweeps;    /* cap on Jacobi sweeps per Rayleigh-Ritz (0: 2); an
                            unfinished sweep set only delays convergence, since
                            residuals are always computed from the new vectors   */
+  double window_margin; /* learned window: first-pass cut = margin x the
+                           predicted converged cut (<= 0: the calibrated 1.4)  */
+  int host_loop;        /* 0 (default): the whole solve is one CUDA graph launch
+                           whose WHILE node repeats the outer iteration on the
+                           device; 1: the host drives the outer iteration (one
+                           filter graph and one Rayleigh-Ritz graph per pass,
+                           the convergence mask read each pass), also taken
+                           with LAPH_TRACE set                                   */
 } laph_solve_opts;
 void laph_solve_opts_default(laph_solve_opts* o);
 
@@ -200,6 +208,9 @@ typedef struct {
   double lam_cut0, lam_max;  /* initial window                                    */
   double max_resid;     /* max over the nev wanted pairs                          */
   double trace_vdv;     /* tr(V^dag V) of the returned eigenvectors               */
+  int window_fallback;  /* 1: the learned first window failed its check after
+                           the first pass and the solve went on with the
+                           non-learned window (lam_max back to 12)             */
 } laph_result;
 
 typedef struct laph_solver laph_solver;

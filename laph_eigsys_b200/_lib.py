@@ -41,12 +41,13 @@ class laph_solve_opts(ctypes.Structure):
                 ("smear_compat", c_int), ("guard", c_int), ("link_prec", c_int), ("tol", c_double),
                 ("max_it", c_int), ("window", c_int), ("lam_cut", c_double), ("lam_max", c_double),
                 ("deg", c_int), ("phase_fix", c_int), ("seed", c_u64), ("block", c_int), ("filter_kernel", c_int),
-                ("jacobi_sweeps", c_int)]
+                ("jacobi_sweeps", c_int), ("window_margin", c_double),
+                ("host_loop", c_int)]
 
 
 class laph_result(ctypes.Structure):
     _fields_ = [("status", c_int), ("iters", c_int), ("nconv", c_int), ("deg", c_int), ("lam_cut0", c_double),
-                ("lam_max", c_double), ("max_resid", c_double), ("trace_vdv", c_double)]
+                ("lam_max", c_double), ("max_resid", c_double), ("trace_vdv", c_double), ("window_fallback", c_int)]
 
 
 class laph_tune_result(ctypes.Structure):

@@ -546,7 +546,9 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
 //   step n: E'_{n+1} = (2 nu_n B E'_n - nu_{n-1} E'_{n-1} + T_n S) / nu_{n+1}
 //   final : W' = (T_m / nu_m) V + E'_m   (= W / nu_m)
 __global__ void k_coef(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, int np,
-                       const double* __restrict__ theta, double* __restrict__ tcoef, double* __restrict__ scol, int m) {
+                       const double* __restrict__ theta, double* __restrict__ tcoef, double* __restrict__ scol, int m,
+                       const int* __restrict__ dm) {
+  if (dm) m = *dm;  // degree decided on the device (the device-side loop)
   const int p = blockIdx.x;
   if (p >= np || !ps[p].active) return;
   const ProbDesc d = pd[p];
@@ -919,8 +921,8 @@ int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* 
   return LAPH_OK;
 }
 int coef(const ProbDesc* pd, const ProbState* ps, int np, const double* theta, double* tcoef, double* scol, int m,
-         cudaStream_t st) {
-  k_coef<<<np, 256, 0, st>>>(pd, ps, np, theta, tcoef, scol, m);
+         const int* dm, cudaStream_t st) {
+  k_coef<<<np, 256, 0, st>>>(pd, ps, np, theta, tcoef, scol, m, dm);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

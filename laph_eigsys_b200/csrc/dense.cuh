@@ -17,9 +17,10 @@ constexpr int kSmallPhases = 7;
 int small_dense(const ProbDesc* pd, ProbState* ps, int np, double2* KK, double* theta, double* tcoef, double* scol,
                 double* dwork, int first_iter, int fixed_cut, int max_sweeps, unsigned long long* tstamp,
                 cudaStream_t st);
-// Chebyshev coefficient table and S scaling for a filter of degree m.
+// Chebyshev coefficient table and S scaling for a filter of degree m (or *dm
+// when dm is not null: the degree the device-side loop chose).
 int coef(const ProbDesc* pd, const ProbState* ps, int np, const double* theta, double* tcoef, double* scol, int m,
-         cudaStream_t st);
+         const int* dm, cudaStream_t st);
 int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* W,
            const double2* KK, double2* V, cudaStream_t st);
 int residual64(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,

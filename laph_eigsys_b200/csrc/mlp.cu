@@ -305,31 +305,34 @@ __global__ void __launch_bounds__(1024) k_features(const ProbDesc* __restrict__ 
   }
 }
 
-constexpr double kFirstPassCut = 1.4;
-
 // Window inference: standardised features -> MLP -> (lam_cut, lam_max, deg)
-// per problem, written into the problem state (lam_cut for the first pass,
-// lam_max = min(12, max(prediction, Lanczos bound))), degrees to out_deg.
+// per problem, written into the problem state for the first filter pass.
+//   lam_cut = margin x exp(prediction 0): target 0 is the log of the cut the
+//             adaptive iteration converges to; the first pass starts above it
+//             because its block is still a random one (margin calibrated on
+//             training lattices, laph_solve_opts.window_margin);
+//   lam_max = min(12, max(prediction 1, Lanczos bound)): the top of the
+//             damped interval, never below the 10-step Lanczos estimate of the
+//             top of the spectrum nor above the exact bound 12 (a first pass
+//             whose residual check fails goes back to 12, see the solver);
+//   degree  = prediction 2, clamped to [8, 64], written to out_deg.
 __global__ void k_window_apply(const ProbDesc* __restrict__ pd, ProbState* __restrict__ ps, int np,
                                const float* __restrict__ O, const float* __restrict__ norm,
-                               const double* __restrict__ bound, int* __restrict__ out_deg) {
+                               const double* __restrict__ bound, int* __restrict__ out_deg, double margin) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
   const float* om = norm + 2 * kMlpIn;  // output mean[3], std[3]
   const double y0 = O[p * kMlpOut + 0] * om[3] + om[0];
   const double y1 = O[p * kMlpOut + 1] * om[4] + om[1];
   const double y2 = O[p * kMlpOut + 2] * om[5] + om[2];
-  // target 0 is log of the cut the adaptive iteration converges to; the first
-  // pass starts above it (x kFirstPassCut) because its Ritz vectors are still
-  // those of a random block
-  const double cut = exp(y0) * kFirstPassCut;
-  (void)y1;
-  (void)bound;
-  // lam_max stays the exact bound 12 of the spectrum of -Delta: an estimate a
-  // little below the true top would let T_m amplify the highest eigenvectors
   ProbState& S = ps[p];
+  const double b = bound[p];
+  double lmax = fmax(y1, b);
+  if (!(lmax > 0.0) || lmax > 12.0) lmax = 12.0;  // NaN or beyond the exact bound
+  S.lam_max = lmax;
+  const double cut = exp(y0) * margin;
   S.lam_cut = fmin(fmax(cut, 1e-3), S.lam_max - 1e-3);
-  out_deg[p] = (int)lrint(fmin(64.0, fmax(8.0, y2)));
+  out_deg[p] = isfinite(y2) ? (int)lrint(fmin(64.0, fmax(8.0, y2))) : 64;
 }
 
 // Standardise features with the model's mean/std.
@@ -356,13 +359,13 @@ int features(const ProbDesc* pd, int np, const double2* U64, const double* plaq,
 }
 
 int window_infer(const ProbDesc* pd, ProbState* ps, int np, const float* feats, const float* model, float* work,
-                 const double* bound, int* out_deg, cudaStream_t st) {
+                 const double* bound, int* out_deg, double margin, cudaStream_t st) {
   // model = [params | norm(16 mean, 16 std, 3 mean, 3 std)]
   float* X = work;
   float* O = work + (size_t)np * kMlpIn;
   k_standardise<<<ceil_div((long long)np * kMlpIn, 256), 256, 0, st>>>(feats, model + kMlpParams, np, X);
   LAPH_TRY(mlp_forward(model, X, np, nullptr, nullptr, O, st));
-  k_window_apply<<<ceil_div(np, 128), 128, 0, st>>>(pd, ps, np, O, model + kMlpParams, bound, out_deg);
+  k_window_apply<<<ceil_div(np, 128), 128, 0, st>>>(pd, ps, np, O, model + kMlpParams, bound, out_deg, margin);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

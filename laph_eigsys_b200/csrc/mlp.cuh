@@ -12,7 +12,10 @@ int mlp_forward(const float* P, const float* X, int n, float* H1, float* H2, flo
 int features(const ProbDesc* pd, int np, const double2* U64, const double* plaq, double2* scratch, float* feats,
              double* bound, cudaStream_t st);
 // model = params (kMlpParams) followed by the normalisation (kMlpNorm);
-// work >= np * (kMlpIn + kMlpOut) floats.
+// work >= np * (kMlpIn + kMlpOut) floats; margin scales the predicted cut.
 int window_infer(const ProbDesc* pd, ProbState* ps, int np, const float* feats, const float* model, float* work,
-                 const double* bound, int* out_deg, cudaStream_t st);
+                 const double* bound, int* out_deg, double margin, cudaStream_t st);
+// First-pass cut of the learned window = this x the predicted converged cut,
+// unless laph_solve_opts.window_margin says otherwise.
+constexpr double kWindowMargin = 1.4;
 }  // namespace laph

@@ -34,6 +34,7 @@
 #include "dense.cuh"
 #include "filter.cuh"
 #include "links.cuh"
+#include "loop.cuh"
 #include "mlp.cuh"
 #include "smear.cuh"
 #include "stencil64cols.cuh"
@@ -77,6 +78,8 @@ struct laph_solver {
   std::vector<int> links_set;
   std::vector<double> sp1, sp2;  // per-problem smearing parameters (opts' by default)
   std::vector<int> degs;  // filter degree of each pass of the last run
+  std::vector<double> lam_max0;  // top of the first pass's window, per problem
+  std::vector<int> fallback;     // learned first window failed its check, per problem
   double ms[4] = {0, 0, 0, 0};
   long long cnt[3] = {0, 0, 0};
   // algorithmic bytes of the filter passes of the last run: [0] what the
@@ -98,6 +101,17 @@ struct laph_solver {
   // the Rayleigh-Ritz pass, captured on first use and replayed
   std::map<int, cudaGraphExec_t> g_filter;
   cudaGraphExec_t g_rr = nullptr;
+  // device-side loop: the whole solve as one graph (setup, a WHILE node over
+  // the outer iteration with a SWITCH node per filter step, phase fix)
+  LoopState* ls = nullptr;
+  int* d_degs = nullptr;                           // degree of each pass
+  double* d_lam_max0 = nullptr;                    // first pass's lam_max per problem
+  int* d_fallback = nullptr;                       // learned window fell back, per problem
+  cudaGraphConditionalHandle* d_steps = nullptr;   // [mdeg] SWITCH handles of the filter steps
+  ProbState* d_ps0 = nullptr;                      // state every run starts from
+  cudaGraphExec_t g_solve = nullptr;
+  long long solve_setup_launches = 0;              // kernels of the graph outside the loop
+  int solve_graph_failed = 0;                      // capture refused: the host loop from then on
 };
 
 namespace {
@@ -150,12 +164,13 @@ int laph_solver_destroy(laph_solver* s) {
                   s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
                   s->phases, s->norms, s->d_nactive, s->model, s->feats, s->mwork, s->bound, s->plaq, s->wdeg,
-                  s->tstamp};
+                  s->tstamp, s->ls, s->d_degs, s->d_lam_max0, s->d_fallback, s->d_steps, s->d_ps0};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->h_nactive) cudaFreeHost(s->h_nactive);
   for (auto& kv : s->g_filter) cudaGraphExecDestroy(kv.second);
   if (s->g_rr) cudaGraphExecDestroy(s->g_rr);
+  if (s->g_solve) cudaGraphExecDestroy(s->g_solve);
   for (auto e : s->evf) cudaEventDestroy(e);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
@@ -274,7 +289,10 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
       (rc = dalloc(&s->d_nactive, 1)) || (rc = dalloc(&s->model, kMlpParams + kMlpNorm)) ||
       (rc = dalloc(&s->feats, (size_t)n * kMlpIn)) || (rc = dalloc(&s->mwork, (size_t)n * (kMlpIn + kMlpOut))) ||
       (rc = dalloc(&s->bound, n)) || (rc = dalloc(&s->plaq, 4 * (size_t)n)) || (rc = dalloc(&s->wdeg, n)) ||
-      (rc = dalloc(&s->tstamp, (size_t)n * kSmallPhases)))
+      (rc = dalloc(&s->tstamp, (size_t)n * kSmallPhases)) || (rc = dalloc(&s->ls, 1)) ||
+      (rc = dalloc(&s->d_degs, (size_t)opts->max_it + 2)) || (rc = dalloc(&s->d_lam_max0, n)) ||
+      (rc = dalloc(&s->d_fallback, n)) || (rc = dalloc(&s->d_steps, (size_t)s->mdeg + 1)) ||
+      (rc = dalloc(&s->d_ps0, n)))
     return fail(rc);
   if (opts->link_prec == LAPH_LINKS_BF16) {
     if ((rc = dalloc(reinterpret_cast<float2**>(&s->Ubf), (size_t)o_uf))) return fail(rc);  // 4 B per element
@@ -297,6 +315,19 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
   cudaEventCreate(&s->ev2);
+  {
+    // the state every run starts from (the spectrum of -Delta lies in [0, 12])
+    std::vector<ProbState> ps0(n, ProbState{});
+    for (auto& p : ps0) {
+      p.lam_max = opts->lam_max > 0.0 ? opts->lam_max : 12.0;
+      p.lam_cut = opts->lam_cut > 0.0 ? opts->lam_cut : 0.0;
+      p.active = 1;
+    }
+    if (cudaMemcpy(s->d_ps0, ps0.data(), n * sizeof(ProbState), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(LAPH_ECUDA);
+    }
+  }
   s->links_set.assign(n, 0);
   s->sp1.assign(n, opts->smear_p1);
   s->sp2.assign(n, opts->smear_p2);
@@ -347,6 +378,9 @@ int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout
 // one outer iteration at 32^3 x 64, but the extra filter steps cost more than
 // the Rayleigh-Ritz they save (20.3 against 21.0 timeslices/s).
 constexpr double kCapResid = 1e-2;
+// Largest wanted residual after the learned window's first pass that counts
+// as a working window (the random start block has residuals of order 1).
+constexpr double kWindowCheck = 0.2;
 
 static int iteration_rr(laph_solver* s, int first_iter) {
   const bool fixed = s->o.window == LAPH_WINDOW_FIXED && s->o.lam_cut > 0.0;
@@ -357,23 +391,25 @@ static int iteration_rr(laph_solver* s, int first_iter) {
                        s->o.jacobi_sweeps > 0 ? s->o.jacobi_sweeps : 2, s->tstamp, s->st));
   LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->KK, s->V, s->st));
   LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_res, s->np, s->nb_res, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
-  LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
+  LAPH_TRY(zero_int(s->d_nactive, s->st));
   LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
   return LAPH_OK;
 }
 
-static int filter(laph_solver* s, int m) {
-  LAPH_TRY(coef(s->d_pd, s->d_ps, s->np, s->theta, s->tcoef, s->scol, m, s->st));
+// Step n (1-based) of a filter pass; fin: the pass's last step (writes W).
+static int filter_step(laph_solver* s, int n, bool fin, cudaStream_t st) {
   const int bf = s->o.link_prec == LAPH_LINKS_BF16;
   const void* links = bf ? s->Ubf : static_cast<const void*>(s->Uf32);
-  for (int n = 1; n < m; ++n) {
-    const bool fin = (n == m - 1);
-    const float2* X = (n == 1) ? s->S : s->E[(n - 2) % 3];
-    const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
-    float2* Yo = s->E[(n - 1) % 3];
-    LAPH_TRY(cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo,
-                       s->V, s->W, s->tcoef, n, fin, s->o.filter_kernel, s->st));
-  }
+  const float2* X = (n == 1) ? s->S : s->E[(n - 2) % 3];
+  const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
+  float2* Yo = s->E[(n - 1) % 3];
+  return cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo, s->V,
+                   s->W, s->tcoef, n, fin, s->o.filter_kernel, st);
+}
+
+static int filter(laph_solver* s, int m) {
+  LAPH_TRY(coef(s->d_pd, s->d_ps, s->np, s->theta, s->tcoef, s->scol, m, nullptr, s->st));
+  for (int n = 1; n < m; ++n) LAPH_TRY(filter_step(s, n, n == m - 1, s->st));
   return LAPH_OK;
 }
 
@@ -420,21 +456,12 @@ static int rr_graph(laph_solver* s) {
   return LAPH_OK;
 }
 
-extern "C" {
-
-int laph_solver_run(laph_solver* s, laph_result* res) {
-  if (!s) {
-    set_error("null solver");
-    return LAPH_EINVAL;
-  }
-  for (int i = 0; i < s->np; ++i)
-    if (!s->links_set[i]) {
-      set_error("laph_solver_run: links of problem %d not set", i);
-      return LAPH_EINVAL;
-    }
-  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+// Everything a solve does before its first outer iteration: the pristine links
+// into the working copy, smearing, the filter links, the start state, the
+// features and the window (learned, Lanczos or fixed), the start block and its
+// residuals.  Queued on the solver's stream; counts its kernels in *nlaunch.
+static int solve_setup(laph_solver* s, bool device_loop, long long* nlaunch_out) {
   const laph_solve_opts& o = s->o;
-  LAPH_CUDA_TRY(cudaEventRecord(s->ev0, s->st));
   long long nlaunch = 0;
   LAPH_CUDA_TRY(cudaMemcpyAsync(s->U64, s->U64raw, s->hd.back().u64 * sizeof(double2) + 27 * sizeof(double2) * s->hd.back().V3,
                                 cudaMemcpyDeviceToDevice, s->st));
@@ -449,15 +476,8 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   }
   LAPH_TRY(pack_links(s->d_pd, s->st_site, s->np, s->nb_site, s->U64, s->Uf32, s->Ubf, s->scale,
                       o.link_prec == LAPH_LINKS_BF16, s->st));
-  // initial state
-  for (int i = 0; i < s->np; ++i) {
-    ProbState& p = s->hps[i];
-    p = ProbState{};
-    p.lam_max = o.lam_max > 0.0 ? o.lam_max : 12.0;  // spectrum of -Delta lies in [0, 12]
-    p.lam_cut = o.lam_cut > 0.0 ? o.lam_cut : 0.0;
-    p.active = 1;
-  }
-  LAPH_CUDA_TRY(cudaMemcpyAsync(s->d_ps, s->hps.data(), s->np * sizeof(ProbState), cudaMemcpyHostToDevice, s->st));
+  // initial state (lam_max = 12 or the fixed one, lam_cut, all active)
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->d_ps, s->d_ps0, s->np * sizeof(ProbState), cudaMemcpyDeviceToDevice, s->st));
   // per-timeslice features (plaquette moments + 10-step Lanczos); the learned
   // window sets the first pass's lam_cut and degree from them
   s->deg0 = 0;
@@ -471,15 +491,15 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     LAPH_TRY(features(s->d_pd, s->np, s->U64, s->plaq, s->W, s->feats, s->bound, s->st));
     nlaunch += 2;
     if (o.window == LAPH_WINDOW_MLP) {
-      if (!s->have_model) {
-        set_error("laph_solver_run: window = MLP but no model set (laph_solver_set_window_model)");
-        return LAPH_EINVAL;
+      const double margin = o.window_margin > 0.0 ? o.window_margin : kWindowMargin;
+      LAPH_TRY(window_infer(s->d_pd, s->d_ps, s->np, s->feats, s->model, s->mwork, s->bound, s->wdeg, margin,
+                            s->st));
+      if (!device_loop) {  // the device-side loop takes the largest degree on the device
+        std::vector<int> dg(s->np);
+        LAPH_CUDA_TRY(cudaMemcpyAsync(dg.data(), s->wdeg, s->np * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+        LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+        for (int d : dg) s->deg0 = std::max(s->deg0, d);
       }
-      LAPH_TRY(window_infer(s->d_pd, s->d_ps, s->np, s->feats, s->model, s->mwork, s->bound, s->wdeg, s->st));
-      std::vector<int> dg(s->np);
-      LAPH_CUDA_TRY(cudaMemcpyAsync(dg.data(), s->wdeg, s->np * sizeof(int), cudaMemcpyDeviceToHost, s->st));
-      LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
-      for (int d : dg) s->deg0 = std::max(s->deg0, d);
       nlaunch += 3;
     }
   }
@@ -489,20 +509,255 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   const bool window_known = o.window == LAPH_WINDOW_MLP || (o.window == LAPH_WINDOW_FIXED && o.lam_cut > 0.0);
   if (window_known) {
     LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->V, o.seed, s->st));
-    LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
+    if (!device_loop) LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
     LAPH_TRY(start_window(s->d_pd, s->d_ps, s->np, s->theta, s->st));
     LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_res, s->np, s->nb_res, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
-    LAPH_CUDA_TRY(cudaMemsetAsync(s->d_nactive, 0, sizeof(int), s->st));
+    LAPH_TRY(zero_int(s->d_nactive, s->st));
     LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
-    nlaunch += 2 + 4;  // pack, random block, window state, residual, check
+    nlaunch += 2 + 5;  // pack, random block, window state, residual, zero, check
   } else {
     LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->W, o.seed, s->st));
-    LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
+    if (!device_loop) LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
     LAPH_TRY(iteration_rr(s, 1));
-    nlaunch += 2 + 7;  // pack, random block, first Rayleigh-Ritz
+    nlaunch += 2 + 8;  // pack, random block, first Rayleigh-Ritz
   }
+  *nlaunch_out = nlaunch;
+  return LAPH_OK;
+}
+
+// Per-problem results of the last run from the host copy of the states.
+static int fill_results(laph_solver* s, laph_result* res) {
+  const laph_solve_opts& o = s->o;
+  int status = LAPH_OK;
+  for (int i = 0; i < s->np; ++i) {
+    const ProbState& p = s->hps[i];
+    if (p.active) status = LAPH_ENOTCONV;
+    if (res) {
+      laph_result& r = res[i];
+      r.status = p.active ? LAPH_ENOTCONV : LAPH_OK;
+      r.iters = p.iters;
+      r.nconv = p.nconv;
+      r.deg = s->mdeg;
+      r.lam_cut0 = o.lam_cut;
+      r.lam_max = s->lam_max0[i];
+      r.window_fallback = s->fallback[i];
+      r.max_resid = p.max_resid;
+      std::vector<double> nv(s->hd[i].nev);
+      cudaMemcpy(nv.data(), s->norms + s->hd[i].kv, nv.size() * sizeof(double), cudaMemcpyDeviceToHost);
+      double tr = 0.0;
+      for (double v : nv) tr += v;
+      r.trace_vdv = tr;
+    }
+  }
+  if (status != LAPH_OK) set_error("laph_solver_run: max_it = %d reached before all problems converged", o.max_it);
+  return status;
+}
+
+// ------------------------------------------------------ device-side loop ---
+// The whole solve as one executable graph:
+//   setup (solve_setup) -> loop_init -> loop_cond
+//   WHILE (any problem active and it < max_it):
+//       loop_pass_begin (degree, the learned window's check, counters, step switches)
+//       coef (degree read on the device)
+//       SWITCH per filter step n = 1..mdeg-1: {plain step n | last step n | nothing}
+//       loop_pass_end, Rayleigh-Ritz + residuals + convergence mask, loop_cond
+//   loop_end -> phase fix
+// so no host round trip separates the passes (the host loop reads the mask
+// once per pass).  Built by stream capture into the graph and its bodies.
+
+// Capture `body` on the solver's stream into `g` after the nodes `deps`;
+// on return `deps` holds the leaf nodes of the capture.
+template <typename F>
+static int capture_into(laph_solver* s, cudaGraph_t g, std::vector<cudaGraphNode_t>& deps, F body) {
+  LAPH_CUDA_TRY(cudaStreamBeginCaptureToGraph(s->st, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                              cudaStreamCaptureModeThreadLocal));
+  int rc = body();
+  if (rc == LAPH_OK) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* d = nullptr;
+    size_t nd = 0;
+    const cudaError_t e = cudaStreamGetCaptureInfo(s->st, &cs, nullptr, nullptr, &d, &nd);
+    if (e != cudaSuccess || cs != cudaStreamCaptureStatusActive) {
+      set_error("graph capture: %s", cudaGetErrorString(e));
+      rc = LAPH_ECUDA;
+    } else {
+      deps.assign(d, d + nd);
+    }
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s->st, &out);
+  if (rc == LAPH_OK && e != cudaSuccess) {
+    set_error("graph capture: %s", cudaGetErrorString(e));
+    rc = LAPH_ECUDA;
+  }
+  return rc;
+}
+
+// A conditional node after `deps` in g; its body graphs go to bodies[0..size).
+static int add_conditional(cudaGraph_t g, std::vector<cudaGraphNode_t>& deps, cudaGraphConditionalHandle h,
+                           cudaGraphConditionalNodeType type, unsigned size, cudaGraph_t* bodies) {
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = type;
+  np.conditional.size = size;
+  cudaGraphNode_t node;
+  LAPH_CUDA_TRY(cudaGraphAddNode(&node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &np));
+  for (unsigned i = 0; i < size; ++i) bodies[i] = np.conditional.phGraph_out[i];
+  deps.assign(1, node);
+  return LAPH_OK;
+}
+
+static int build_solve_graph(laph_solver* s) {
+  const laph_solve_opts& o = s->o;
+  cudaGraph_t g = nullptr;
+  LAPH_CUDA_TRY(cudaGraphCreate(&g, 0));
+  auto done = [&](int rc) {
+    cudaGraphDestroy(g);
+    return rc;
+  };
+  cudaGraphConditionalHandle h_loop;
+  if (cudaGraphConditionalHandleCreate(&h_loop, g, 0, 0) != cudaSuccess) {
+    set_error("conditional graph nodes not available");
+    return done(LAPH_ECUDA);
+  }
+  LoopParams lp{};
+  lp.mdeg = s->mdeg;
+  lp.max_it = o.max_it;
+  lp.kb = s->kb;
+  lp.mlp = o.window == LAPH_WINDOW_MLP;
+  lp.lbytes = o.link_prec == LAPH_LINKS_BF16 ? 112.0 : 216.0;
+  lp.lam_top = o.lam_max > 0.0 ? o.lam_max : 12.0;
+  lp.cap_resid = kCapResid;
+  lp.win_check = kWindowCheck;
+  long long nsetup = 0;
+  std::vector<cudaGraphNode_t> deps;
+  int rc = capture_into(s, g, deps, [&]() -> int {
+    LAPH_TRY(loop_stamp(&s->ls->t_start, s->st));
+    LAPH_TRY(solve_setup(s, true, &nsetup));
+    LAPH_CUDA_TRY(cudaMemsetAsync(s->d_fallback, 0, sizeof(int) * s->np, s->st));
+    LAPH_TRY(loop_init(s->ls, o.window == LAPH_WINDOW_MLP ? s->wdeg : nullptr, s->np, s->st));
+    return loop_cond(s->ls, s->d_nactive, o.max_it, h_loop, s->st);
+  });
+  if (rc != LAPH_OK) return done(rc);
+  cudaGraph_t body;
+  if ((rc = add_conditional(g, deps, h_loop, cudaGraphCondTypeWhile, 1, &body)) != LAPH_OK) return done(rc);
+  std::vector<cudaGraphNode_t> top = deps;  // the WHILE node
+  // the pass: one SWITCH handle per filter step position
+  std::vector<cudaGraphConditionalHandle> hs(s->mdeg + 1, 0);
+  for (int n = 1; n < s->mdeg; ++n)
+    if (cudaGraphConditionalHandleCreate(&hs[n], body, 2, 0) != cudaSuccess) {
+      set_error("conditional graph nodes not available");
+      return done(LAPH_ECUDA);
+    }
+  if (cudaMemcpy(s->d_steps, hs.data(), hs.size() * sizeof(hs[0]), cudaMemcpyHostToDevice) != cudaSuccess)
+    return done(LAPH_ECUDA);
+  std::vector<cudaGraphNode_t> bd;
+  rc = capture_into(s, body, bd, [&]() -> int {
+    LAPH_TRY(loop_pass_begin(s->d_pd, s->d_ps, s->np, s->ls, s->d_degs, s->d_lam_max0, s->d_fallback, s->d_steps,
+                             lp, s->st));
+    return coef(s->d_pd, s->d_ps, s->np, s->theta, s->tcoef, s->scol, 0, &s->ls->m, s->st);
+  });
+  if (rc != LAPH_OK) return done(rc);
+  for (int n = 1; n < s->mdeg; ++n) {
+    cudaGraph_t b[2];
+    if ((rc = add_conditional(body, bd, hs[n], cudaGraphCondTypeSwitch, 2, b)) != LAPH_OK) return done(rc);
+    for (int fin = 0; fin < 2; ++fin) {
+      std::vector<cudaGraphNode_t> none;
+      if ((rc = capture_into(s, b[fin], none, [&]() -> int { return filter_step(s, n, fin == 1, s->st); })) != LAPH_OK)
+        return done(rc);
+    }
+  }
+  rc = capture_into(s, body, bd, [&]() -> int {
+    LAPH_TRY(loop_pass_end(s->ls, s->st));
+    LAPH_TRY(iteration_rr(s, 0));
+    return loop_cond(s->ls, s->d_nactive, o.max_it, h_loop, s->st);
+  });
+  if (rc != LAPH_OK) return done(rc);
+  rc = capture_into(s, g, top, [&]() -> int {
+    LAPH_TRY(loop_end(s->ls, s->st));
+    return phase_fix(s->d_pd, s->st_col, s->np, s->nb_col, s->V, s->phases, s->norms, o.phase_fix, s->st);
+  });
+  if (rc != LAPH_OK) return done(rc);
+  const cudaError_t ei = cudaGraphInstantiate(&s->g_solve, g, 0);
+  if (ei != cudaSuccess) {
+    s->g_solve = nullptr;
+    set_error("solve graph instantiation failed: %s", cudaGetErrorString(ei));
+    return done(LAPH_ECUDA);
+  }
+  // kernels outside the loop: stamp, setup, loop_init, loop_cond, loop_end, phase fix
+  s->solve_setup_launches = 1 + nsetup + 2 + 2;
+  return done(LAPH_OK);
+}
+
+static int run_device_loop(laph_solver* s, laph_result* res) {
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev0, s->st));
+  LAPH_CUDA_TRY(cudaGraphLaunch(s->g_solve, s->st));
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev2, s->st));
+  LoopState ls;
+  LAPH_CUDA_TRY(cudaMemcpyAsync(&ls, s->ls, sizeof ls, cudaMemcpyDeviceToHost, s->st));
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->hps.data(), s->d_ps, s->np * sizeof(ProbState), cudaMemcpyDeviceToHost, s->st));
+  s->lam_max0.assign(s->np, 0.0);
+  s->fallback.assign(s->np, 0);
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->lam_max0.data(), s->d_lam_max0, s->np * sizeof(double), cudaMemcpyDeviceToHost,
+                                s->st));
+  LAPH_CUDA_TRY(cudaMemcpyAsync(s->fallback.data(), s->d_fallback, s->np * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  s->degs.assign(std::max(ls.npass, 0), 0);
+  if (ls.npass > 0)
+    LAPH_CUDA_TRY(cudaMemcpy(s->degs.data(), s->d_degs, ls.npass * sizeof(int), cudaMemcpyDeviceToHost));
+  float b = 0.f;
+  cudaEventElapsedTime(&b, s->ev0, s->ev2);
+  s->ms[0] = 1e-6 * (double)(ls.t_loop - ls.t_start);
+  s->ms[1] = 1e-6 * ls.filt_ns;
+  s->ms[3] = b;
+  s->ms[2] = b - s->ms[0] - s->ms[1];
+  long long fl = 0;
+  for (int m : s->degs) fl += m - 1;
+  s->cnt[0] = (long long)ls.sv_steps;
+  s->cnt[1] = fl;
+  // per pass: loop_pass_begin, coef, the m - 1 steps, loop_pass_end, 8 Rayleigh-Ritz kernels, loop_cond
+  s->cnt[2] = s->solve_setup_launches + 12LL * ls.npass + fl;
+  s->fbytes[0] = ls.fbytes[0];
+  s->fbytes[1] = ls.fbytes[1];
+  s->ran = 1;
+  return fill_results(s, res);
+}
+extern "C" {
+
+int laph_solver_run(laph_solver* s, laph_result* res) {
+  if (!s) {
+    set_error("null solver");
+    return LAPH_EINVAL;
+  }
+  for (int i = 0; i < s->np; ++i)
+    if (!s->links_set[i]) {
+      set_error("laph_solver_run: links of problem %d not set", i);
+      return LAPH_EINVAL;
+    }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  const laph_solve_opts& o = s->o;
+  if (o.window == LAPH_WINDOW_MLP && !s->have_model) {
+    set_error("laph_solver_run: window = MLP but no model set (laph_solver_set_window_model)");
+    return LAPH_EINVAL;
+  }
+  const char* tr_env = std::getenv("LAPH_TRACE");
+  const bool trace = tr_env && *tr_env && *tr_env != '0';
+  if (!trace && !o.host_loop && !s->solve_graph_failed) {
+    if (!s->g_solve && build_solve_graph(s) != LAPH_OK) {
+      // conditional graph nodes refused (driver or runtime too old): the host loop from here on
+      s->solve_graph_failed = 1;
+      cudaGetLastError();
+    }
+    if (s->g_solve) return run_device_loop(s, res);
+  }
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev0, s->st));
+  long long nlaunch = 0;
+  LAPH_TRY(solve_setup(s, false, &nlaunch));
   s->cnt[0] = s->cnt[1] = s->cnt[2] = 0;
   s->fbytes[0] = s->fbytes[1] = 0.0;
+  s->fallback.assign(s->np, 0);
+  s->lam_max0.assign(s->np, 0.0);
   s->degs.clear();
   double filt_ms = 0.0;
   if (s->evf.empty()) {
@@ -510,8 +765,6 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     cudaEventCreate(&s->evf[0]);
     cudaEventCreate(&s->evf[1]);
   }
-  const char* tr_env = std::getenv("LAPH_TRACE");
-  const bool trace = tr_env && *tr_env && *tr_env != '0';
   if (trace) LAPH_CUDA_TRY(cudaMemsetAsync(s->tstamp, 0, (size_t)s->np * kSmallPhases * sizeof(unsigned long long), s->st));
   int it = 1;
   for (; it < o.max_it; ++it) {
@@ -549,6 +802,34 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
                        "sort+C %.0f window %.0f\n",
                        it, ph[0] / cnt, ph[1] / cnt, ph[2] / cnt, ph[3] / cnt, ph[4] / cnt, ph[5] / cnt);
       }
+    }
+    if (it == 1) {
+      s->lam_max0.resize(s->np);
+      for (int i = 0; i < s->np; ++i) s->lam_max0[i] = s->hps[i].lam_max;
+    }
+    // The learned window's check, after its first pass and Rayleigh-Ritz: a
+    // problem whose wanted residuals did not fall below kWindowCheck, whose
+    // Cholesky needed a clamped pivot or whose state is not finite goes on as
+    // the non-learned method would (lam_max back to the exact bound 12, the
+    // cut from its Ritz values).
+    if (it == 2 && o.window == LAPH_WINDOW_MLP) {
+      bool any = false;
+      for (int i = 0; i < s->np; ++i) {
+        ProbState& p = s->hps[i];
+        if (!p.active || (p.max_resid < kWindowCheck && !p.chol_fail && std::isfinite(p.lam_cut))) continue;
+        s->fallback[i] = 1;
+        any = true;
+        const double top = o.lam_max > 0.0 ? o.lam_max : 12.0;
+        if (!(p.lam_max < top) && std::isfinite(p.lam_cut)) continue;  // window already the non-learned one
+        p.lam_max = top;
+        double cut = std::isfinite(p.lam_cut) ? p.lam_cut : 0.5 * top;
+        cut = std::min(std::max(cut, 1e-6), top - 1e-3);
+        p.lam_cut = cut;
+        p.c_hop = 2.0 / (top - cut);
+        p.c_diag = (top + cut - 12.0) / (top - cut);
+      }
+      if (any)
+        LAPH_CUDA_TRY(cudaMemcpyAsync(s->d_ps, s->hps.data(), s->np * sizeof(ProbState), cudaMemcpyHostToDevice, s->st));
     }
     if (*s->h_nactive == 0) break;
     // Degree of this pass.  While the Ritz vectors are still poor (largest
@@ -590,7 +871,7 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     LAPH_TRY(filter_graph(s, m));
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[1], s->st));
     LAPH_TRY(rr_graph(s));
-    nlaunch += 1 + (m - 1) + 7;
+    nlaunch += 1 + (m - 1) + 8;
     float f = 0.f;
     LAPH_CUDA_TRY(cudaEventSynchronize(s->evf[1]));
     LAPH_CUDA_TRY(cudaEventElapsedTime(&f, s->evf[0], s->evf[1]));
@@ -609,28 +890,7 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   s->ms[3] = b;
   s->ms[2] = b - a - filt_ms;
   s->ran = 1;
-  int status = LAPH_OK;
-  for (int i = 0; i < s->np; ++i) {
-    const ProbState& p = s->hps[i];
-    if (p.active) status = LAPH_ENOTCONV;
-    if (res) {
-      laph_result& r = res[i];
-      r.status = p.active ? LAPH_ENOTCONV : LAPH_OK;
-      r.iters = p.iters;
-      r.nconv = p.nconv;
-      r.deg = s->mdeg;
-      r.lam_cut0 = o.lam_cut;
-      r.lam_max = p.lam_max;
-      r.max_resid = p.max_resid;
-      std::vector<double> nv(s->hd[i].nev);
-      cudaMemcpy(nv.data(), s->norms + s->hd[i].kv, nv.size() * sizeof(double), cudaMemcpyDeviceToHost);
-      double tr = 0.0;
-      for (double v : nv) tr += v;
-      r.trace_vdv = tr;
-    }
-  }
-  if (status != LAPH_OK) set_error("laph_solver_run: max_it = %d reached before all problems converged", o.max_it);
-  return status;
+  return fill_results(s, res);
 }
 
 int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double* phases, int on_device) {
@@ -720,8 +980,14 @@ int laph_solver_set_smear(laph_solver* s, int i, double p1, double p2) {
     set_error("laph_solver_set_smear: bad argument");
     return LAPH_EINVAL;
   }
-  s->sp1[i] = p1;
-  s->sp2[i] = p2;
+  if (s->sp1[i] != p1 || s->sp2[i] != p2) {
+    s->sp1[i] = p1;
+    s->sp2[i] = p2;
+    if (s->g_solve) {  // its smearing launches carry the old parameters
+      cudaGraphExecDestroy(s->g_solve);
+      s->g_solve = nullptr;
+    }
+  }
   return LAPH_OK;
 }
 

@@ -1,0 +1,95 @@
+"""The whole solve as one graph launch (the default): its WHILE node repeats the
+outer iteration on the device, SWITCH nodes pick each pass's filter steps, and
+small kernels make the decisions the host loop makes between its graph
+launches (degree cap, the learned window's check, convergence).  Both loops
+must run the same kernels in the same order, so they give the same iterations
+and bitwise the same eigenpairs; an uneven batch (timeslices of different L
+and nev in one launch) is checked against the oracle's FP64 Krylov-Schur (the
+reference's EPSSolve on T_12(B), src/ev_ts.cpp:231-263) at 16^3 and 24^3."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import random_links
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(gpu, probs, links, **kw):
+    s = gpu.Solver(probs, **kw)
+    if kw.get("window") == gpu.WINDOW_MLP:
+        from laph_eigsys_b200 import window
+        window.set_model(s, window.load_model())
+    for i, U in enumerate(links):
+        s.set_links(i, U)
+    st, res = s.run()
+    out = dict(status=st, res=res, eig=[s.get(i) for i in range(len(probs))], counters=s.counters(),
+               fbytes=s.filter_bytes(), timings=s.timings())
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("window", ["lanczos", "mlp"])
+def test_device_loop_matches_host_loop(gpu, window):
+    probs = [(8, 20), (6, 12), (10, 30), (8, 20)]
+    links = [random_links(L, 0.35, 3100 + i) for i, (L, _) in enumerate(probs)]
+    kw = dict(smear_kind=gpu.SMEAR_STOUT, smear_p1=0.1, smear_iters=3, guard=16, tol=1e-10, deg=24, max_it=200,
+              window=gpu.WINDOW_MLP if window == "mlp" else gpu.WINDOW_LANCZOS)
+    dev = _solve(gpu, probs, links, host_loop=0, **kw)
+    host = _solve(gpu, probs, links, host_loop=1, **kw)
+    assert dev["status"] == 0 and host["status"] == 0
+    for a, b in zip(dev["res"], host["res"]):
+        assert a["iters"] == b["iters"] and a["nconv"] == b["nconv"]
+        assert a["window_fallback"] == b["window_fallback"]
+        assert a["lam_max"] == b["lam_max"]
+    for (ea, va, pa), (eb, vb, pb) in zip(dev["eig"], host["eig"]):
+        assert np.array_equal(ea, eb)
+        assert np.array_equal(va, vb)
+        assert np.array_equal(pa, pb)
+    assert dev["counters"][:2] == host["counters"][:2]
+    assert np.allclose(dev["fbytes"], host["fbytes"], rtol=1e-12)
+    t = dev["timings"]
+    assert t[1] > 0 and t[3] >= t[1] and t[0] > 0
+
+
+def test_device_loop_reports_not_converged_at_max_it(gpu):
+    L, nev = 8, 30
+    s = gpu.Solver([(L, nev)], guard=16, tol=1e-13, deg=8, max_it=3)
+    s.set_links(0, random_links(L, 0.4, 3200))
+    st, res = s.run()
+    assert st == gpu._lib.LAPH_ENOTCONV
+    assert res[0]["status"] == gpu._lib.LAPH_ENOTCONV and res[0]["iters"] <= 3
+    s.close()
+
+
+def test_uneven_batch_in_one_launch_matches_oracle_krylov_schur(gpu, orc):
+    """16^3 (nev 60) and 24^3 (nev 120) timeslices, APE 0.5 x 10 as the survey's mixed-volume configuration, in one
+    batch and one graph launch, each against the oracle's smearing + FP64 Krylov-Schur on T_12(B): eigenvalues
+    (Rayleigh quotients) to 1e-10 relative each, residuals at the tolerance, tr(V^dag V) = nev, and the nev-block
+    subspace to the residual over the gap."""
+    specs = [(16, 60, 1230, 0), (24, 120, 1231, 0), (16, 60, 1230, 1)]
+    links, probs = [], []
+    for L, nev, seed, t in specs:
+        conf = gpu.gauge_random(L, t + 1, 0.3, seed)
+        links.append(np.ascontiguousarray(conf[t, :, 1:4]))
+        probs.append((L, nev))
+    tol = 1e-11
+    out = _solve(gpu, probs, links, smear_kind=gpu.SMEAR_APE, smear_p1=0.5, smear_iters=10, guard=16, tol=tol,
+                 deg=48, max_it=300, window=gpu.WINDOW_LANCZOS)
+    assert out["status"] == 0
+    orc.set_threads(os.cpu_count() or 1)
+    for (L, nev), U, (ev, V, _) in zip(probs, links, out["eig"]):
+        Us = orc.smear_ape(U, L, 0.5, 10, 1)
+        lam = -ev
+        st, _, Vk, _, _, _ = orc.eps_solve(Us, L, 12.0, float(1.1 * lam[-1]), 12, nev, tol=1e-12, max_it=300)
+        assert st == 0
+        Vo, _ = orc.fix_phase(Vk)
+        r = orc.compare_eigensystems(Us, L, V, Vo)
+        print(L, nev, {k: r[k] for k in ("max_rel_eig", "max_resid_checked", "max_resid_oracle", "block_proj",
+                                           "max_vec_phase_fixed", "gap_min_isolated")})
+        assert r["max_rel_eig"] <= 1e-10
+        assert r["max_resid_checked"] <= tol * 1.01
+        assert abs(r["trace_vdv_checked"] - nev) <= 1e-9
+        # both blocks span the lowest nev eigenvectors to within their residuals over the gap after lambda_nev
+        assert r["block_proj"] <= 1e-6
