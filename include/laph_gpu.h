@@ -228,6 +228,16 @@ int laph_solver_run(laph_solver* s, laph_result* results);
 /* Fetch problem i: evals[nev] (reference convention, see top), evecs column-major
  * complex128 [3*V3][nev] (may be NULL), phases[nev] (may be NULL). */
 int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double* phases, int on_device);
+/* The same results without waiting: the copies are queued on a read-back
+ * stream of the solver and overlap whatever the solver does next (the next
+ * laph_solver_set_links / laph_solver_run), which waits only for the
+ * conversion of the eigenvectors out of the solver's block, not for the
+ * copies.  evals, evecs, phases: host buffers as for laph_solver_get (any may
+ * be NULL); page-locked memory makes the copies truly asynchronous.  They are
+ * complete after laph_solver_wait.  The first call allocates a device staging
+ * pool of sum(3 V3 nev) complex128 for the batch. */
+int laph_solver_get_async(laph_solver* s, int i, double* evals, double* evecs, double* phases);
+int laph_solver_wait(laph_solver* s);
 /* The CUDA stream (cudaStream_t) every kernel and copy of the solver runs on,
  * for callers that time or order work around laph_solver_run. */
 int laph_solver_stream(laph_solver* s, void** stream);

@@ -455,6 +455,17 @@ class Solver:
         check(lib.laph_solver_get(self._h, i, _ptr(evals), ctypes.c_void_p(evecs.ctypes.data) if evecs is not None
                                   else None, _ptr(phases), 0), "laph_solver_get")
 
+    def get_async(self, i, evals, evecs, phases):
+        """Queue problem i's results into caller-provided host arrays (pinned for overlap) on the solver's read-back
+        stream (laph_solver_get_async); they are complete after wait()."""
+        check(lib.laph_solver_get_async(self._h, i, _ptr(evals) if evals is not None else None,
+                                        ctypes.c_void_p(evecs.ctypes.data) if evecs is not None else None,
+                                        _ptr(phases) if phases is not None else None), "laph_solver_get_async")
+
+    def wait(self):
+        """Block until every queued read-back has landed (laph_solver_wait)."""
+        check(lib.laph_solver_wait(self._h), "laph_solver_wait")
+
     def timings(self):
         """Device ms of the last run: smearing + setup, filter, dense + FP64 stencils, total."""
         t = (ctypes.c_double * 4)()

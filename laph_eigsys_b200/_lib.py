@@ -100,6 +100,8 @@ _sig("laph_solver_set_links", c_int, c_void_p, c_int, c_void_p, c_int, c_int)
 _sig("laph_solver_run", c_int, c_void_p, P(laph_result))
 _sig("laph_solver_get", c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int)
 _sig("laph_solver_stream", c_int, c_void_p, P(c_void_p))
+_sig("laph_solver_get_async", c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p)
+_sig("laph_solver_wait", c_int, c_void_p)
 _sig("laph_solver_filter_bytes", c_int, c_void_p, P(c_double))
 _sig("laph_ctx_stream", c_int, c_void_p, P(c_void_p))
 _sig("laph_binary_version", c_int, P(c_int))

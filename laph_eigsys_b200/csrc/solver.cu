@@ -112,6 +112,16 @@ struct laph_solver {
   cudaGraphExec_t g_solve = nullptr;
   long long solve_setup_launches = 0;              // kernels of the graph outside the loop
   int solve_graph_failed = 0;                      // capture refused: the host loop from then on
+  // asynchronous read-back (laph_solver_get_async): its own stream and a device
+  // staging pool the runs never touch, so the copies of one run's results
+  // overlap the next run; a run waits only for the conversions out of V
+  cudaStream_t st_out = nullptr;
+  double2* out_vec = nullptr;   // reference-layout eigenvectors, sum of dim x nev
+  double* out_val = nullptr;    // eigenvalues (recover_spectrum sign) and phases, 2 x sum of nev
+  std::vector<size_t> out_off;  // per problem: offset of its block in out_vec
+  std::vector<size_t> out_voff; // per problem: offset of its 2 nev values in out_val
+  cudaEvent_t ev_run = nullptr, ev_conv = nullptr;
+  int conv_pending = 0;
 };
 
 namespace {
@@ -168,6 +178,12 @@ int laph_solver_destroy(laph_solver* s) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->h_nactive) cudaFreeHost(s->h_nactive);
+  if (s->st_out) cudaStreamSynchronize(s->st_out);
+  if (s->out_vec) cudaFree(s->out_vec);
+  if (s->out_val) cudaFree(s->out_val);
+  if (s->ev_run) cudaEventDestroy(s->ev_run);
+  if (s->ev_conv) cudaEventDestroy(s->ev_conv);
+  if (s->st_out) cudaStreamDestroy(s->st_out);
   for (auto& kv : s->g_filter) cudaGraphExecDestroy(kv.second);
   if (s->g_rr) cudaGraphExecDestroy(s->g_rr);
   if (s->g_solve) cudaGraphExecDestroy(s->g_solve);
@@ -741,6 +757,10 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     set_error("laph_solver_run: window = MLP but no model set (laph_solver_set_window_model)");
     return LAPH_EINVAL;
   }
+  if (s->conv_pending) {  // asynchronous read-backs still converting V: let them finish reading it
+    LAPH_CUDA_TRY(cudaStreamWaitEvent(s->st, s->ev_conv, 0));
+    s->conv_pending = 0;
+  }
   const char* tr_env = std::getenv("LAPH_TRACE");
   const bool trace = tr_env && *tr_env && *tr_env != '0';
   if (!trace && !o.host_loop && !s->solve_graph_failed) {
@@ -919,6 +939,73 @@ int laph_solver_get(laph_solver* s, int i, double* evals, double* evecs, double*
   }
   if (phases) LAPH_CUDA_TRY(cudaMemcpyAsync(phases, s->phases + d.kv, d.nev * sizeof(double), kd, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return LAPH_OK;
+}
+
+// Negate the Ritz values of one problem into the staging pool (the
+// eigenvalues of Delta, recover_spectrum's sign) and copy its phases beside them.
+__global__ void k_out_vals(const double* __restrict__ theta, const double* __restrict__ phases, int nev,
+                           double* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nev) return;
+  out[j] = -theta[j];
+  out[nev + j] = phases[j];
+}
+
+int laph_solver_get_async(laph_solver* s, int i, double* evals, double* evecs, double* phases) {
+  if (!s || i < 0 || i >= s->np || !s->ran) {
+    set_error("laph_solver_get_async: bad argument or solver not run");
+    return LAPH_EINVAL;
+  }
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  if (!s->st_out) {
+    size_t nvec = 0, nval = 0;
+    s->out_off.resize(s->np);
+    s->out_voff.resize(s->np);
+    for (int p = 0; p < s->np; ++p) {
+      s->out_off[p] = nvec;
+      s->out_voff[p] = nval;
+      nvec += (size_t)s->hd[p].dim * s->hd[p].nev;
+      nval += 2 * (size_t)s->hd[p].nev;
+    }
+    if (cudaStreamCreateWithFlags(&s->st_out, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_run, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_conv, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&s->out_vec, sizeof(double2) * nvec) != cudaSuccess ||
+        cudaMalloc(&s->out_val, sizeof(double) * nval) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("laph_solver_get_async: cannot set up the read-back stream and its %zu-byte staging pool",
+                sizeof(double2) * nvec);
+      return LAPH_ENOMEM;
+    }
+  }
+  const ProbDesc& d = s->hd[i];
+  double2* ov = s->out_vec + s->out_off[i];
+  double* oval = s->out_val + s->out_voff[i];
+  // everything queued on the compute stream so far (the run) before the conversions
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev_run, s->st));
+  LAPH_CUDA_TRY(cudaStreamWaitEvent(s->st_out, s->ev_run, 0));
+  if (evecs) LAPH_TRY(to_reference(s->V + d.blk, ov, d.V3, d.nev, s->st_out));
+  k_out_vals<<<ceil_div(d.nev, 128), 128, 0, s->st_out>>>(s->theta + d.kv, s->phases + d.kv, d.nev, oval);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev_conv, s->st_out));
+  s->conv_pending = 1;
+  if (evecs)
+    LAPH_CUDA_TRY(cudaMemcpyAsync(evecs, ov, sizeof(double2) * d.dim * d.nev, cudaMemcpyDeviceToHost, s->st_out));
+  if (evals) LAPH_CUDA_TRY(cudaMemcpyAsync(evals, oval, sizeof(double) * d.nev, cudaMemcpyDeviceToHost, s->st_out));
+  if (phases)
+    LAPH_CUDA_TRY(cudaMemcpyAsync(phases, oval + d.nev, sizeof(double) * d.nev, cudaMemcpyDeviceToHost, s->st_out));
+  return LAPH_OK;
+}
+
+int laph_solver_wait(laph_solver* s) {
+  if (!s) {
+    set_error("laph_solver_wait: null solver");
+    return LAPH_EINVAL;
+  }
+  if (!s->st_out) return LAPH_OK;
+  LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st_out));
   return LAPH_OK;
 }
 

@@ -93,3 +93,36 @@ def test_uneven_batch_in_one_launch_matches_oracle_krylov_schur(gpu, orc):
         assert abs(r["trace_vdv_checked"] - nev) <= 1e-9
         # both blocks span the lowest nev eigenvectors to within their residuals over the gap after lambda_nev
         assert r["block_proj"] <= 1e-6
+
+
+def test_async_read_back_overlaps_the_next_run(gpu):
+    """laph_solver_get_async queues each problem's results on the solver's read-back stream; the next run may start
+    at once (it waits only for the conversions out of the block) and the first run's results still land intact in
+    the host buffers, equal to what laph_solver_get returned for that run."""
+    import torch
+    probs = [(8, 20), (10, 30), (6, 12)]
+    s = gpu.Solver(probs, smear_kind=gpu.SMEAR_STOUT, smear_p1=0.1, smear_iters=2, guard=16, tol=1e-10, deg=24)
+    sets = [[random_links(L, 0.35, 3300 + 10 * k + i) for i, (L, _) in enumerate(probs)] for k in range(2)]
+    ref = []
+    for k in range(2):  # reference results of each link set, read synchronously
+        for i, U in enumerate(sets[k]):
+            s.set_links(i, U)
+        assert s.run()[0] == 0
+        ref.append([s.get(i) for i in range(len(probs))])
+    bufs = [[(torch.empty(nev, dtype=torch.float64, pin_memory=True).numpy(),
+              torch.empty((3 * L ** 3) * nev, dtype=torch.complex128, pin_memory=True).numpy(),
+              torch.empty(nev, dtype=torch.float64, pin_memory=True).numpy()) for L, nev in probs] for _ in range(2)]
+    for k in range(2):
+        for i, U in enumerate(sets[k]):
+            s.set_links(i, U)
+        assert s.run()[0] == 0
+        for i in range(len(probs)):
+            s.get_async(i, *bufs[k][i])
+    s.wait()
+    for k in range(2):
+        for i, (L, nev) in enumerate(probs):
+            ev, V, ph = ref[k][i]
+            e, v, p = bufs[k][i]
+            assert np.array_equal(e, ev) and np.array_equal(p, ph)
+            assert np.array_equal(v.reshape(nev, 3 * L ** 3).T, V)
+    s.close()
