@@ -629,8 +629,9 @@ def main():
     ap.add_argument("--no-io", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the learned-window A/B and the sub-records of the other survey configurations")
-    ap.add_argument("--autotune", type=int, default=0, metavar="NSAMPLE",
-                    help="tune deg / block / guard on the first NSAMPLE timeslices before measuring (0: off)")
+    ap.add_argument("--autotune", type=int, default=4, metavar="NSAMPLE",
+                    help="tune deg / block / guard on the first NSAMPLE timeslices before measuring (0: off, the "
+                         "configuration's own settings)")
     ap.add_argument("--tune-cache", default=None, help="autotuner cache file")
     ap.add_argument("--cpu-layout", default="omp", choices=["omp", "per-core"],
                     help="reference arm: OpenMP inside one timeslice (default) or one single-threaded timeslice per "

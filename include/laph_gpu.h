@@ -290,7 +290,7 @@ int laph_autotune_search(const int* deg_c, int nd, const int* block_c, int nb, c
  * setting that does not converge within opts->max_it is dropped.  model /
  * nmodel: the window model (as laph_solver_set_window_model) when
  * opts->window is LAPH_WINDOW_MLP, else ignored (may be NULL).  Candidates:
- * deg 40, 48, 56, 60, 64 (start: opts->deg, or 60 if <= 1), block 16, 32, 64
+ * deg 40, 48, 56, 60, 64 (start: opts->deg, or 60 if <= 1), block 8, 16, 32, 64
  * (start: opts->block, or 32), guard opts->guard and opts->guard + 32.
  * cache_path (may be NULL): a text file of earlier results, one line per
  * device and batch shape; a hit sets opts without timing anything, a new

@@ -462,6 +462,14 @@ class Solver:
                                         ctypes.c_void_p(evecs.ctypes.data) if evecs is not None else None,
                                         _ptr(phases) if phases is not None else None), "laph_solver_get_async")
 
+    def ritz(self, i):
+        """All k Ritz values of problem i's block after the last run (the nev wanted ones and the guard), ascending
+        (laph_solver_ritz)."""
+        th = np.empty(512)
+        k = ctypes.c_int()
+        check(lib.laph_solver_ritz(self._h, i, _ptr(th), ctypes.byref(k)), "laph_solver_ritz")
+        return np.sort(th[:k.value])
+
     def wait(self):
         """Block until every queued read-back has landed (laph_solver_wait)."""
         check(lib.laph_solver_wait(self._h), "laph_solver_wait")

@@ -208,10 +208,10 @@ int laph_solver_autotune(const laph_problem* probs, int n, const double* const* 
   const int block0 = opts->block > 0 ? opts->block : 32;
   const int guard0 = opts->guard;
   const int degs[] = {40, 48, 56, 60, 64};
-  const int blocks[] = {16, 32, 64};
+  const int blocks[] = {8, 16, 32, 64};
   const int guards[] = {guard0, guard0 + 32};
   SampleCtx ctx{probs, ns, links, layout, *opts, model, nmodel, device, LAPH_OK};
-  int st = laph_autotune_search(degs, 5, blocks, 3, guards, 2, deg0, block0, guard0, sample_trial, &ctx, out);
+  int st = laph_autotune_search(degs, 5, blocks, 4, guards, 2, deg0, block0, guard0, sample_trial, &ctx, out);
   if (st != LAPH_OK) {
     if (ctx.last_status != LAPH_OK && ctx.last_status != LAPH_ENOTCONV)
       set_error("laph_solver_autotune: every setting failed; the last with status %d (%s)", ctx.last_status,

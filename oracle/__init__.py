@@ -262,14 +262,16 @@ def _subspace_distance(A, B):
     return float(np.linalg.norm(A - B @ (B.conj().T @ A), 2))
 
 
-def compare_eigensystems(U, L, Va, Vb, lam_max=12.0, gap=1e-3):
+def compare_eigensystems(U, L, Va, Vb, lam_max=12.0, gap=1e-3, lam_next=None):
     """Eigenpair parity of two eigensystems Va (the one checked) and Vb (the oracle's) of -Delta on links U, both
     (dim, nev) column-major with the reference's phase fix applied (fix_phase).  Eigenvalues are compared as FP64
     Rayleigh quotients on -Delta, each relative to itself (where lambda > 1e-12 lambda_max) and relative to
     lambda_max; eigenvectors one by one where the eigenvalue is isolated (no neighbour within `gap`, absolute, in
     units of lambda), and by subspace distance (sin of the largest principal angle) on clusters of eigenvalues
     closer than `gap`.  `gap_min` is the smallest separation of an isolated eigenvalue: an eigenvector with residual
-    r is determined to about r / gap_min, which bounds what any two solvers can agree to."""
+    r is determined to about r / gap_min, which bounds what any two solvers can agree to.  lam_next: the next
+    eigenvalue beyond the block, where known; a last cluster that it joins is cut by the block boundary, so the two
+    blocks may hold different vectors of it, and it is left out of the vector comparison (boundary_cut)."""
     la, ra = rayleigh(U, L, Va)
     lb, rb = rayleigh(U, L, Vb)
     ia, ib = np.argsort(la), np.argsort(lb)
@@ -291,12 +293,17 @@ def compare_eigensystems(U, L, Va, Vb, lam_max=12.0, gap=1e-3):
             cur = [j]
     cl.append(cur)
     vec, vec_al, proj, gmin = 0.0, 0.0, 0.0, np.inf
+    cut = lam_next is not None and lam_next - lb[-1] < gap
+    if cut:
+        cl = cl[:-1]
     for c in cl:
         if len(c) == 1:
             j = c[0]
             g = lb[j] - lb[j - 1] if j > 0 else np.inf
             if j + 1 < len(lb):
                 g = min(g, lb[j + 1] - lb[j])
+            elif lam_next is not None:
+                g = min(g, lam_next - lb[j])
             gmin = min(gmin, g)
             a, b = Va[:, j], Vb[:, j]
             vec = max(vec, float(np.linalg.norm(a - b)))
@@ -307,5 +314,5 @@ def compare_eigensystems(U, L, Va, Vb, lam_max=12.0, gap=1e-3):
     out.update({"clusters": int(sum(len(c) > 1 for c in cl)), "in_clusters": int(sum(len(c) for c in cl if len(c) > 1)),
                 "max_vec_phase_fixed": vec, "max_vec_aligned": vec_al, "max_cluster_proj": proj,
                 "gap_min_isolated": float(gmin) if np.isfinite(gmin) else None,
-                "block_proj": _subspace_distance(Va, Vb), "cluster_gap": gap})
+                "block_proj": _subspace_distance(Va, Vb), "cluster_gap": gap, "boundary_cut": bool(cut)})
     return out
