@@ -88,6 +88,10 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
 #pragma unroll
     for (int j = 0; j < 4; ++j) accr[i][j][0] = accr[i][j][1] = acci[i][j][0] = acci[i][j][1] = 0.0;
   const int nstep = (r1 - r0 + GK - 1) / GK;
+  // On a diagonal tile pair (ti == tj) the reduction keeps only the upper
+  // triangle (G and H are Hermitian), so the 8x8 MMA tiles below the diagonal
+  // are skipped: 10 of 16 per warp.
+  const bool diag = ti == tj;
   load(r0, 0);
   for (int it = 0; it < nstep; ++it) {
     const int b = it & 1;
@@ -121,6 +125,7 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
+          if (diag && i > j) continue;  // below the diagonal of a diagonal tile: never read
           dmma884(accr[i][j], wr[i], br[j]);
           dmma884(accr[i][j], wi[i], bi[j]);
           dmma884(acci[i][j], wr[i], bi[j]);
@@ -134,10 +139,12 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < 4; ++j) {
+      if (diag && i > j) continue;
 #pragma unroll
       for (int e = 0; e < 2; ++e)
         o[(8 * i + fr) * GT + 8 * j + 2 * fk + e] = make_double2(accr[i][j][e], acci[i][j][e]);
+    }
 }
 
 

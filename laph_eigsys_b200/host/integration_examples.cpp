@@ -168,3 +168,16 @@ for (int i = 0; i < ngrid; ++i) {
 laph_solver_run(s, results);
   return 0;
 }
+
+// ---- guide block: streaming several configurations with overlapped read-back
+int example_streaming(laph_solver* s, laph_result* results, double* const* configs, int nconf, int todo, int V_TS,
+                      double* const* const* ev_buf, double* const* const* vec_buf, double* const* const* ph_buf) {
+  for (int c = 0; c < nconf; ++c) {
+    for (int ts = 0; ts < todo; ++ts) laph_solver_set_links(s, ts, configs[c] + ts * V_TS, LAPH_LAYOUT_CONF, 0);
+    laph_solver_run(s, results);
+    for (int ts = 0; ts < todo; ++ts)   // buffers of configuration c, page-locked (cudaHostAlloc)
+      laph_solver_get_async(s, ts, ev_buf[c][ts], vec_buf[c][ts], ph_buf[c][ts]);
+  }
+  laph_solver_wait(s);                  // every queued copy has landed
+  return 0;
+}
