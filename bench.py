@@ -168,6 +168,7 @@ def make_opts(cfg):
                          link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
                          max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
                          filter_kernel=cfg.get("filter_kernel", 1), jacobi_sweeps=cfg.get("sweeps", 0),
+                         filter_tile=cfg.get("tile", 0),
                          lam_cut=cfg.get("lam_cut0", 0.0),
                          window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
                              cfg.get("window", "mlp")])
@@ -186,8 +187,9 @@ def autotune_cfg(cfg, batch, device, nsample, cache):
                             opts=make_opts(cfg), model=model, device=device, cache=cache)
     res["seconds"] = time.perf_counter() - t0
     res["sample_timeslices"] = min(nsample, len(batch))
-    res["before"] = {"deg": cfg["deg"], "block": cfg.get("block", 0) or 32, "guard": cfg["guard"]}
-    cfg["deg"], cfg["block"], cfg["guard"] = opts.deg, opts.block, opts.guard
+    res["before"] = {"deg": cfg["deg"], "block": cfg.get("block", 0) or 32, "guard": cfg["guard"],
+                     "tile": cfg.get("tile", 0) or 128}
+    cfg["deg"], cfg["block"], cfg["guard"], cfg["tile"] = opts.deg, opts.block, opts.guard, opts.filter_tile
     return res
 
 
@@ -445,6 +447,7 @@ def workload_config(cfg):
     return {"workload": f"{shape}, eps {cfg['eps']} {cfg['smear']} {cfg['iters']}x{cfg['p1']}, "
                         f"+{cfg['guard']} guard, resid<=1e-9",
             "L": cfg["L"], "timeslices": cfg["T"], "nev": cfg["nev"], "guard": cfg["guard"], "deg": cfg["deg"],
+            "block": cfg.get("block") or 32, "tile": cfg.get("tile") or 128,
             "window": cfg.get("window", "mlp"),
             "links": cfg["link_prec"], "filter": "fp32", "rayleigh_ritz": "fp64",
             "l2": "inputs larger than L2 (each 64-timeslice block of vectors is 8 GB)"}

@@ -197,6 +197,8 @@ typedef struct {
                            filter graph and one Rayleigh-Ritz graph per pass,
                            the convergence mask read each pass), also taken
                            with LAPH_TRACE set                                   */
+  int filter_tile;      /* sites per CTA of the filter (64, 128 or 256; 0: 128);
+                           laph_solver_autotune picks it                        */
 } laph_solve_opts;
 void laph_solve_opts_default(laph_solve_opts* o);
 
@@ -274,6 +276,7 @@ typedef struct {
   double ms_per_problem;   /* device time per problem with them, on the sample   */
   int trials;              /* settings timed (0 when read from the cache)        */
   int from_cache;          /* 1: taken from the cache file, nothing timed        */
+  int tile;                /* filter sites per CTA (laph_solver_autotune only)    */
 } laph_tune_result;
 /* One trial: device ms per problem of the setting, or < 0 if it failed. */
 typedef double (*laph_tune_trial)(void* user, int deg, int block, int guard);
@@ -291,7 +294,9 @@ int laph_autotune_search(const int* deg_c, int nd, const int* block_c, int nb, c
  * nmodel: the window model (as laph_solver_set_window_model) when
  * opts->window is LAPH_WINDOW_MLP, else ignored (may be NULL).  Candidates:
  * deg 40, 48, 56, 60, 64 (start: opts->deg, or 60 if <= 1), block 8, 16, 32, 64
- * (start: opts->block, or 32), guard opts->guard and opts->guard + 32.
+ * (start: opts->block, or 32), guard opts->guard and opts->guard + 32, then the
+ * filter's tile of 64, 128 or 256 sites per CTA (start: opts->filter_tile, or
+ * 128) with the other three at their best.
  * cache_path (may be NULL): a text file of earlier results, one line per
  * device and batch shape; a hit sets opts without timing anything, a new
  * result is appended. */

@@ -42,7 +42,7 @@ class laph_solve_opts(ctypes.Structure):
                 ("max_it", c_int), ("window", c_int), ("lam_cut", c_double), ("lam_max", c_double),
                 ("deg", c_int), ("phase_fix", c_int), ("seed", c_u64), ("block", c_int), ("filter_kernel", c_int),
                 ("jacobi_sweeps", c_int), ("window_margin", c_double),
-                ("host_loop", c_int)]
+                ("host_loop", c_int), ("filter_tile", c_int)]
 
 
 class laph_result(ctypes.Structure):
@@ -52,7 +52,7 @@ class laph_result(ctypes.Structure):
 
 class laph_tune_result(ctypes.Structure):
     _fields_ = [("deg", c_int), ("block", c_int), ("guard", c_int), ("ms_per_problem", c_double),
-                ("trials", c_int), ("from_cache", c_int)]
+                ("trials", c_int), ("from_cache", c_int), ("tile", c_int)]
 
 
 TUNE_TRIAL = ctypes.CFUNCTYPE(c_double, c_void_p, c_int, c_int, c_int)

@@ -6,6 +6,9 @@
 //   block  columns per CTA of the filter kernel (links read once per block)
 //   guard  vectors beyond nev, hence the block width k (faster convergence of
 //          the wanted pairs against more work per pass)
+//   tile   sites per CTA of the filter (64, 128, 256: the shared-memory share
+//          of the backward links and the prefetch run per CTA), tried last
+//          with the other three at their best
 //
 // laph_autotune_search walks them one axis at a time (deg, then block, then
 // guard; each candidate of an axis timed with the others at their best so far,
@@ -46,6 +49,7 @@ struct SampleCtx {
   int nmodel;
   int device;
   int last_status;
+  int tile;  // filter sites per CTA of the trials
 };
 
 // One setting: device milliseconds per problem of the faster of two runs, or -1.
@@ -55,6 +59,7 @@ double sample_trial(void* user, int deg, int block, int guard) {
   o.deg = deg;
   o.block = block;
   o.guard = guard;
+  o.filter_tile = c->tile;
   laph_solver* s = nullptr;
   int st = laph_solver_create(&s, c->probs, c->ns, &o, c->device);
   c->last_status = st;
@@ -93,7 +98,7 @@ std::string shape_key(const cudaDeviceProp& prop, const laph_problem* probs, int
   return k;
 }
 
-// "key<TAB>deg block guard ms" lines; the last line with the key wins.
+// "key<TAB>deg block guard ms [tile]" lines; the last line with the key wins.
 bool cache_lookup(const char* path, const std::string& key, laph_tune_result* r) {
   FILE* f = std::fopen(path, "r");
   if (!f) return false;
@@ -102,13 +107,15 @@ bool cache_lookup(const char* path, const std::string& key, laph_tune_result* r)
   while (std::fgets(line.data(), (int)line.size(), f)) {
     const char* tab = std::strchr(line.data(), '\t');
     if (!tab || std::string(line.data(), (size_t)(tab - line.data())) != key) continue;
-    int d = 0, b = 0, g = 0;
+    int d = 0, b = 0, g = 0, t = 0;
     double ms = 0.0;
-    if (std::sscanf(tab + 1, "%d %d %d %lf", &d, &b, &g, &ms) == 4) {
+    const int n = std::sscanf(tab + 1, "%d %d %d %lf %d", &d, &b, &g, &ms, &t);
+    if (n >= 4) {
       r->deg = d;
       r->block = b;
       r->guard = g;
       r->ms_per_problem = ms;
+      r->tile = n == 5 ? t : 128;
       found = true;
     }
   }
@@ -202,6 +209,7 @@ int laph_solver_autotune(const laph_problem* probs, int n, const double* const* 
     opts->deg = out->deg;
     opts->block = out->block;
     opts->guard = out->guard;
+    opts->filter_tile = out->tile;
     return LAPH_OK;
   }
   const int deg0 = opts->deg > 1 ? std::min(opts->deg, 64) : 60;
@@ -210,7 +218,8 @@ int laph_solver_autotune(const laph_problem* probs, int n, const double* const* 
   const int degs[] = {40, 48, 56, 60, 64};
   const int blocks[] = {8, 16, 32, 64};
   const int guards[] = {guard0, guard0 + 32};
-  SampleCtx ctx{probs, ns, links, layout, *opts, model, nmodel, device, LAPH_OK};
+  const int tile0 = opts->filter_tile > 0 ? opts->filter_tile : 128;
+  SampleCtx ctx{probs, ns, links, layout, *opts, model, nmodel, device, LAPH_OK, tile0};
   int st = laph_autotune_search(degs, 5, blocks, 4, guards, 2, deg0, block0, guard0, sample_trial, &ctx, out);
   if (st != LAPH_OK) {
     if (ctx.last_status != LAPH_OK && ctx.last_status != LAPH_ENOTCONV)
@@ -218,16 +227,33 @@ int laph_solver_autotune(const laph_problem* probs, int n, const double* const* 
                 laph_strerror(ctx.last_status));
     return st;
   }
+  // the tile axis, with deg / block / guard at their best (the kernel variant
+  // with FP32 coefficients per CTA only: wider blocks keep 128 sites)
+  out->tile = tile0;
+  if (opts->filter_kernel == 1 && out->block <= 64) {
+    for (int t : {64, 128, 256}) {
+      if (t == tile0) continue;
+      ctx.tile = t;
+      const double ms = sample_trial(&ctx, out->deg, out->block, out->guard);
+      ++out->trials;
+      if (ms > 0.0 && ms < (1.0 - kTuneMargin) * out->ms_per_problem) {
+        out->ms_per_problem = ms;
+        out->tile = t;
+      }
+    }
+  }
   opts->deg = out->deg;
   opts->block = out->block;
   opts->guard = out->guard;
+  opts->filter_tile = out->tile;
   if (cache_path && *cache_path) {
     FILE* f = std::fopen(cache_path, "a");
     if (!f) {
       set_error("laph_solver_autotune: cannot append to %s", cache_path);
       return LAPH_EIO;
     }
-    std::fprintf(f, "%s\t%d %d %d %.6f\n", key.c_str(), out->deg, out->block, out->guard, out->ms_per_problem);
+    std::fprintf(f, "%s\t%d %d %d %.6f %d\n", key.c_str(), out->deg, out->block, out->guard, out->ms_per_problem,
+                 out->tile);
     std::fclose(f);
   }
   return LAPH_OK;

@@ -235,8 +235,10 @@ struct ChebCol {
   float2 xu[3][3], xd[3][3], xs[3], ss[3], zz[3];
 };
 
-template <typename LT, bool HAS_Z, bool FINAL>
-__global__ void __launch_bounds__(128, 4)
+// NT sites (threads) per CTA, the tile the autotuner picks (64, 128 or 256);
+// 16 warps per SM at 128 registers whichever NT.
+template <typename LT, bool HAS_Z, bool FINAL, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
     k_cheb_mrhs2(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, const int* __restrict__ start,
                  int np, int kb, const LT* __restrict__ links, const float* __restrict__ scale,
                  const float2* __restrict__ Xp, const float2* __restrict__ Zp, const float2* __restrict__ Sp,
@@ -245,10 +247,10 @@ __global__ void __launch_bounds__(128, 4)
   const int p = find_prob(start, np, blockIdx.x);
   if (!ps[p].active) return;
   const ProbDesc d = pd[p];
-  const int nst = (d.V3 + 127) >> 7;
+  const int nst = (d.V3 + NT - 1) / NT;
   const int t = blockIdx.x - start[p];
   const int st = t % nst, cb = t / nst;
-  const int s = st * 128 + threadIdx.x;
+  const int s = st * NT + threadIdx.x;
   const bool valid = s < d.V3;
   const int j1 = min(cb * kb + kb, d.k);
   const int nlock = ps[p].nlock;
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(128, 4)
   {
     const double c_hop = ps[p].c_hop, c_diag = ps[p].c_diag;
     const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
-    for (int j = j0 + (int)threadIdx.x; j < j1; j += 128) {
+    for (int j = j0 + (int)threadIdx.x; j < j1; j += NT) {
       const double a = tc[j];
       cf[j - j0] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
       if (FINAL) ctm[j - j0] = tc[(size_t)3 * d.k + j];
@@ -286,9 +288,10 @@ __global__ void __launch_bounds__(128, 4)
   const LT* U = links + d.uf;
   const float* scl = scale + d.sc;
   // forward links in registers (54), backward links U_mu(s - mu) in shared
-  // memory, each thread reading only its own column of sUb (no sharing, no
-  // barrier): 128 registers instead of 168, so 4 CTAs (16 warps) per SM
-  __shared__ float2 sUb[27][128];
+  // memory (dynamic, 27 x NT float2), each thread reading only its own column
+  // of sUb (no sharing, no barrier): 128 registers instead of 168, 16 warps per SM
+  extern __shared__ float2 sUb_dyn[];
+  float2 (*sUb)[NT] = reinterpret_cast<float2 (*)[NT]>(sUb_dyn);
   float2 uf[3][9];
 #pragma unroll
   for (int mu = 0; mu < 3; ++mu)
@@ -300,7 +303,7 @@ __global__ void __launch_bounds__(128, 4)
       sUb[mu * 9 + e][threadIdx.x] = bwl;
     }
   const size_t base = (size_t)d.blk;
-  const int s0 = st * 128, nsite = min(128, d.V3 - s0);
+  const int s0 = st * NT, nsite = min(NT, d.V3 - s0);
   const bool pf = threadIdx.x == 0 && (nsite % 2 == 0) && (d.dim % 2 == 0);
   auto prefetch = [&](int j) {
     if (!pf || j >= j1) return;
@@ -465,27 +468,69 @@ int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const dou
   return LAPH_OK;
 }
 
+template <int NT>
+static void launch_cheb2(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
+                         const void* links, const float* scale, const float2* X, const float2* Z, const float2* S,
+                         float2* Y, const double2* V, double2* W, const double* tcoef, int step, bool final_step,
+                         cudaStream_t st) {
+  const bool hz = Z != nullptr;
+  const size_t smem = sizeof(float2) * 27 * NT;
+#define LAPH_CHEB2(LT, HZ, FIN)                                                                                   \
+  k_cheb_mrhs2<LT, HZ, FIN, NT><<<nblk, NT, smem, st>>>(pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), \
+                                                        scale, X, Z, S, Y, V, W, tcoef, step)
+  if (bf16) {
+    if (hz && final_step) LAPH_CHEB2(__nv_bfloat162, true, true);
+    else if (hz) LAPH_CHEB2(__nv_bfloat162, true, false);
+    else if (final_step) LAPH_CHEB2(__nv_bfloat162, false, true);
+    else LAPH_CHEB2(__nv_bfloat162, false, false);
+  } else {
+    if (hz && final_step) LAPH_CHEB2(float2, true, true);
+    else if (hz) LAPH_CHEB2(float2, true, false);
+    else if (final_step) LAPH_CHEB2(float2, false, true);
+    else LAPH_CHEB2(float2, false, false);
+  }
+#undef LAPH_CHEB2
+}
+
+template <int NT>
+static int cheb2_attributes() {
+  const int smem = (int)sizeof(float2) * 27 * NT;
+#define LAPH_ATTR(LT, HZ, FIN) \
+  LAPH_CUDA_TRY(cudaFuncSetAttribute(k_cheb_mrhs2<LT, HZ, FIN, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))
+  LAPH_ATTR(float2, true, true);
+  LAPH_ATTR(float2, true, false);
+  LAPH_ATTR(float2, false, true);
+  LAPH_ATTR(float2, false, false);
+  LAPH_ATTR(__nv_bfloat162, true, true);
+  LAPH_ATTR(__nv_bfloat162, true, false);
+  LAPH_ATTR(__nv_bfloat162, false, true);
+  LAPH_ATTR(__nv_bfloat162, false, false);
+#undef LAPH_ATTR
+  return LAPH_OK;
+}
+
+// the 256-site tile keeps 55 KB of backward links in dynamic shared memory
+int cheb_init() {
+  LAPH_TRY(cheb2_attributes<64>());
+  LAPH_TRY(cheb2_attributes<128>());
+  LAPH_TRY(cheb2_attributes<256>());
+  return LAPH_OK;
+}
+
 int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
               const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
-              const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant,
+              const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant, int tile,
               cudaStream_t st) {
   const bool hz = Z != nullptr;
   if (variant == 1 && kb <= kCoefMax) {
-#define LAPH_CHEB2(LT, HZ, FIN)                                                                             \
-  k_cheb_mrhs2<LT, HZ, FIN><<<nblk, 128, 0, st>>>(pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), \
-                                                  scale, X, Z, S, Y, V, W, tcoef, step)
-    if (bf16) {
-      if (hz && final_step) LAPH_CHEB2(__nv_bfloat162, true, true);
-      else if (hz) LAPH_CHEB2(__nv_bfloat162, true, false);
-      else if (final_step) LAPH_CHEB2(__nv_bfloat162, false, true);
-      else LAPH_CHEB2(__nv_bfloat162, false, false);
-    } else {
-      if (hz && final_step) LAPH_CHEB2(float2, true, true);
-      else if (hz) LAPH_CHEB2(float2, true, false);
-      else if (final_step) LAPH_CHEB2(float2, false, true);
-      else LAPH_CHEB2(float2, false, false);
-    }
-#undef LAPH_CHEB2
+    if (tile == 64)
+      launch_cheb2<64>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step, st);
+    else if (tile == 256)
+      launch_cheb2<256>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step,
+                        st);
+    else
+      launch_cheb2<128>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step,
+                        st);
     LAPH_CUDA_TRY(cudaGetLastError());
     return LAPH_OK;
   }

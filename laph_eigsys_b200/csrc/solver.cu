@@ -52,7 +52,7 @@ struct laph_solver {
   int dev = 0;
   cudaStream_t st = nullptr;
   laph_solve_opts o{};
-  int np = 0, mdeg = 16, kb = 32;
+  int np = 0, mdeg = 16, kb = 32, tile = 128;
   std::vector<ProbDesc> hd;
   ProbDesc* d_pd = nullptr;
   ProbState* d_ps = nullptr;
@@ -202,9 +202,10 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     return LAPH_EINVAL;
   }
   if (opts->deg < 2 || opts->deg > 64 || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1 ||
-      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 1) {
+      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 1 ||
+      (opts->filter_tile != 0 && opts->filter_tile != 64 && opts->filter_tile != 128 && opts->filter_tile != 256)) {
     set_error("laph_solver_create: need 2 <= deg <= 64, guard >= 0, tol > 0, max_it >= 1, 0 <= block <= 512, "
-              "filter_kernel in {0, 1}");
+              "filter_kernel in {0, 1}, filter_tile in {0, 64, 128, 256}");
     return LAPH_EINVAL;
   }
   for (int i = 0; i < n; ++i) {
@@ -232,12 +233,15 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   s->np = n;
   s->mdeg = opts->deg;
   s->kb = opts->block > 0 ? opts->block : 32;
+  // sites per CTA of the filter; the per-thread-coefficient variant and blocks wider than 64 keep 128
+  s->tile = opts->filter_tile > 0 && opts->filter_kernel == 1 && s->kb <= 64 ? opts->filter_tile : 128;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     set_error("laph_solver_create: cannot use device %d", device);
     return fail(LAPH_ECUDA);
   }
   if (int e = dense_init()) return fail(e);
+  if (int e = cheb_init()) return fail(e);
   // descriptors and pool offsets
   long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
   size_t max_run = 0, max_v3 = 0;
@@ -276,7 +280,7 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     max_v3 = std::max(max_v3, (size_t)d.V3);
     const int nst = (d.V3 + 127) / 128;
     per_site.push_back(nst);
-    per_filt.push_back(nst * ((d.k + s->kb - 1) / s->kb));
+    per_filt.push_back(((d.V3 + s->tile - 1) / s->tile) * ((d.k + s->kb - 1) / s->kb));
     per_nl.push_back(nst * ((d.k + kColsFP64 - 1) / kColsFP64));
     per_res.push_back(nst * d.k);
     per_gram.push_back(d.nchunk * npair);
@@ -420,7 +424,7 @@ static int filter_step(laph_solver* s, int n, bool fin, cudaStream_t st) {
   const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
   float2* Yo = s->E[(n - 1) % 3];
   return cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo, s->V,
-                   s->W, s->tcoef, n, fin, s->o.filter_kernel, st);
+                   s->W, s->tcoef, n, fin, s->o.filter_kernel, s->tile, st);
 }
 
 static int filter(laph_solver* s, int m) {

@@ -17,14 +17,16 @@ def test_autotune_picks_cached_settings_that_solve_correctly(gpu, orc, tmp_path)
     cache = tmp_path / "tune.txt"
     kw = dict(tol=1e-10, deg=60, max_it=300, guard=16, window=gpu.WINDOW_LANCZOS, link_prec=gpu.LINKS_FP32)
     opts, r = gpu.autotune(probs, links, nsample=2, cache=cache, **kw)
-    assert r["from_cache"] == 0 and 1 <= r["trials"] <= 8 and r["ms_per_problem"] > 0
-    assert r["deg"] in (40, 48, 56, 60, 64) and r["block"] in (16, 32, 64) and r["guard"] in (16, 48)
-    assert (opts.deg, opts.block, opts.guard) == (r["deg"], r["block"], r["guard"])
+    # deg (5) + block (3 more) + guard (1 more) + tile (2 more)
+    assert r["from_cache"] == 0 and 1 <= r["trials"] <= 11 and r["ms_per_problem"] > 0
+    assert r["deg"] in (40, 48, 56, 60, 64) and r["block"] in (8, 16, 32, 64) and r["guard"] in (16, 48)
+    assert r["tile"] in (64, 128, 256)
+    assert (opts.deg, opts.block, opts.guard, opts.filter_tile) == (r["deg"], r["block"], r["guard"], r["tile"])
     lines = cache.read_text().splitlines()
     assert len(lines) == 1 and lines[0].split("\t")[1].split()[:3] == [str(r["deg"]), str(r["block"]), str(r["guard"])]
     opts2, r2 = gpu.autotune(probs, links, nsample=2, cache=cache, **kw)
     assert r2["from_cache"] == 1 and r2["trials"] == 0
-    assert (r2["deg"], r2["block"], r2["guard"]) == (r["deg"], r["block"], r["guard"])
+    assert (r2["deg"], r2["block"], r2["guard"], r2["tile"]) == (r["deg"], r["block"], r["guard"], r["tile"])
     s = gpu.Solver(probs, opts=opts)
     for i in range(3):
         s.set_links(i, links[i])

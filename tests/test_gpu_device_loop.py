@@ -126,3 +126,21 @@ def test_async_read_back_overlaps_the_next_run(gpu):
             assert np.array_equal(e, ev) and np.array_equal(p, ph)
             assert np.array_equal(v.reshape(nev, 3 * L ** 3).T, V)
     s.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_filter_tiles_are_bitwise_identical(gpu, prec):
+    """The filter's site tile (64, 128 or 256 sites per CTA, an autotuner axis) changes only which CTA computes a
+    site, not the arithmetic: every tile gives bitwise the same eigenpairs, on a batch with a ragged last tile
+    (10^3 = 1000 sites, 12^3 = 1728)."""
+    probs = [(10, 24), (12, 30)]
+    links = [random_links(L, 0.35, 3400 + i) for i, (L, _) in enumerate(probs)]
+    outs = []
+    for tile in (64, 128, 256):
+        o = _solve(gpu, probs, links, guard=16, tol=1e-10, deg=24, filter_tile=tile,
+                   link_prec=gpu.LINKS_BF16 if prec == "bf16" else gpu.LINKS_FP32)
+        assert o["status"] == 0
+        outs.append(o)
+    for o in outs[1:]:
+        for (ea, va, _), (eb, vb, _) in zip(outs[0]["eig"], o["eig"]):
+            assert np.array_equal(ea, eb) and np.array_equal(va, vb)
