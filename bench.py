@@ -573,6 +573,7 @@ def measure_sourceshape(solver, stream, batch, no_cpu, reps=4):
     import laph_eigsys_b200 as lb
     L, nev, _ = batch[0]
     n = min(reps, len(batch))
+    fma_peak, dmma_peak = lb.probe_fp64(torch.cuda.current_device())
     solver.sourceshape(0)  # warm-up
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -585,9 +586,10 @@ def measure_sourceshape(solver, stream, batch, no_cpu, reps=4):
     fl = sourceshape_flops(L, nev)
     out = {"workload": f"psi(r) of {L}^3 x nev {nev}, (L/2)^3 = {(L // 2) ** 3} displacements, FP64",
            "kernel": "k_ss_tile, FP64 tensor path (mma.sync m8n8k4.f64)",
-           "ms_per_timeslice": ms, "tflops": fl / (ms / 1e3) / 1e12, "bound": "fp64",
-           "fp64_peak_tflops": 33.5, "peak_source": "FP64 FMA loop measured on this pool's B200",
-           "frac": fl / (ms / 1e3) / 1e12 / 33.5, "timeslices": n}
+           "ms_per_timeslice": ms, "tflops": fl / (ms / 1e3) / 1e12, "bound": "fp64 tensor (DMMA)",
+           "fp64_peak_tflops": dmma_peak, "fp64_fma_tflops": fma_peak,
+           "peak_source": "laph_probe_fp64 in this run (saturating mma.sync.m8n8k4.f64 loop)",
+           "frac": fl / (ms / 1e3) / 1e12 / dmma_peak, "timeslices": n}
     if not no_cpu:
         import oracle as orc
         Ls, nevs = 16, min(nev, 120)

@@ -53,6 +53,11 @@ int laph_version(void);
 /* The device architecture the library's kernels were built for, as the CUDA
  * runtime reports it (cudaFuncAttributes::binaryVersion: 100 = sm_100a). */
 int laph_binary_version(int* version);
+/* The device's FP64 throughput measured in place (TFLOP/s): a saturating loop
+ * of fma.rn.f64 and one of mma.sync.m8n8k4.f64 (the FP64 tensor path), each
+ * timed with CUDA events; the denominators of the FP64 kernels' rooflines.
+ * No counterpart in the reference. */
+int laph_probe_fp64(int device, double* fma_tflops, double* dmma_tflops);
 
 /* ---- link layouts accepted at the boundary -------------------------------- */
 enum {

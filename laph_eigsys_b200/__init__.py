@@ -382,6 +382,13 @@ def autotune(problems, links, nsample=4, cache=None, device=0, layout=LAYOUT_ROW
     return o, _tune_dict(r)
 
 
+def probe_fp64(device=0):
+    """(FP64 FMA TFLOP/s, FP64 tensor-path DMMA TFLOP/s) measured in place on the device (laph_probe_fp64)."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    check(lib.laph_probe_fp64(device, ctypes.byref(a), ctypes.byref(b)), "laph_probe_fp64")
+    return a.value, b.value
+
+
 def solve_opts(**kw):
     o = _lib.laph_solve_opts()
     lib.laph_solve_opts_default(ctypes.byref(o))

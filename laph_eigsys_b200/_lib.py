@@ -105,6 +105,7 @@ _sig("laph_solver_wait", c_int, c_void_p)
 _sig("laph_solver_filter_bytes", c_int, c_void_p, P(c_double))
 _sig("laph_ctx_stream", c_int, c_void_p, P(c_void_p))
 _sig("laph_binary_version", c_int, P(c_int))
+_sig("laph_probe_fp64", c_int, c_int, P(c_double), P(c_double))
 _sig("laph_solver_set_window_model", c_int, c_void_p, c_void_p, c_int)
 _sig("laph_solver_features", c_int, c_void_p, c_void_p, c_void_p)
 _sig("laph_solver_ritz", c_int, c_void_p, c_int, c_void_p, P(c_int))

@@ -52,3 +52,12 @@ def test_binary_version_without_a_device_is_an_error_not_a_guess():
     v = ctypes.c_int(-1)
     assert lb.lib.laph_binary_version(ctypes.byref(v)) != 0
     assert v.value == -1
+
+
+@pytest.mark.gpu
+def test_fp64_probe_measures_plausible_peaks():
+    """laph_probe_fp64 (the FP64 rooflines' denominators, measured in place) gives B200-sized figures: tens of
+    TFLOP/s on the FMA pipe and on the FP64 tensor path."""
+    import laph_eigsys_b200 as lb
+    fma, dmma = lb.probe_fp64(0)
+    assert 10.0 < fma < 120.0 and 10.0 < dmma < 120.0, (fma, dmma)
