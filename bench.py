@@ -6,23 +6,36 @@ field (U = exp(i*0.3*H), stout-smeared 5 x rho=0.1 on the device in FP64),
 solved for the lowest nev = 120 eigenpairs of -Delta to a residual
 ||(-Delta)v - lambda v|| / (||v|| lambda_max) <= 1e-9 by the batched block
 solver (FP32 filter matvecs on FP32 links, FP64 Gram / Cholesky /
-Rayleigh-Ritz / residuals), phase-fixed.  All 64 timeslices run as one batch.
+Rayleigh-Ritz / residuals), phase-fixed.  All 64 timeslices run as one batch,
+one CUDA graph launch per solve; the solver's degree, column block, guard and
+filter tile are tuned on 4 timeslices first (--autotune 0: the defaults).
 
 value : timeslices/s with links resident in HBM (device-timed, CUDA events on
         the solver's stream, K steps between barriers, max over ranks).
 e2e   : the same through the public C ABI with host buffers: each step copies
-        the links from pinned host memory and reads every eigenpair back.
-roofline: lap_cheb_mrhs (the FP32 multi-RHS Chebyshev stencil), algorithmic
-        bytes / its event-timed duration, against the measured HBM copy peak.
+        the links from pinned host memory and reads every eigenpair back
+        (laph_solver_get_async into pinned buffers, overlapping the next step;
+        the last step waits for its copies).
+roofline: lap_cheb_mrhs (the FP32 multi-RHS Chebyshev stencil), the solver's
+        own count of algorithmic bytes / its device-timed duration, against
+        the measured HBM copy peak; frac on the correction form's bytes and
+        frac_s8d on the plain recurrence's 72 B + links per site-vector-step.
+parity: timeslice 0 of the timed batch against the CPU FP64 oracle's run.
 cpu_baseline: the CPU FP64 oracle (restated reference ev_ts path: stout
         smearing + Krylov-Schur on T_DEG(B)) on one timeslice of the same
         workload, all host cores.
-Also reported: the plain GPU form (MatShell + Krylov-Schur), the source shape
-and displacement kernels on the solved eigenvectors, the LIME reader's
-throughput (lime_io), and with --autotune N the autotuner's choice.
+Also reported: the plain GPU form (MatShell + Krylov-Schur, its one-launch
+MatMult event-timed), the learned window against the non-learned one on the
+headline batch (window_ab), sub-records of the survey's other configurations
+(C1 with parity, C2 with parity, C3 with BF16 links, a wave of C4's mixed
+volumes, a wave of C5), the source shape and displacement kernels on the
+solved eigenvectors with an FP64 peak measured in place, the LIME reader's
+throughput (lime_io), and the autotuner's choice.
 
---impl reference runs that CPU path as the reference arm (--cpu-layout
-per-core: one single-threaded timeslice per core, the reference's MPI layout).
+--impl reference runs that CPU path as the reference arm without loading the
+product library (inputs from the oracle's generator), plus one round of the
+reference's MPI layout (one single-threaded timeslice per core) recorded
+beside it; --cpu-layout per-core times that layout as the arm itself.
 Multi-GPU (torchrun): timeslices are independent; each rank solves its own
 64-timeslice batch (weak scaling), no collective on the data path.
 """

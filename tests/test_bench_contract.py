@@ -72,3 +72,20 @@ def test_reference_arm_per_core_layout():
     assert ln["impl"] == "reference" and ln["value"] > 0 and cb["layout"] == "one timeslice per core"
     assert cb["cores"] == (os.cpu_count() or 1)
     assert abs(ln["ms_per_step"] * ln["value"] / 1000.0 - cb["cores"]) < 1e-6 * cb["cores"]
+
+
+def test_reference_arm_never_loads_the_product_library():
+    """The reference arm times the oracle's restatement of the reference path: its process must not import the
+    product package nor map liblaph_gpu.so (its inputs come from the oracle's own field generator)."""
+    code = ("import runpy, sys\n"
+            "sys.argv = " + repr(ARGS + ["--no-per-core"]) + "\n"
+            "try:\n    runpy.run_path('bench.py', run_name='__main__')\nexcept SystemExit as e:\n    assert not e.code\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'liblaph_gpu' not in maps, 'liblaph_gpu.so mapped'\n"
+            "assert not any(m.startswith('laph_eigsys_b200') for m in sys.modules), 'package imported'\n"
+            "print('CLEAN')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600, env=_env())
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "CLEAN" in r.stdout
+    line = _json_lines(r.stdout)[0]
+    assert "inputs" in line["cpu_baseline"]
