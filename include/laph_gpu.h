@@ -299,7 +299,8 @@ int laph_autotune_search(const int* deg_c, int nd, const int* block_c, int nb, c
  * nmodel: the window model (as laph_solver_set_window_model) when
  * opts->window is LAPH_WINDOW_MLP, else ignored (may be NULL).  Candidates:
  * deg 40, 48, 56, 60, 64 (start: opts->deg, or 60 if <= 1), block 8, 16, 32, 64
- * (start: opts->block, or 32), guard opts->guard and opts->guard + 32, then the
+ * (start: opts->block, or 32), guard opts->guard, opts->guard + 32 and the fewest
+ * (>= 4) that give the smallest block width above nev + 4, then the
  * filter's tile of 64, 128 or 256 sites per CTA (start: opts->filter_tile, or
  * 128) with the other three at their best.
  * cache_path (may be NULL): a text file of earlier results, one line per

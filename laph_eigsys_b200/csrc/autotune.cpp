@@ -217,10 +217,16 @@ int laph_solver_autotune(const laph_problem* probs, int n, const double* const* 
   const int guard0 = opts->guard;
   const int degs[] = {40, 48, 56, 60, 64};
   const int blocks[] = {8, 16, 32, 64};
-  const int guards[] = {guard0, guard0 + 32};
+  // guard: the given one, 32 more, and the fewest (>= 4) that keep the block width at its smallest multiple of 32
+  // (nev 120: guard 8, k = 128 instead of 160 -- less work per pass against slower convergence of the top pairs)
+  const int gmin = std::max(4, ((probs[0].nev + 4 + 31) / 32) * 32 - probs[0].nev);
+  std::vector<int> guards = {guard0, guard0 + 32};
+  if (gmin != guard0 && gmin != guard0 + 32 && ((probs[0].nev + gmin + 31) / 32 != (probs[0].nev + guard0 + 31) / 32))
+    guards.push_back(gmin);
   const int tile0 = opts->filter_tile > 0 ? opts->filter_tile : 128;
   SampleCtx ctx{probs, ns, links, layout, *opts, model, nmodel, device, LAPH_OK, tile0};
-  int st = laph_autotune_search(degs, 5, blocks, 4, guards, 2, deg0, block0, guard0, sample_trial, &ctx, out);
+  int st = laph_autotune_search(degs, 5, blocks, 4, guards.data(), (int)guards.size(), deg0, block0, guard0,
+                                sample_trial, &ctx, out);
   if (st != LAPH_OK) {
     if (ctx.last_status != LAPH_OK && ctx.last_status != LAPH_ENOTCONV)
       set_error("laph_solver_autotune: every setting failed; the last with status %d (%s)", ctx.last_status,
