@@ -19,6 +19,7 @@
 #include "batch.cuh"
 #include "dense.cuh"
 #include "filter.cuh"
+#include "stencil64cols.cuh"
 
 namespace laph {
 
@@ -765,6 +766,76 @@ __global__ void __launch_bounds__(128) k_residual64(const ProbDesc* __restrict__
   if (threadIdx.x == 0) rpart[d.rp + (size_t)st * d.k + j] = red[0] + red[1] + red[2] + red[3];
 }
 
+// The same residual laid out like the FP64 block stencil A W: CTA = 128 sites x
+// a block of kColsFP64 columns, the site's forward links in registers and its
+// backward links in shared memory, read once per column block instead of
+// once per (site, column).  Each thread leaves |r|^2 of its site and column in
+// shared memory (FP32: one site's share of a norm needs no more); after the
+// column loop the CTA reduces the 128 sites of every column in a fixed order
+// (FP64 sums) into the same per-tile partials as the kernel above, so the
+// column loop carries no per-column reduction.
+constexpr int kResidSmem = kStencil64Smem + kColsFP64 * kSites64 * (int)sizeof(float);
+
+__global__ void __launch_bounds__(kSites64, 3)
+    k_residual64_cols(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, const int* __restrict__ start,
+                      int np, const double2* __restrict__ U64, const double2* __restrict__ Vp,
+                      const double* __restrict__ theta, float2* __restrict__ Sp, double* __restrict__ rpart) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int nst = (d.V3 + kSites64 - 1) / kSites64;
+  const int t = blockIdx.x - start[p];
+  const int st = t % nst, cb = t / nst;
+  const int c0 = ps[p].c0;
+  const int j0 = cb * kColsFP64, j1 = min(d.k, j0 + kColsFP64);
+  if (j1 <= c0) return;  // frozen columns: their residual partials stand
+  const int jstart = max(j0, c0);
+  // threads past the last site compute the last site again and write nothing
+  const bool valid = st * kSites64 + (int)threadIdx.x < d.V3;
+  const int s = min(st * kSites64 + (int)threadIdx.x, d.V3 - 1);
+  extern __shared__ double2 s64[];
+  double2 (*sUb)[kSites64] = reinterpret_cast<double2 (*)[kSites64]>(s64);
+  float (*sPart)[kSites64] = reinterpret_cast<float (*)[kSites64]>(s64 + 27 * kSites64);
+  const Lat g{d.L, d.L * d.L, d.V3};
+  int up[3], dn[3], sx, sy, sz;
+  site_xyz(g, s, sx, sy, sz);
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu) {
+    up[mu] = nb_up(g, sx, sy, sz, mu);
+    dn[mu] = nb_dn(g, sx, sy, sz, mu);
+  }
+  Links64 l;
+  load_links64(U64 + d.u64, g, s, dn, l, sUb);
+  const double sc = -2.0 * ps[p].c_hop;
+#pragma unroll 1
+  for (int j = jstart; j < j1; ++j) {
+    const size_t col = (size_t)d.blk + (size_t)j * d.dim;
+    const double2* x = Vp + col;
+    double2 acc[3];
+    hop64_col(l, sUb, d.V3, up, dn, x, acc);
+    const double th = __ldg(theta + d.kv + j);
+    double r2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double2 xs = __ldg(x + (size_t)a * d.V3 + s);
+      const double2 r = make_double2((6.0 - th) * xs.x - acc[a].x, (6.0 - th) * xs.y - acc[a].y);
+      r2 += r.x * r.x + r.y * r.y;
+      if (valid) Sp[col + (size_t)a * d.V3 + s] = make_float2((float)(sc * r.x), (float)(sc * r.y));
+    }
+    sPart[j - j0][threadIdx.x] = valid ? (float)r2 : 0.f;
+  }
+  __syncthreads();
+  // column c = tid / 4 summed by 4 threads over 32 sites each, then across them
+  const int c = threadIdx.x >> 2, q = threadIdx.x & 3;
+  double sum = 0.0;
+  if (j0 + c >= jstart && j0 + c < j1)
+#pragma unroll 8
+    for (int i = 0; i < kSites64 / 4; ++i) sum += (double)sPart[c][q * (kSites64 / 4) + i];
+  sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+  sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+  if (q == 0 && j0 + c >= jstart && j0 + c < j1) rpart[d.rp + (size_t)st * d.k + j0 + c] = sum;
+}
+
 // ------------------------------------------------------- residuals/conv ----
 __global__ void k_resid(const ProbDesc* __restrict__ pd, ProbState* __restrict__ ps, const double* __restrict__ rpart,
                         double* __restrict__ resid, double tol, int* __restrict__ n_active) {
@@ -905,6 +976,7 @@ int to_reference(const double2* in, double2* out, int V3, int nev, cudaStream_t 
 int dense_init() {
   LAPH_CUDA_TRY(cudaFuncSetAttribute(k_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, kGramSmem));
   LAPH_CUDA_TRY(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, kRotSmem));
+  LAPH_CUDA_TRY(cudaFuncSetAttribute(k_residual64_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kResidSmem));
   LAPH_TRY(neglap64_init());
   return LAPH_OK;
 }
@@ -942,6 +1014,12 @@ int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, in
 int residual64(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
                const double2* V, const double* theta, float2* S, double* rpart, cudaStream_t st) {
   k_residual64<<<nblk, 128, 0, st>>>(pd, ps, start, np, U64, V, theta, S, rpart);
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+int residual64_cols(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
+                    const double2* V, const double* theta, float2* S, double* rpart, cudaStream_t st) {
+  k_residual64_cols<<<nblk, kSites64, kResidSmem, st>>>(pd, ps, start, np, U64, V, theta, S, rpart);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

@@ -25,6 +25,10 @@ int rotate(const ProbDesc* pd, const ProbState* ps, const int* start, int np, in
            const double2* KK, double2* V, cudaStream_t st);
 int residual64(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
                const double2* V, const double* theta, float2* S, double* rpart, cudaStream_t st);
+// The same on CTAs of 128 sites x 32 columns (links read once per column block);
+// nblk and start as for neglap64_batch.
+int residual64_cols(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, const double2* U64,
+                    const double2* V, const double* theta, float2* S, double* rpart, cudaStream_t st);
 int resid_check(const ProbDesc* pd, ProbState* ps, int np, const double* rpart, double* resid, double tol,
                 int* n_active, cudaStream_t st);
 // Ritz values lam_max and filter map of the state's window for a start block that

@@ -402,6 +402,19 @@ constexpr double kCapResid = 1e-2;
 // as a working window (the random start block has residuals of order 1).
 constexpr double kWindowCheck = 0.2;
 
+// R = A V - V Theta, S = -2 c_hop R and the residual partials: the column-block
+// kernel by default, the one-thread-per-(site, column) kernel with
+// LAPH_RESID_KERNEL=0 (both leave the same per-tile partials).
+static int residual(laph_solver* s) {
+  static const int kind = [] {
+    const char* e = std::getenv("LAPH_RESID_KERNEL");
+    return e && *e == '0' ? 0 : 1;
+  }();
+  if (kind == 0)
+    return residual64(s->d_pd, s->d_ps, s->st_res, s->np, s->nb_res, s->U64, s->V, s->theta, s->S, s->rpart, s->st);
+  return residual64_cols(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->V, s->theta, s->S, s->rpart, s->st);
+}
+
 static int iteration_rr(laph_solver* s, int first_iter) {
   const bool fixed = s->o.window == LAPH_WINDOW_FIXED && s->o.lam_cut > 0.0;
   LAPH_TRY(neglap64_batch(s->d_pd, s->d_ps, s->st_nl, s->np, s->nb_nl, s->U64, s->W, s->Y, s->st));
@@ -410,7 +423,7 @@ static int iteration_rr(laph_solver* s, int first_iter) {
   LAPH_TRY(small_dense(s->d_pd, s->d_ps, s->np, s->KK, s->theta, s->tcoef, s->scol, s->dwork, first_iter, fixed ? 1 : 0,
                        s->o.jacobi_sweeps > 0 ? s->o.jacobi_sweeps : 2, s->tstamp, s->st));
   LAPH_TRY(rotate(s->d_pd, s->d_ps, s->st_rot, s->np, s->nb_rot, s->W, s->KK, s->V, s->st));
-  LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_res, s->np, s->nb_res, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
+  LAPH_TRY(residual(s));
   LAPH_TRY(zero_int(s->d_nactive, s->st));
   LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
   return LAPH_OK;
@@ -531,7 +544,7 @@ static int solve_setup(laph_solver* s, bool device_loop, long long* nlaunch_out)
     LAPH_TRY(random_block(s->d_pd, s->st_rand, s->np, s->nb_rand, s->V, o.seed, s->st));
     if (!device_loop) LAPH_CUDA_TRY(cudaEventRecord(s->ev1, s->st));
     LAPH_TRY(start_window(s->d_pd, s->d_ps, s->np, s->theta, s->st));
-    LAPH_TRY(residual64(s->d_pd, s->d_ps, s->st_res, s->np, s->nb_res, s->U64, s->V, s->theta, s->S, s->rpart, s->st));
+    LAPH_TRY(residual(s));
     LAPH_TRY(zero_int(s->d_nactive, s->st));
     LAPH_TRY(resid_check(s->d_pd, s->d_ps, s->np, s->rpart, s->resid, s->o.tol, s->d_nactive, s->st));
     nlaunch += 2 + 5;  // pack, random block, window state, residual, zero, check
