@@ -740,6 +740,7 @@ def main():
         flaunch += cn[1]
         launches += cn[2]
         iters.append(max(r["iters"] for r in results))
+        loop_info = solver.loop_info()
         window_fallbacks = sum(r["window_fallback"] for r in results)
     e1.record(stream)
     barrier()
@@ -885,6 +886,7 @@ def main():
                 "data": "synthetic (seeded U = exp(i eps H) gauge field)", "config": workload_config(cfg),
                 "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "plain_gpu": plain, "e2e": e2e,
                 "gpu_launches": launches,
+                "graph_launches_per_solve": loop_info[1], "device_loop": bool(loop_info[0]),
                 "clocks": clk, "sourceshape": shape, "displacement": disp, "lime_io": lime_io, "autotune": tune,
                 "window_ab": window_ab, "configs": configs,
                 "detail": {"outer_iterations": iters, "max_resid": max_resid,

@@ -260,6 +260,11 @@ int laph_solver_counters(laph_solver* s, long long* c3);
  * b2[1] = the plain recurrence's unit, 72 B per site-vector-step (X, Z read, Y
  * written) plus the links once per column block. */
 int laph_solver_filter_bytes(laph_solver* s, double* b2);
+/* How the last run looped: device_loop = 1 when the whole solve was one
+ * graph launch (the WHILE node on the device), 0 when the host drove the
+ * outer iteration; graph_launches = the graph launches it made (1, or two
+ * per pass for the host loop). */
+int laph_solver_loop_info(laph_solver* s, int* device_loop, long long* graph_launches);
 
 /* Device memory a solver for probs[0..n) with opts allocates (bytes, each
  * allocation rounded up to 2 MiB), without touching a device. */

@@ -516,6 +516,12 @@ class Solver:
         check(lib.laph_solver_counters(self._h, c), "laph_solver_counters")
         return list(c)
 
+    def loop_info(self):
+        """(device_loop, graph launches) of the last run (laph_solver_loop_info)."""
+        a, b = ctypes.c_int(), ctypes.c_longlong()
+        check(lib.laph_solver_loop_info(self._h, ctypes.byref(a), ctypes.byref(b)), "laph_solver_loop_info")
+        return a.value, b.value
+
     def filter_bytes(self):
         """Algorithmic bytes of the last run's filter passes (laph_solver_filter_bytes): (correction form as
         run, 72 B + links per site-vector-step)."""

@@ -103,6 +103,7 @@ _sig("laph_solver_stream", c_int, c_void_p, P(c_void_p))
 _sig("laph_solver_get_async", c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p)
 _sig("laph_solver_wait", c_int, c_void_p)
 _sig("laph_solver_filter_bytes", c_int, c_void_p, P(c_double))
+_sig("laph_solver_loop_info", c_int, c_void_p, P(c_int), P(ctypes.c_longlong))
 _sig("laph_ctx_stream", c_int, c_void_p, P(c_void_p))
 _sig("laph_binary_version", c_int, P(c_int))
 _sig("laph_probe_fp64", c_int, c_int, P(c_double), P(c_double))

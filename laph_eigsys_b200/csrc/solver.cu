@@ -112,6 +112,8 @@ struct laph_solver {
   cudaGraphExec_t g_solve = nullptr;
   long long solve_setup_launches = 0;              // kernels of the graph outside the loop
   int solve_graph_failed = 0;                      // capture refused: the host loop from then on
+  int last_loop = 0;                               // the last run: 1 device-side loop (one launch), 0 host loop
+  long long last_graph_launches = 0;               // graph launches the last run made
   // asynchronous read-back (laph_solver_get_async): its own stream and a device
   // staging pool the runs never touch, so the copies of one run's results
   // overlap the next run; a run waits only for the conversions out of V
@@ -754,6 +756,8 @@ static int run_device_loop(laph_solver* s, laph_result* res) {
   s->fbytes[0] = ls.fbytes[0];
   s->fbytes[1] = ls.fbytes[1];
   s->ran = 1;
+  s->last_loop = 1;
+  s->last_graph_launches = 1;
   return fill_results(s, res);
 }
 extern "C" {
@@ -927,6 +931,8 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
   s->ms[3] = b;
   s->ms[2] = b - a - filt_ms;
   s->ran = 1;
+  s->last_loop = 0;
+  s->last_graph_launches = 2LL * (long long)s->degs.size();
   return fill_results(s, res);
 }
 
@@ -1126,6 +1132,16 @@ int laph_solver_displace(laph_solver* s, int i, int dir, double* W, int on_devic
   if (!on_device)
     LAPH_CUDA_TRY(cudaMemcpyAsync(W, out, sizeof(double2) * d.dim * d.nev, cudaMemcpyDeviceToHost, s->st));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return LAPH_OK;
+}
+
+int laph_solver_loop_info(laph_solver* s, int* device_loop, long long* graph_launches) {
+  if (!s || !device_loop || !graph_launches || !s->ran) {
+    set_error("laph_solver_loop_info: bad argument or solver not run");
+    return LAPH_EINVAL;
+  }
+  *device_loop = s->last_loop;
+  *graph_launches = s->last_graph_launches;
   return LAPH_OK;
 }
 

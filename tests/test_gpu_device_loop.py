@@ -25,7 +25,7 @@ def _solve(gpu, probs, links, **kw):
         s.set_links(i, U)
     st, res = s.run()
     out = dict(status=st, res=res, eig=[s.get(i) for i in range(len(probs))], counters=s.counters(),
-               fbytes=s.filter_bytes(), timings=s.timings())
+               fbytes=s.filter_bytes(), timings=s.timings(), loop=s.loop_info())
     s.close()
     return out
 
@@ -39,6 +39,8 @@ def test_device_loop_matches_host_loop(gpu, window):
     dev = _solve(gpu, probs, links, host_loop=0, **kw)
     host = _solve(gpu, probs, links, host_loop=1, **kw)
     assert dev["status"] == 0 and host["status"] == 0
+    assert dev["loop"] == (1, 1), dev["loop"]  # the whole solve was one graph launch
+    assert host["loop"][0] == 0 and host["loop"][1] >= 2
     for a, b in zip(dev["res"], host["res"]):
         assert a["iters"] == b["iters"] and a["nconv"] == b["nconv"]
         assert a["window_fallback"] == b["window_fallback"]
