@@ -311,10 +311,13 @@ __global__ void __launch_bounds__(1024) k_features(const ProbDesc* __restrict__ 
 //             adaptive iteration converges to; the first pass starts above it
 //             because its block is still a random one (margin calibrated on
 //             training lattices, laph_solve_opts.window_margin);
-//   lam_max = min(12, max(prediction 1, Lanczos bound)): the top of the
-//             damped interval, never below the 10-step Lanczos estimate of the
-//             top of the spectrum nor above the exact bound 12 (a first pass
-//             whose residual check fails goes back to 12, see the solver);
+//   lam_max stays the exact bound 12 of the spectrum of -Delta (or the fixed
+//             one): prediction 1 learns the 10-step Lanczos estimate of the
+//             top, which lies well below the true top (9.3-10.6 against
+//             11.5+ on 16^3-32^3 smeared fields), and a window whose top is
+//             below the spectrum's lets T_m amplify the highest eigenvectors
+//             past the wanted ones -- solves with it did not converge in 300
+//             passes -- so it is not used;
 //   degree  = prediction 2, clamped to [8, 64], written to out_deg.
 __global__ void k_window_apply(const ProbDesc* __restrict__ pd, ProbState* __restrict__ ps, int np,
                                const float* __restrict__ O, const float* __restrict__ norm,
@@ -323,15 +326,11 @@ __global__ void k_window_apply(const ProbDesc* __restrict__ pd, ProbState* __res
   if (p >= np) return;
   const float* om = norm + 2 * kMlpIn;  // output mean[3], std[3]
   const double y0 = O[p * kMlpOut + 0] * om[3] + om[0];
-  const double y1 = O[p * kMlpOut + 1] * om[4] + om[1];
   const double y2 = O[p * kMlpOut + 2] * om[5] + om[2];
+  (void)bound;
   ProbState& S = ps[p];
-  const double b = bound[p];
-  double lmax = fmax(y1, b);
-  if (!(lmax > 0.0) || lmax > 12.0) lmax = 12.0;  // NaN or beyond the exact bound
-  S.lam_max = lmax;
   const double cut = exp(y0) * margin;
-  S.lam_cut = fmin(fmax(cut, 1e-3), S.lam_max - 1e-3);
+  S.lam_cut = isfinite(cut) ? fmin(fmax(cut, 1e-3), S.lam_max - 1e-3) : 0.5 * S.lam_max;
   out_deg[p] = isfinite(y2) ? (int)lrint(fmin(64.0, fmax(8.0, y2))) : 64;
 }
 

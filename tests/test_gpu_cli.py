@@ -41,7 +41,9 @@ def test_ev_ts_cli(gpu, orc, tmp_path, solver):
         f"tol = 1e-11\nsolver = {solver}\n")
     r = subprocess.run([EXE, "--conf", str(cfgno)], cwd=tmp_path, capture_output=True, text=True, timeout=600, env=ENV)
     assert r.returncode == 0, r.stderr
-    assert len([ln for ln in r.stdout.splitlines() if ln.startswith("{")]) == T
+    # one line per timeslice, plus the rank's launcher line
+    assert len([ln for ln in r.stdout.splitlines() if ln.startswith('{"t"')]) == T
+    assert sum(ln.startswith('{"launcher"') for ln in r.stdout.splitlines()) == 1
     for t in range(T):
         ev = lb.read_eigenvalues_bin(out, "eigenvalues", cfgno, t, nev)
         V = lb.read_eigsys_bin(out, "eigenvectors", cfgno, t, 3 * L ** 3, nev)  # runs check_trace

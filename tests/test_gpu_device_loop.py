@@ -69,7 +69,8 @@ def test_uneven_batch_in_one_launch_matches_oracle_krylov_schur(gpu, orc):
     """16^3 (nev 60) and 24^3 (nev 120) timeslices, APE 0.5 x 10 as the survey's mixed-volume configuration, in one
     batch and one graph launch, each against the oracle's smearing + FP64 Krylov-Schur on T_12(B): eigenvalues
     (Rayleigh quotients) to 1e-10 relative each, residuals at the tolerance, tr(V^dag V) = nev, and the nev-block
-    subspace to the residual over the gap."""
+    subspace to the residual over the gap.  The oracle's Krylov-Schur runs at 1e-10 relative to |theta| (near the
+    window's edge theta is close to 1 and a tighter test needs hundreds of restarts on these smooth fields)."""
     specs = [(16, 60, 1230, 0), (24, 120, 1231, 0), (16, 60, 1230, 1)]
     links, probs = [], []
     for L, nev, seed, t in specs:
@@ -84,7 +85,7 @@ def test_uneven_batch_in_one_launch_matches_oracle_krylov_schur(gpu, orc):
     for (L, nev), U, (ev, V, _) in zip(probs, links, out["eig"]):
         Us = orc.smear_ape(U, L, 0.5, 10, 1)
         lam = -ev
-        st, _, Vk, _, _, _ = orc.eps_solve(Us, L, 12.0, float(1.1 * lam[-1]), 12, nev, tol=1e-12, max_it=300)
+        st, _, Vk, _, _, _ = orc.eps_solve(Us, L, 12.0, float(1.1 * lam[-1]), 12, nev, tol=1e-10, max_it=400)
         assert st == 0
         Vo, _ = orc.fix_phase(Vk)
         r = orc.compare_eigensystems(Us, L, V, Vo)
