@@ -78,8 +78,8 @@ def test_uneven_batch_in_one_launch_matches_oracle_krylov_schur(gpu, orc):
         links.append(np.ascontiguousarray(conf[t, :, 1:4]))
         probs.append((L, nev))
     tol = 1e-11
-    out = _solve(gpu, probs, links, smear_kind=gpu.SMEAR_APE, smear_p1=0.5, smear_iters=10, guard=16, tol=tol,
-                 deg=48, max_it=300, window=gpu.WINDOW_LANCZOS)
+    out = _solve(gpu, probs, links, smear_kind=gpu.SMEAR_APE, smear_p1=0.5, smear_iters=10, smear_compat=1,
+                 guard=16, tol=tol, deg=48, max_it=300, window=gpu.WINDOW_LANCZOS)
     assert out["status"] == 0
     orc.set_threads(os.cpu_count() or 1)
     for (L, nev), U, (ev, V, _) in zip(probs, links, out["eig"]):

