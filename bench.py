@@ -181,7 +181,7 @@ def make_opts(cfg):
                          link_prec=lb.LINKS_BF16 if cfg["link_prec"] == "bf16" else lb.LINKS_FP32, tol=cfg["tol"],
                          max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
                          filter_kernel=cfg.get("filter_kernel", 1), jacobi_sweeps=cfg.get("sweeps", 0),
-                         filter_tile=cfg.get("tile", 0),
+                         filter_tile=cfg.get("tile", 0), host_loop=cfg.get("host_loop", 0),
                          lam_cut=cfg.get("lam_cut0", 0.0),
                          window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
                              cfg.get("window", "mlp")])
@@ -645,6 +645,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-shape", action="store_true")
     ap.add_argument("--no-io", action="store_true")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="drive the outer iteration from the host (same kernels; ncu cannot profile kernels inside "
+                         "a graph with conditional nodes)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the learned-window A/B and the sub-records of the other survey configurations")
     ap.add_argument("--autotune", type=int, default=4, metavar="NSAMPLE",
@@ -673,6 +676,7 @@ def main():
     if args.guard is not None:
         cfg["guard"] = args.guard
     cfg["filter_kernel"] = args.filter_kernel
+    cfg["host_loop"] = int(args.host_loop)
     if args.impl == "reference":
         return run_reference(args, cfg)
 

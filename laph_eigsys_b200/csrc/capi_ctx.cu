@@ -22,7 +22,8 @@ struct laph_ctx {
   double2* h_stage = nullptr;  // pinned staging, 2 vectors
   double* d_scalar = nullptr;
   laph::GridBar* bar = nullptr;  // grid barrier of the fused MatMult
-  int* h_err = nullptr;          // pinned: that barrier's error flag after a product
+  int* h_err = nullptr;          // page-locked, mapped: set by a grid barrier that gave up
+  int* d_herr = nullptr;         // its device address
 };
 
 using namespace laph;
@@ -94,7 +95,8 @@ int laph_ctx_create(laph_ctx** out, const laph_params* p) {
       cudaMalloc(&c->vec, sizeof(double2) * 4 * dim) != cudaSuccess ||
       cudaMalloc(&c->d_scalar, sizeof(double) * 64) != cudaSuccess ||
       cudaMalloc(&c->bar, sizeof(GridBar)) != cudaSuccess || cudaMemset(c->bar, 0, sizeof(GridBar)) != cudaSuccess ||
-      cudaMallocHost(&c->h_err, sizeof(int)) != cudaSuccess ||
+      cudaHostAlloc(&c->h_err, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void**>(&c->d_herr), c->h_err, 0) != cudaSuccess ||
       cudaMallocHost(&c->h_stage, sizeof(double2) * 2 * dim) != cudaSuccess) {
     cudaGetLastError();
     set_error("laph_ctx_create: allocation failed for L=%d", p->L);
@@ -233,12 +235,14 @@ int laph_matmult(laph_ctx* c, const double* x, double* y, int deg, int on_device
   LAPH_TRY(stage_in(c, x, on_device, &dx));
   double2* dy = on_device ? reinterpret_cast<double2*>(y) : c->vec + dim;
   // the whole recurrence in one launch (tv_iter, shell_matop.cpp:136-168)
-  LAPH_TRY(cheb64_fused(c->U, c->g.L, c->lam_l, c->lam_c, deg, dx, dy, c->vec + 2 * dim, dim, c->bar, c->st));
-  LAPH_CUDA_TRY(cudaMemcpyAsync(c->h_err, &c->bar->err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  LAPH_TRY(stage_out(c, y, on_device));
-  if (*c->h_err) {
+  *reinterpret_cast<volatile int*>(c->h_err) = 0;
+  LAPH_TRY(cheb64_fused(c->U, c->g.L, c->lam_l, c->lam_c, deg, dx, dy, c->vec + 2 * dim, dim, c->bar, c->d_herr,
+                        c->st));
+  LAPH_TRY(stage_out(c, y, on_device));  // synchronises the stream
+  if (*reinterpret_cast<volatile int*>(c->h_err)) {
     cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->st);
     cudaStreamSynchronize(c->st);
+    *reinterpret_cast<volatile int*>(c->h_err) = 0;
     set_error("laph_matmult: a grid barrier of the fused product gave up waiting; y is not valid");
     return LAPH_ECUDA;
   }

@@ -286,6 +286,8 @@ struct DeviceBasis : Basis {
   cublasHandle_t hb = nullptr;
   double2 *V = nullptr, *w = nullptr, *tmp = nullptr, *h = nullptr, *Zd = nullptr;
   GridBar* bar = nullptr;  // grid barrier of the fused T_deg(B) product
+  int* h_err = nullptr;    // page-locked, mapped: set by a barrier that gave up
+  int* d_herr = nullptr;
   int ok = 0;
   DeviceBasis(laph_ctx* c, long dim, int m) : ctx(c) {
     n = dim;
@@ -295,10 +297,13 @@ struct DeviceBasis : Basis {
     if (cudaMalloc(&V, sizeof(double2) * n * (cap + 1)) != cudaSuccess || cudaMalloc(&w, sizeof(double2) * n) != cudaSuccess ||
         cudaMalloc(&tmp, sizeof(double2) * n * 2) != cudaSuccess || cudaMalloc(&h, sizeof(double2) * 2 * cap) != cudaSuccess ||
         cudaMalloc(&Zd, sizeof(double2) * cap * cap) != cudaSuccess || cudaMalloc(&bar, sizeof(GridBar)) != cudaSuccess ||
-        cudaMemset(bar, 0, sizeof(GridBar)) != cudaSuccess) {
+        cudaMemset(bar, 0, sizeof(GridBar)) != cudaSuccess ||
+        cudaHostAlloc(&h_err, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&d_herr), h_err, 0) != cudaSuccess) {
       cudaGetLastError();
       return;
     }
+    *reinterpret_cast<volatile int*>(h_err) = 0;
     if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) return;
     cublasSetStream(hb, st);
     ok = 1;
@@ -311,12 +316,12 @@ struct DeviceBasis : Basis {
     cudaFree(h);
     cudaFree(Zd);
     cudaFree(bar);
+    if (h_err) cudaFreeHost(h_err);
   }
   // nonzero if a grid barrier of any product so far gave up (sticky)
   int barrier_failed() {
-    int e = 0;
-    if (cudaMemcpy(&e, &bar->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
-    return e;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 1;
+    return *reinterpret_cast<volatile int*>(h_err);
   }
   double2* col(int j) { return V + (size_t)j * n; }
   int start(const std::vector<cd>& v0) override {
@@ -325,7 +330,7 @@ struct DeviceBasis : Basis {
   }
   int op(int j) override {
     ++nmatvec;
-    return cheb64_fused(U, L, lam_l, lam_c, deg, col(j), w, tmp, n, bar, st);
+    return cheb64_fused(U, L, lam_l, lam_c, deg, col(j), w, tmp, n, bar, d_herr, st);
   }
   int orth(int j, std::vector<cd>& hh, double* beta) override {
     const cuDoubleComplex one = {1.0, 0.0}, zero = {0.0, 0.0}, mone = {-1.0, 0.0};

@@ -114,10 +114,13 @@ struct laph_solver {
   int solve_graph_failed = 0;                      // capture refused: the host loop from then on
   int last_loop = 0;                               // the last run: 1 device-side loop (one launch), 0 host loop
   long long last_graph_launches = 0;               // graph launches the last run made
-  // asynchronous read-back (laph_solver_get_async): its own stream and a device
-  // staging pool the runs never touch, so the copies of one run's results
-  // overlap the next run; a run waits only for the conversions out of V
-  cudaStream_t st_out = nullptr;
+  // asynchronous read-back (laph_solver_get_async): a conversion stream (out
+  // of V into a device staging pool the runs never touch) and a copy stream
+  // (staging pool -> host), so the copies of one run's results overlap the
+  // next run, which waits only for the conversions
+  cudaStream_t st_conv = nullptr, st_out = nullptr;
+  std::vector<cudaEvent_t> ev_ready, ev_copied;  // per problem: converted / copied out
+  std::vector<int> copied_rec;                    // ev_copied[i] has been recorded
   double2* out_vec = nullptr;   // reference-layout eigenvectors, sum of dim x nev
   double* out_val = nullptr;    // eigenvalues (recover_spectrum sign) and phases, 2 x sum of nev
   std::vector<size_t> out_off;  // per problem: offset of its block in out_vec
@@ -181,6 +184,10 @@ int laph_solver_destroy(laph_solver* s) {
     if (p) cudaFree(p);
   if (s->h_nactive) cudaFreeHost(s->h_nactive);
   if (s->st_out) cudaStreamSynchronize(s->st_out);
+  if (s->st_conv) cudaStreamSynchronize(s->st_conv);
+  for (auto e : s->ev_ready) cudaEventDestroy(e);
+  for (auto e : s->ev_copied) cudaEventDestroy(e);
+  if (s->st_conv) cudaStreamDestroy(s->st_conv);
   if (s->out_vec) cudaFree(s->out_vec);
   if (s->out_val) cudaFree(s->out_val);
   if (s->ev_run) cudaEventDestroy(s->ev_run);
@@ -991,13 +998,21 @@ int laph_solver_get_async(laph_solver* s, int i, double* evals, double* evecs, d
       nvec += (size_t)s->hd[p].dim * s->hd[p].nev;
       nval += 2 * (size_t)s->hd[p].nev;
     }
-    if (cudaStreamCreateWithFlags(&s->st_out, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->ev_run, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->ev_conv, cudaEventDisableTiming) != cudaSuccess ||
-        cudaMalloc(&s->out_vec, sizeof(double2) * nvec) != cudaSuccess ||
-        cudaMalloc(&s->out_val, sizeof(double) * nval) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&s->st_out, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->st_conv, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&s->ev_run, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&s->ev_conv, cudaEventDisableTiming) == cudaSuccess &&
+              cudaMalloc(&s->out_vec, sizeof(double2) * nvec) == cudaSuccess &&
+              cudaMalloc(&s->out_val, sizeof(double) * nval) == cudaSuccess;
+    s->ev_ready.assign(s->np, nullptr);
+    s->ev_copied.assign(s->np, nullptr);
+    s->copied_rec.assign(s->np, 0);
+    for (int p = 0; p < s->np && ok; ++p)
+      ok = cudaEventCreateWithFlags(&s->ev_ready[p], cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&s->ev_copied[p], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
       cudaGetLastError();
-      set_error("laph_solver_get_async: cannot set up the read-back stream and its %zu-byte staging pool",
+      set_error("laph_solver_get_async: cannot set up the read-back streams and the %zu-byte staging pool",
                 sizeof(double2) * nvec);
       return LAPH_ENOMEM;
     }
@@ -1005,19 +1020,26 @@ int laph_solver_get_async(laph_solver* s, int i, double* evals, double* evecs, d
   const ProbDesc& d = s->hd[i];
   double2* ov = s->out_vec + s->out_off[i];
   double* oval = s->out_val + s->out_voff[i];
-  // everything queued on the compute stream so far (the run) before the conversions
+  // conversion stream: after everything queued on the compute stream so far (the
+  // run), and after the previous read-back of this problem's staging left it
   LAPH_CUDA_TRY(cudaEventRecord(s->ev_run, s->st));
-  LAPH_CUDA_TRY(cudaStreamWaitEvent(s->st_out, s->ev_run, 0));
-  if (evecs) LAPH_TRY(to_reference(s->V + d.blk, ov, d.V3, d.nev, s->st_out));
-  k_out_vals<<<ceil_div(d.nev, 128), 128, 0, s->st_out>>>(s->theta + d.kv, s->phases + d.kv, d.nev, oval);
+  LAPH_CUDA_TRY(cudaStreamWaitEvent(s->st_conv, s->ev_run, 0));
+  if (s->copied_rec[i]) LAPH_CUDA_TRY(cudaStreamWaitEvent(s->st_conv, s->ev_copied[i], 0));
+  if (evecs) LAPH_TRY(to_reference(s->V + d.blk, ov, d.V3, d.nev, s->st_conv));
+  k_out_vals<<<ceil_div(d.nev, 128), 128, 0, s->st_conv>>>(s->theta + d.kv, s->phases + d.kv, d.nev, oval);
   LAPH_CUDA_TRY(cudaGetLastError());
-  LAPH_CUDA_TRY(cudaEventRecord(s->ev_conv, s->st_out));
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev_ready[i], s->st_conv));
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev_conv, s->st_conv));  // the next run waits for this (conversions only)
   s->conv_pending = 1;
+  // copy stream: staging -> host once converted
+  LAPH_CUDA_TRY(cudaStreamWaitEvent(s->st_out, s->ev_ready[i], 0));
   if (evecs)
     LAPH_CUDA_TRY(cudaMemcpyAsync(evecs, ov, sizeof(double2) * d.dim * d.nev, cudaMemcpyDeviceToHost, s->st_out));
   if (evals) LAPH_CUDA_TRY(cudaMemcpyAsync(evals, oval, sizeof(double) * d.nev, cudaMemcpyDeviceToHost, s->st_out));
   if (phases)
     LAPH_CUDA_TRY(cudaMemcpyAsync(phases, oval + d.nev, sizeof(double) * d.nev, cudaMemcpyDeviceToHost, s->st_out));
+  LAPH_CUDA_TRY(cudaEventRecord(s->ev_copied[i], s->st_out));
+  s->copied_rec[i] = 1;
   return LAPH_OK;
 }
 
@@ -1028,6 +1050,7 @@ int laph_solver_wait(laph_solver* s) {
   }
   if (!s->st_out) return LAPH_OK;
   LAPH_CUDA_TRY(cudaSetDevice(s->dev));
+  LAPH_CUDA_TRY(cudaStreamSynchronize(s->st_conv));
   LAPH_CUDA_TRY(cudaStreamSynchronize(s->st_out));
   return LAPH_OK;
 }

@@ -106,10 +106,15 @@ int cheb64(const double2* U, int L, double lam_l, double lam_c, int deg, const d
 // fits the device's co-resident CTAs (up to 296 CTAs of 128 sites on a
 // B200: L <= 33); otherwise a grid-stride variant reads the links per step.
 
-// Grid barrier with a bounded wait: a CTA that waits longer than
-// kBarSpinLimit polls sets `err` and every CTA leaves at its next barrier.
+// Grid barrier with a bounded wait, one atomic per CTA and arrival: every CTA
+// adds 1 to the counter except CTA 0, which adds 2^31 - (nblk - 1), so the
+// last arrival flips bit 31 and leaves the low bits at zero for the next
+// barrier; a CTA waits for bit 31 to differ from the value its own add
+// returned (no reset, no second word).  A CTA that waits longer than
+// kBarSpinLimit polls sets `err` (and *herr, page-locked host memory the host
+// reads after its synchronisation) and every CTA leaves at its next barrier.
 // Cooperative launches guarantee co-residency, so the limit is a safety net.
-constexpr unsigned kBarSpinLimit = 1u << 22;
+constexpr unsigned kBarSpinLimit = 1u << 24;
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   unsigned v;
@@ -117,28 +122,25 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   return v;
 }
 
-__device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblk) {
+__device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblk, int* herr) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned gen = ld_acquire_gpu(&b->gen);
+    const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (nblk - 1) : 1u;
     __threadfence();  // this CTA's writes before its arrival
-    if (atomicAdd(&b->count, 1u) == nblk - 1) {
-      atomicExch(&b->count, 0u);
-      __threadfence();
-      atomicAdd(&b->gen, 1u);
-    } else {
-      unsigned it = 0;
-      while (ld_acquire_gpu(&b->gen) == gen) {
-        if (++it > kBarSpinLimit || *reinterpret_cast<volatile int*>(&b->err)) {
-          atomicExch(&b->err, 1);
-          break;
-        }
-        __nanosleep(32);
+    const unsigned old = atomicAdd(&b->count, inc);
+    bool ok = true;
+    unsigned it = 0;
+    while (((ld_acquire_gpu(&b->count) ^ old) & 0x80000000u) == 0) {
+      if ((++it & 1023u) == 0 && (it > kBarSpinLimit || *reinterpret_cast<volatile int*>(&b->err))) {
+        atomicExch(&b->err, 1);
+        *reinterpret_cast<volatile int*>(herr) = 1;
+        ok = false;
+        break;
       }
     }
     __threadfence();
-    s_ok = *reinterpret_cast<volatile int*>(&b->err) == 0;
+    s_ok = ok && *reinterpret_cast<volatile int*>(&b->err) == 0;
   }
   __syncthreads();
   return s_ok != 0;
@@ -149,7 +151,7 @@ constexpr int kFusedSmem = 27 * 128 * (int)sizeof(double2);
 template <bool RESIDENT>
 __global__ void __launch_bounds__(128, 2)
     k_cheb64_fused(const double2* __restrict__ U, Lat g, const double2* __restrict__ x, double2* y, double2* t0,
-                   double2* t1, int deg, double c, double a, GridBar* bar) {
+                   double2* t1, int deg, double c, double a, GridBar* bar, int* herr) {
   extern __shared__ double2 s_ub[];  // [27][128] backward links (RESIDENT only)
   double2 (*sUb)[128] = reinterpret_cast<double2 (*)[128]>(s_ub);
   const unsigned nblk = gridDim.x;
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(128, 2)
         __stcg(Y + 3 * (size_t)si + aa, r);
       }
     }
-    if (n < deg && !grid_barrier(bar, nblk)) return;
+    if (n < deg && !grid_barrier(bar, nblk, herr)) return;
   }
 }
 
@@ -260,7 +262,7 @@ int fused_occupancy(FusedOcc* out) {
 }  // namespace
 
 int cheb64_fused(const double2* U, int L, double lam_l, double lam_c, int deg, const double2* x, double2* y,
-                 double2* tmp, size_t ld, GridBar* bar, cudaStream_t st) {
+                 double2* tmp, size_t ld, GridBar* bar, int* herr, cudaStream_t st) {
   const double c = 2.0 / (lam_l - lam_c);
   const double a = 1.0 + c * lam_c;
   const Lat g = make_lat(L);
@@ -274,13 +276,13 @@ int cheb64_fused(const double2* U, int L, double lam_l, double lam_c, int deg, c
     set_error("cheb64_fused: no co-resident grid for L = %d", L);
     return LAPH_ECUDA;
   }
-  // count and generation back to zero; err is sticky until the owner reads it
-  LAPH_CUDA_TRY(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
+  // the barrier's counter is left ready by every completed launch (its owner
+  // resets it only after a barrier gave up)
   double2* t0 = tmp;
   double2* t1 = tmp + ld;
   Lat gg = g;
   void* args[] = {(void*)&U, (void*)&gg, (void*)&x, (void*)&y, (void*)&t0, (void*)&t1, (void*)&deg, (void*)&c,
-                  (void*)&a, (void*)&bar};
+                  (void*)&a, (void*)&bar, (void*)&herr};
   if (resident)
     LAPH_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_cheb64_fused<true>, dim3(grid), dim3(128), args,
                                               kFusedSmem, st));
