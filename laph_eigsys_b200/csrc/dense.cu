@@ -23,11 +23,15 @@
 
 namespace laph {
 
-// d(8x8, 2 per thread) += a(8x4, 1 per thread) b(4x8, 1 per thread), FP64 tensor MMA
+// d(8x8, 2 per thread) += a(8x4, 1 per thread) b(4x8, 1 per thread), FP64 tensor MMA.
+// Not volatile: a pure function of its operands, so the compiler may schedule
+// it; the callers issue the MMAs of one k-step accumulator-major (all tiles'
+// first product, then all tiles' second, ...) so that consecutive MMAs never
+// feed the same accumulator and the tensor pipe does not wait on its latency.
 __device__ __forceinline__ void dmma884(double (&acc)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(acc[0]), "+d"(acc[1])
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(acc[0]), "+d"(acc[1])
+      : "d"(a), "d"(b));
 }
 
 // ------------------------------------------------------------------ Gram ---
@@ -122,16 +126,27 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
         br[j] = bb.x;
         bi[j] = bb.y;
       }
+      // below the diagonal of a diagonal tile: never read
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          if (diag && i > j) continue;  // below the diagonal of a diagonal tile: never read
-          dmma884(accr[i][j], wr[i], br[j]);
-          dmma884(accr[i][j], wi[i], bi[j]);
-          dmma884(acci[i][j], wr[i], bi[j]);
-          dmma884(acci[i][j], wn[i], br[j]);
-        }
+        for (int j = 0; j < 4; ++j)
+          if (!diag || i <= j) dmma884(accr[i][j], wr[i], br[j]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (!diag || i <= j) dmma884(acci[i][j], wr[i], bi[j]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (!diag || i <= j) dmma884(accr[i][j], wi[i], bi[j]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (!diag || i <= j) dmma884(acci[i][j], wn[i], br[j]);
     }
     __syncthreads();
   }
@@ -682,12 +697,19 @@ __global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd,
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          dmma884(accr[i][j], ar[i], br[j]);
-          dmma884(accr[i][j], ai[i], bn[j]);
-          dmma884(acci[i][j], ar[i], bi[j]);
-          dmma884(acci[i][j], ai[i], br[j]);
-        }
+        for (int j = 0; j < 4; ++j) dmma884(accr[i][j], ar[i], br[j]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma884(acci[i][j], ar[i], bi[j]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma884(accr[i][j], ai[i], bn[j]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma884(acci[i][j], ai[i], br[j]);
     }
   }
   cp_async_wait<0>();

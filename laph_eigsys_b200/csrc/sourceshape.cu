@@ -40,10 +40,11 @@ namespace laph {
 namespace {
 
 // d(8x8, 2 per thread) += a(8x4, 1 per thread) b(4x8, 1 per thread), FP64 tensor MMA
+// (not volatile: the compiler may schedule it; issued accumulator-major below)
 __device__ __forceinline__ void dmma884(double (&acc)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(acc[0]), "+d"(acc[1])
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(acc[0]), "+d"(acc[1])
+      : "d"(a), "d"(b));
 }
 
 constexpr int kSsSites = 32;               // sites per tile side
@@ -155,15 +156,23 @@ __global__ void __launch_bounds__(512, 1) k_ss_tile(const double2* __restrict__ 
         bi[j] = b.y;
         bn[j] = -b.y;
       }
+      // accumulator-major: consecutive MMAs never feed the same accumulator
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          dmma884(accr[i][j], ar[i], br[j]);
-          dmma884(accr[i][j], ai[i], bi[j]);
-          dmma884(acci[i][j], ai[i], br[j]);
-          dmma884(acci[i][j], ar[i], bn[j]);
-        }
+        for (int j = 0; j < 3; ++j) dmma884(accr[i][j], ar[i], br[j]);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) dmma884(acci[i][j], ai[i], br[j]);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) dmma884(accr[i][j], ai[i], bi[j]);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) dmma884(acci[i][j], ar[i], bn[j]);
     }
     __syncthreads();
   }
