@@ -110,7 +110,9 @@ int cheb64(const double2* U, int L, double lam_l, double lam_c, int deg, const d
 // adds 1 to the counter except CTA 0, which adds 2^31 - (nblk - 1), so the
 // last arrival flips bit 31 and leaves the low bits at zero for the next
 // barrier; a CTA waits for bit 31 to differ from the value its own add
-// returned (no reset, no second word).  A CTA that waits longer than
+// returned (no reset, no second word).  The add is a release and the polling
+// load an acquire at GPU scope; with the CTA barriers on either side they order
+// every thread's step-n writes before every thread's step-n+1 reads.  A CTA that waits longer than
 // kBarSpinLimit polls sets `err` (and *herr, page-locked host memory the host
 // reads after its synchronisation) and every CTA leaves at its next barrier.
 // Cooperative launches guarantee co-residency, so the limit is a safety net.
@@ -127,8 +129,10 @@ __device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblk, int* her
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (nblk - 1) : 1u;
-    __threadfence();  // this CTA's writes before its arrival
-    const unsigned old = atomicAdd(&b->count, inc);
+    // release: the CTA's writes (ordered before this thread by the CTA barrier
+    // above) become visible to every CTA whose acquire load sees this arrival
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(&b->count), "r"(inc) : "memory");
     bool ok = true;
     unsigned it = 0;
     while (((ld_acquire_gpu(&b->count) ^ old) & 0x80000000u) == 0) {
@@ -139,7 +143,6 @@ __device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblk, int* her
         break;
       }
     }
-    __threadfence();
     s_ok = ok && *reinterpret_cast<volatile int*>(&b->err) == 0;
   }
   __syncthreads();
