@@ -65,12 +65,12 @@ def test_matmult_parity(gpu, orc, L, deg):
     ctx.close()
 
 
-@pytest.mark.parametrize("L,deg", [(32, 12), (36, 5), (5, 7)])
+@pytest.mark.parametrize("L,deg", [(32, 12), (16, 9), (24, 8), (36, 5), (5, 7)])
 def test_matmult_fused_launch_shapes(gpu, orc, L, deg):
     """The one-launch product at the largest lattice whose sites all fit the device's co-resident CTAs one per
-    thread (32^3: 256 CTAs, links held in registers and shared memory), beyond it (36^3: grid-stride, links read
-    per step) and at a ragged last CTA (5^3 = 125 sites), against the oracle's tv_iter, through host and device
-    pointers, twice in a row on one context."""
+    thread (32^3: 256 CTAs, links held in registers and shared memory), at 16^3 and 24^3, beyond co-residency
+    (36^3: grid-stride, links read per step) and at a ragged last CTA (5^3 = 125 sites), against the oracle's
+    tv_iter, through host and device pointers, twice in a row on one context."""
     import torch
     U = random_links(L, 0.3, 1500 + L)
     lam_l, lam_c = 12.0, 0.7
