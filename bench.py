@@ -26,7 +26,7 @@ cpu_baseline: the CPU FP64 oracle (restated reference ev_ts path: stout
         workload, all host cores.
 Also reported: the plain GPU form (MatShell + Krylov-Schur, its one-launch
 MatMult event-timed), the learned window against the non-learned one on the
-headline batch (window_ab), sub-records of the survey's other configurations
+headline batch (window_ab), sub-records of the other benchmark configurations
 (C1 with parity, C2 with parity, C3 with BF16 links, a wave of C4's mixed
 volumes, a wave of C5), the source shape and displacement kernels on the
 solved eigenvectors with an FP64 peak measured in place, the LIME reader's
@@ -354,7 +354,7 @@ def run_reference(args, cfg):
 
 
 def solve_config(cfg, device, reps=1, window=None, link_prec=None, wave=None, parity=None, no_cpu=False):
-    """One configuration of the survey as a compact sub-record: its batch (or one memory-bounded wave of it) solved
+    """One benchmark configuration as a compact sub-record: its batch (or one memory-bounded wave of it) solved
     once untimed (graph capture) and `reps` times timed with CUDA events on the solver's stream, with iterations,
     residual, the filter's algorithmic bandwidth and, where asked, parity of timeslice 0 (or all timeslices of a
     small lattice) against the oracle.  Everything here runs outside the headline's timed region."""
@@ -649,7 +649,7 @@ def main():
                     help="drive the outer iteration from the host (same kernels; ncu cannot profile kernels inside "
                          "a graph with conditional nodes)")
     ap.add_argument("--no-configs", action="store_true",
-                    help="skip the learned-window A/B and the sub-records of the other survey configurations")
+                    help="skip the learned-window A/B and the sub-records of the other benchmark configurations")
     ap.add_argument("--autotune", type=int, default=4, metavar="NSAMPLE",
                     help="tune deg / block / guard on the first NSAMPLE timeslices before measuring (0: off, the "
                          "configuration's own settings)")
@@ -756,7 +756,7 @@ def main():
 
     # ---- roofline of lap_cheb_mrhs -----------------------------------------
     # algorithmic bytes of the timed filter passes, counted by the solver pass by pass (each pass's own degree,
-    # its unlocked columns and column blocks): what the correction-form recurrence moves, and the survey's unit
+    # its unlocked columns and column blocks): what the correction-form recurrence moves, and the unit
     # of one step Y = 2BX - Z (72 B per site-vector-step + links once per column block)
     kb = cfg["block"] or 32
     link_b = 112 if cfg["link_prec"] == "bf16" else 216
@@ -863,7 +863,7 @@ def main():
 
     timings_last = solver.timings()
     solver.close()
-    # ---- learned window A/B and the survey's other configurations (rank 0, N = 1, untimed for the headline) --
+    # ---- learned window A/B and the other benchmark configurations (rank 0, N = 1, untimed for the headline) --
     window_ab = configs = None
     if rank == 0 and world == 1 and not args.no_configs and args.config == "c3":
         torch.cuda.synchronize()

@@ -1,4 +1,4 @@
-"""Parity at the survey's benchmark configurations, against the FP64 oracle,
+"""Parity at the benchmark configurations, against the FP64 oracle,
 with every error stated (printed) as well as bounded:
 
   C1  8^3 x 16, eps 0.4, seed 1227, stout 3 x 0.1 (the reference's backward

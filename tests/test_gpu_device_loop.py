@@ -66,7 +66,7 @@ def test_device_loop_reports_not_converged_at_max_it(gpu):
 
 
 def test_uneven_batch_in_one_launch_matches_oracle_krylov_schur(gpu, orc):
-    """16^3 (nev 60) and 24^3 (nev 120) timeslices, APE 0.5 x 10 as the survey's mixed-volume configuration, in one
+    """16^3 (nev 60) and 24^3 (nev 120) timeslices, APE 0.5 x 10 as the mixed-volume benchmark configuration, in one
     batch and one graph launch, each against the oracle's smearing + FP64 Krylov-Schur on T_12(B): eigenvalues
     (Rayleigh quotients) to 1e-10 relative each, residuals at the tolerance, tr(V^dag V) = nev, and the nev-block
     subspace to the residual over the gap.  The oracle's Krylov-Schur runs at 1e-10 relative to |theta| (near the
