@@ -182,7 +182,7 @@ typedef struct {
   int window;           /* LAPH_WINDOW_*                                          */
   double lam_cut;       /* fixed window: cut (<= 0: from the first Rayleigh-Ritz) */
   double lam_max;       /* fixed window: upper end (<= 0: Lanczos bound)          */
-  int deg;              /* filter degree cap, 2..64 (default 16; 48-60 measured
+  int deg;              /* filter degree cap, 2..128 (default 16; 48-60 measured
                            best at 24^3-48^3; laph_solver_autotune picks it)     */
   int phase_fix;        /* apply fix_phase to the output eigenvectors             */
   uint64_t seed;        /* start block                                            */
@@ -303,7 +303,7 @@ int laph_autotune_search(const int* deg_c, int nd, const int* block_c, int nb, c
  * setting that does not converge within opts->max_it is dropped.  model /
  * nmodel: the window model (as laph_solver_set_window_model) when
  * opts->window is LAPH_WINDOW_MLP, else ignored (may be NULL).  Candidates:
- * deg 40, 48, 56, 60, 64 (start: opts->deg, or 60 if <= 1), block 8, 16, 32, 64
+ * deg 40, 48, 56, 60, 64, 72, 80, 96 (start: opts->deg, or 60 if <= 1), block 8, 16, 32, 64
  * (start: opts->block, or 32), guard opts->guard, opts->guard + 32 and the fewest
  * (>= 4) that give the smallest block width above nev + 4, then the
  * filter's tile of 64, 128 or 256 sites per CTA (start: opts->filter_tile, or

@@ -212,10 +212,10 @@ int laph_solver_autotune(const laph_problem* probs, int n, const double* const* 
     opts->filter_tile = out->tile;
     return LAPH_OK;
   }
-  const int deg0 = opts->deg > 1 ? std::min(opts->deg, 64) : 60;
+  const int deg0 = opts->deg > 1 ? std::min(opts->deg, 96) : 60;
   const int block0 = opts->block > 0 ? opts->block : 32;
   const int guard0 = opts->guard;
-  const int degs[] = {40, 48, 56, 60, 64};
+  const int degs[] = {40, 48, 56, 60, 64, 72, 80, 96};
   const int blocks[] = {8, 16, 32, 64};
   // guard: the given one, 32 more, and the fewest (>= 4) that keep the block width at its smallest multiple of 32
   // (nev 120: guard 8, k = 128 instead of 160 -- less work per pass against slower convergence of the top pairs)
@@ -225,7 +225,7 @@ int laph_solver_autotune(const laph_problem* probs, int n, const double* const* 
     guards.push_back(gmin);
   const int tile0 = opts->filter_tile > 0 ? opts->filter_tile : 128;
   SampleCtx ctx{probs, ns, links, layout, *opts, model, nmodel, device, LAPH_OK, tile0};
-  int st = laph_autotune_search(degs, 5, blocks, 4, guards.data(), (int)guards.size(), deg0, block0, guard0,
+  int st = laph_autotune_search(degs, 8, blocks, 4, guards.data(), (int)guards.size(), deg0, block0, guard0,
                                 sample_trial, &ctx, out);
   if (st != LAPH_OK) {
     if (ctx.last_status != LAPH_OK && ctx.last_status != LAPH_ENOTCONV)

@@ -5,6 +5,9 @@
 #include "common.cuh"
 
 namespace laph {
+// Largest filter degree of a pass (laph_solve_opts.deg).
+constexpr int kMaxFilterDeg = 128;
+
 
 // One problem (timeslice).  All offsets are in elements of the pool they
 // index.  Blocks of k vectors are column-major with column stride dim.

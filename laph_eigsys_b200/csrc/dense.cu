@@ -581,7 +581,7 @@ __global__ void k_coef(const ProbDesc* __restrict__ pd, const ProbState* __restr
   double* tc = tcoef + d.tc;
   for (int j = threadIdx.x; j < k; j += blockDim.x) {
     const double tb = 1.0 + 2.0 * (S.lam_cut - th[j]) / (S.lam_max - S.lam_cut);
-    double tn[66], nu[66];
+    double tn[kMaxFilterDeg + 2], nu[kMaxFilterDeg + 2];
     tn[0] = 1.0;
     tn[1] = tb;
     for (int n = 2; n <= m; ++n) tn[n] = 2.0 * tb * tn[n - 1] - tn[n - 2];

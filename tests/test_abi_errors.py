@@ -40,7 +40,7 @@ def _solver_create(probs, n=None, **kw):
 
 @pytest.mark.parametrize("probs,kw", [
     ([(8, 10)], {"deg": 1}),
-    ([(8, 10)], {"deg": 65}),
+    ([(8, 10)], {"deg": 129}),
     ([(8, 10)], {"guard": -1}),
     ([(8, 10)], {"tol": 0.0}),
     ([(8, 10)], {"tol": float("nan")}),
