@@ -188,9 +188,15 @@ typedef struct {
   uint64_t seed;        /* start block                                            */
   int block;            /* columns per CTA of the filter kernel, 1..512 (0: 32);
                            above 64 the filter runs as variant 0               */
-  int filter_kernel;    /* filter variant, both with register-resident links and L2
-                           bulk prefetch: 0 FP64 coefficients per thread; 1 FP32
-                           coefficients staged per CTA (default; block <= 64)    */
+  int filter_kernel;    /* filter variant, all with register-resident forward
+                           links and L2 bulk prefetch: 0 FP64 coefficients per
+                           thread; 1 FP32 coefficients staged per CTA, backward
+                           links in shared memory (default; block <= 64); 2 as 1
+                           with the backward links in tensor memory; 3 as 2 with
+                           the vectors staged by a bulk-copy pipeline; 4 as 2 on
+                           512-site bricks (2-4: block <= 64; 3 and 4 need every
+                           L in {16, 32, 64, 128}, else 1 runs).  All give the
+                           same results bit for bit; 1 is the fastest measured  */
   int jacobi_sweeps;    /* cap on Jacobi sweeps per Rayleigh-Ritz (0: 2); an
                            unfinished sweep set only delays convergence, since
                            residuals are always computed from the new vectors   */

@@ -9,12 +9,19 @@ int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const dou
 // One Chebyshev step Y_j = a_j (c_hop hop(X_j) + c_diag X_j) + z_j Z_j + g_j S_j (FP32)
 // with (a, z, g) = tcoef[step][0..2][j]; final_step writes W_j = tcoef[step+1][0][j] V_j + Y_j
 // in FP64 instead of Y.  variant 0: per-thread FP64 coefficients; 1: FP32 coefficients
-// staged in shared memory (kb <= 64; larger blocks take variant 0).  tile: sites per
-// CTA of variant 1 (64, 128 or 256; variant 0 uses 128); nblk must match it.
+// staged in shared memory, backward links in shared memory; 2: as 1 with the backward
+// links in tensor memory; 3: as 2 with every vector operand staged in shared memory by a
+// bulk-copy pipeline (needs tile 128 and cheb_staged_ok(L) for every problem; lmax = the
+// largest L of the batch; a pipeline wait that gives up sets *err); 4: as 2 on 512-site
+// bricks (TX = 128 / L planes x 4 z-rows; tile 512, same L condition).  Variants 1-4 need
+// kb <= 64; larger blocks take variant 0.  tile: sites per CTA of variants 1 and 2 (64,
+// 128 or 256; variant 0 uses 128); nblk must match it.
 int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
               const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
               const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant, int tile,
-              cudaStream_t st);
+              int lmax, int* err, cudaStream_t st);
+// Whether a lattice of extent L takes the staged variant (L even, L | 128, 128 | L^2, L <= 128).
+bool cheb_staged_ok(int L);
 // Opt the filter's 256-site tile into its dynamic shared memory on the current device.
 int cheb_init();
 // Opt the FP64 stencil into its dynamic shared memory on the current device.

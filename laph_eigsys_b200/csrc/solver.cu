@@ -53,6 +53,8 @@ struct laph_solver {
   cudaStream_t st = nullptr;
   laph_solve_opts o{};
   int np = 0, mdeg = 16, kb = 32, tile = 128;
+  int fvariant = 1, lmax = 0;  // filter variant in use (opts.filter_kernel, or 1 where 3 does not apply)
+  int* d_ferr = nullptr;       // set by the staged filter when a pipeline wait gives up
   std::vector<ProbDesc> hd;
   ProbDesc* d_pd = nullptr;
   ProbState* d_ps = nullptr;
@@ -179,7 +181,7 @@ int laph_solver_destroy(laph_solver* s) {
                   s->st_col, s->U64raw, s->U64, s->Utmp, s->dec, s->stage, s->Uf32, s->Ubf, s->scale, s->V, s->W, s->Y, s->S, s->E[0],
                   s->E[1], s->E[2], s->KK, s->gpart, s->rpart, s->theta, s->tcoef, s->scol, s->dwork, s->resid,
                   s->phases, s->norms, s->d_nactive, s->model, s->feats, s->mwork, s->bound, s->plaq, s->wdeg,
-                  s->tstamp, s->ls, s->d_degs, s->d_lam_max0, s->d_fallback, s->d_steps, s->d_ps0};
+                  s->tstamp, s->ls, s->d_degs, s->d_lam_max0, s->d_fallback, s->d_steps, s->d_ps0, s->d_ferr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (s->h_nactive) cudaFreeHost(s->h_nactive);
@@ -211,10 +213,10 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     return LAPH_EINVAL;
   }
   if (opts->deg < 2 || opts->deg > kMaxFilterDeg || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1 ||
-      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 1 ||
+      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 4 ||
       (opts->filter_tile != 0 && opts->filter_tile != 64 && opts->filter_tile != 128 && opts->filter_tile != 256)) {
     set_error("laph_solver_create: need 2 <= deg <= 128, guard >= 0, tol > 0, max_it >= 1, 0 <= block <= 512, "
-              "filter_kernel in {0, 1}, filter_tile in {0, 64, 128, 256}");
+              "filter_kernel in {0, ..., 4}, filter_tile in {0, 64, 128, 256}");
     return LAPH_EINVAL;
   }
   for (int i = 0; i < n; ++i) {
@@ -243,7 +245,16 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   s->mdeg = opts->deg;
   s->kb = opts->block > 0 ? opts->block : 32;
   // sites per CTA of the filter; the per-thread-coefficient variant and blocks wider than 64 keep 128
-  s->tile = opts->filter_tile > 0 && opts->filter_kernel == 1 && s->kb <= 64 ? opts->filter_tile : 128;
+  s->tile = opts->filter_tile > 0 && opts->filter_kernel >= 1 && s->kb <= 64 ? opts->filter_tile : 128;
+  // the staged variant (3) needs 128-site tiles of whole z-rows inside one plane for every problem
+  s->fvariant = opts->filter_kernel;
+  for (int i = 0; i < n; ++i) s->lmax = std::max(s->lmax, probs[i].L);
+  if (s->fvariant >= 3) {  // staged rows (3) or 512-site bricks (4): L in {16, 32, 64, 128} for every problem
+    bool ok = s->kb <= 64;
+    for (int i = 0; i < n; ++i) ok = ok && cheb_staged_ok(probs[i].L);
+    if (ok) s->tile = s->fvariant == 4 ? 512 : 128;
+    else s->fvariant = 1;
+  }
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     set_error("laph_solver_create: cannot use device %d", device);
@@ -321,8 +332,9 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
       (rc = dalloc(&s->tstamp, (size_t)n * kSmallPhases)) || (rc = dalloc(&s->ls, 1)) ||
       (rc = dalloc(&s->d_degs, (size_t)opts->max_it + 2)) || (rc = dalloc(&s->d_lam_max0, n)) ||
       (rc = dalloc(&s->d_fallback, n)) || (rc = dalloc(&s->d_steps, (size_t)s->mdeg + 1)) ||
-      (rc = dalloc(&s->d_ps0, n)))
+      (rc = dalloc(&s->d_ps0, n)) || (rc = dalloc(&s->d_ferr, 1)))
     return fail(rc);
+  if (cudaMemset(s->d_ferr, 0, sizeof(int)) != cudaSuccess) return fail(LAPH_ECUDA);
   if (opts->link_prec == LAPH_LINKS_BF16) {
     if ((rc = dalloc(reinterpret_cast<float2**>(&s->Ubf), (size_t)o_uf))) return fail(rc);  // 4 B per element
   } else {
@@ -446,7 +458,7 @@ static int filter_step(laph_solver* s, int n, bool fin, cudaStream_t st) {
   const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
   float2* Yo = s->E[(n - 1) % 3];
   return cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo, s->V,
-                   s->W, s->tcoef, n, fin, s->o.filter_kernel, s->tile, st);
+                   s->W, s->tcoef, n, fin, s->fvariant, s->tile, s->lmax, s->d_ferr, st);
 }
 
 static int filter(laph_solver* s, int m) {
@@ -571,6 +583,14 @@ static int solve_setup(laph_solver* s, bool device_loop, long long* nlaunch_out)
 static int fill_results(laph_solver* s, laph_result* res) {
   const laph_solve_opts& o = s->o;
   int status = LAPH_OK;
+  if (s->fvariant == 3) {
+    int ferr = 0;
+    if (cudaMemcpy(&ferr, s->d_ferr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return LAPH_ECUDA;
+    if (ferr != 0) {
+      set_error("laph_solver_run: the staged filter's copy pipeline failed (code %d); results are invalid", ferr);
+      return LAPH_ECUDA;
+    }
+  }
   for (int i = 0; i < s->np; ++i) {
     const ProbState& p = s->hps[i];
     if (p.active) status = LAPH_ENOTCONV;

@@ -135,15 +135,37 @@ def test_async_read_back_overlaps_the_next_run(gpu):
 def test_filter_tiles_are_bitwise_identical(gpu, prec):
     """The filter's site tile (64, 128 or 256 sites per CTA, an autotuner axis) changes only which CTA computes a
     site, not the arithmetic: every tile gives bitwise the same eigenpairs, on a batch with a ragged last tile
-    (10^3 = 1000 sites, 12^3 = 1728)."""
+    (10^3 = 1000 sites, 12^3 = 1728).  The same holds for where the backward links wait between columns (shared
+    memory, filter_kernel 1, or tensor memory, filter_kernel 2): both run the same FMAs in the same order."""
     probs = [(10, 24), (12, 30)]
     links = [random_links(L, 0.35, 3400 + i) for i, (L, _) in enumerate(probs)]
     outs = []
-    for tile in (64, 128, 256):
-        o = _solve(gpu, probs, links, guard=16, tol=1e-10, deg=24, filter_tile=tile,
-                   link_prec=gpu.LINKS_BF16 if prec == "bf16" else gpu.LINKS_FP32)
-        assert o["status"] == 0
-        outs.append(o)
+    for variant in (1, 2):
+        for tile in (64, 128, 256):
+            o = _solve(gpu, probs, links, guard=16, tol=1e-10, deg=24, filter_tile=tile, filter_kernel=variant,
+                       link_prec=gpu.LINKS_BF16 if prec == "bf16" else gpu.LINKS_FP32)
+            assert o["status"] == 0
+            outs.append(o)
     for o in outs[1:]:
         for (ea, va, _), (eb, vb, _) in zip(outs[0]["eig"], o["eig"]):
             assert np.array_equal(ea, eb) and np.array_equal(va, vb)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_staged_filter_is_bitwise_identical(gpu, prec):
+    """filter_kernel 3 feeds the same column loop from a bulk-copy pipeline (X with its x- and y-neighbour rows, S
+    and Z staged in shared memory) instead of global loads: the same FMAs in the same order, so the eigenpairs match
+    filter_kernel 1 bit for bit.  The batch mixes 16^3 and 32^3 timeslices (two tile geometries in one launch, the
+    ring sized for L = 32); a batch with a lattice the staged tiles do not fit (12^3) runs variant 1 instead.
+    filter_kernel 4 (the same loop as variant 2 on 512-site bricks of TX planes x 4 z-rows) must match as well."""
+    lp = gpu.LINKS_BF16 if prec == "bf16" else gpu.LINKS_FP32
+    for probs in ([(16, 40), (32, 24), (16, 20)], [(12, 30), (16, 24)]):
+        links = [random_links(L, 0.35, 3500 + i) for i, (L, _) in enumerate(probs)]
+        outs = [_solve(gpu, probs, links, guard=16, tol=1e-10, deg=24, filter_kernel=v, link_prec=lp)
+                for v in (1, 3, 4)]
+        for o in outs:
+            assert o["status"] == 0
+        for o in outs[1:]:
+            for (ea, va, pa), (eb, vb, pb) in zip(outs[0]["eig"], o["eig"]):
+                assert np.array_equal(ea, eb) and np.array_equal(va, vb) and np.array_equal(pa, pb)
+            assert outs[0]["res"][0]["iters"] == o["res"][0]["iters"]
