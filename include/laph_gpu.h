@@ -59,6 +59,25 @@ int laph_binary_version(int* version);
  * No counterpart in the reference. */
 int laph_probe_fp64(int device, double* fma_tflops, double* dmma_tflops);
 
+/* ---- bounds-checked build ---------------------------------------------------
+ * liblaph_gpu_check.so is the same library compiled with -DLAPH_CHECK: every
+ * lattice neighbour index, the filter's coefficient and staging offsets and
+ * the dense kernels' tile and column indices are checked against their ranges
+ * in the kernels.  An index out of range is counted and the first one
+ * recorded, and its access goes to index 0 instead (nothing traps, nothing
+ * leaves its buffer).  No counterpart in the reference (it has no sanitizer
+ * runs).  laph_check_enabled: 1 in the checked build, 0 otherwise.
+ * laph_check_report: *count = indices out of range so far, summed over the
+ * library's translation units; the first one's value, bound, source line and
+ * unit (any pointer but count may be NULL); reset != 0 clears the records.
+ * In the normal build *count is always 0.  laph_check_selftest (checked build
+ * only; LAPH_EINVAL otherwise) runs a kernel that checks one index past its
+ * bound, which the next report shows. */
+int laph_check_enabled(void);
+int laph_check_report(unsigned long long* count, long long* index, long long* bound, int* line, char* unit,
+                      int unit_len, int reset);
+int laph_check_selftest(int device);
+
 /* ---- link layouts accepted at the boundary -------------------------------- */
 enum {
   LAPH_LAYOUT_ROWMAJOR = 0, /* double[V3][3][3][3][2]: [site][dir][a][b][re,im]                */

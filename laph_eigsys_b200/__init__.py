@@ -389,6 +389,25 @@ def probe_fp64(device=0):
     return a.value, b.value
 
 
+def check_report(reset=False):
+    """Indices found out of range by the bounds-checked build (laph_check_report): a dict with the count and, when
+    it is not zero, the first one's value, bound, source line and translation unit.  Always a count of 0 in the
+    normal build (check_enabled() tells which build is loaded)."""
+    n, i, b, ln = ctypes.c_uint64(), ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int()
+    unit = ctypes.create_string_buffer(256)
+    check(lib.laph_check_report(ctypes.byref(n), ctypes.byref(i), ctypes.byref(b), ctypes.byref(ln), unit, 256,
+                                1 if reset else 0), "laph_check_report")
+    out = {"count": n.value}
+    if n.value:
+        out.update(index=i.value, bound=b.value, line=ln.value, unit=unit.value.decode())
+    return out
+
+
+def check_enabled():
+    """True when the loaded library is the bounds-checked build (LAPH_GPU_LIB=check)."""
+    return bool(lib.laph_check_enabled())
+
+
 def solve_opts(**kw):
     o = _lib.laph_solve_opts()
     lib.laph_solve_opts_default(ctypes.byref(o))

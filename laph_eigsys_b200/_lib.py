@@ -2,16 +2,22 @@
 
 The shared library is built in-tree (laph_eigsys_b200/liblaph_gpu.so).  There
 is no fallback: if the library is missing, importing this module raises.
+LAPH_GPU_LIB=check selects the bounds-checked build of the same sources
+(liblaph_gpu_check.so, -DLAPH_CHECK) instead.
 """
 import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblaph_gpu.so")
+_VARIANTS = {"": "liblaph_gpu.so", "check": "liblaph_gpu_check.so"}
+_variant = os.environ.get("LAPH_GPU_LIB", "")
+if _variant not in _VARIANTS:
+    raise ImportError(f"LAPH_GPU_LIB={_variant!r}: expected one of {sorted(_VARIANTS)}")
+LIB_PATH = os.path.join(_HERE, _VARIANTS[_variant])
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
-        f"{LIB_PATH} is missing: build it with `make -C laph_eigsys_b200/csrc` "
+        f"{LIB_PATH} is missing: build it with `make -C laph_eigsys_b200/csrc all check` "
         "(or __graft_entry__.build()); there is no CPU fallback")
 
 lib = ctypes.CDLL(LIB_PATH)
@@ -107,6 +113,9 @@ _sig("laph_solver_loop_info", c_int, c_void_p, P(c_int), P(ctypes.c_longlong))
 _sig("laph_ctx_stream", c_int, c_void_p, P(c_void_p))
 _sig("laph_binary_version", c_int, P(c_int))
 _sig("laph_probe_fp64", c_int, c_int, P(c_double), P(c_double))
+_sig("laph_check_enabled", c_int)
+_sig("laph_check_report", c_int, P(c_u64), P(c_ll), P(c_ll), P(c_int), c_char_p, c_int, c_int)
+_sig("laph_check_selftest", c_int, c_int)
 _sig("laph_solver_set_window_model", c_int, c_void_p, c_void_p, c_int)
 _sig("laph_solver_features", c_int, c_void_p, c_void_p, c_void_p)
 _sig("laph_solver_ritz", c_int, c_void_p, c_int, c_void_p, P(c_int))

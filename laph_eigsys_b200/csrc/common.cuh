@@ -8,6 +8,7 @@
 #include <string>
 
 #include "../../include/laph_gpu.h"
+#include "check.cuh"
 
 namespace laph {
 
@@ -90,15 +91,16 @@ __host__ __device__ __forceinline__ int nb_up(const Lat& g, int x, int y, int z,
   if (dir == 0) x = (x + 1 == g.L) ? 0 : x + 1;
   else if (dir == 1) y = (y + 1 == g.L) ? 0 : y + 1;
   else z = (z + 1 == g.L) ? 0 : z + 1;
-  return x * g.L2 + y * g.L + z;
+  return LAPH_IX(x * g.L2 + y * g.L + z, g.V3);
 }
 __host__ __device__ __forceinline__ int nb_dn(const Lat& g, int x, int y, int z, int dir) {
   if (dir == 0) x = (x == 0) ? g.L - 1 : x - 1;
   else if (dir == 1) y = (y == 0) ? g.L - 1 : y - 1;
   else z = (z == 0) ? g.L - 1 : z - 1;
-  return x * g.L2 + y * g.L + z;
+  return LAPH_IX(x * g.L2 + y * g.L + z, g.V3);
 }
 __host__ __device__ __forceinline__ void site_xyz(const Lat& g, int s, int& x, int& y, int& z) {
+  s = LAPH_IX(s, g.V3);
   x = s / g.L2;
   const int r = s - x * g.L2;
   y = r / g.L;

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
     pr -= T - ti;
     ++ti;
   }
-  const int tj = ti + pr;
+  const int tj = LAPH_IX(ti + pr, T);
   if ((tj + 1) * GT <= ps[p].c0) return;  // both tiles frozen: not needed
   const double2* A = W + d.blk + (size_t)(ti * GT) * d.dim;
   const double2* BW = W + d.blk + (size_t)(tj * GT) * d.dim;
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
       const int row = r + q;
       const bool ok = row < r1;
       const size_t off = (size_t)c * d.dim + (ok ? row : 0);
-      cp_async16(s + c * GP + q, A + off, ok);
+      cp_async16(s + LAPH_IX(c * GP + q, GT * GP), A + off, ok);
       cp_async16(s + (GT + c) * GP + q, BW + off, ok);
       cp_async16(s + (2 * GT + c) * GP + q, BY + off, ok);
     }
@@ -654,13 +654,13 @@ __global__ void __launch_bounds__(128) k_rotate(const ProbDesc* __restrict__ pd,
       const int c = idx >> 7, r = idx & 127;
       const int row = row0 + r;
       const bool ok = row < d.dim;
-      cp_async16(sW + c * RR + r, Wb + (size_t)(q0 + c) * d.dim + (ok ? row : 0), ok);
+      cp_async16(sW + c * RR + r, Wb + (size_t)LAPH_IX(q0 + c, k) * d.dim + (ok ? row : 0), ok);
     }
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const int idx = threadIdx.x + 128 * e;
       const int c = idx & 31, r = idx >> 5;
-      cp_async16(sC + r * RC + c, C + (size_t)(col0 + c) * k + q0 + r, true);
+      cp_async16(sC + r * RC + c, C + (size_t)LAPH_IX(col0 + c, k) * k + LAPH_IX(q0 + r, k), true);
     }
     cp_async_commit();
   };
@@ -835,7 +835,7 @@ __global__ void __launch_bounds__(kSites64, 3)
     const double2* x = Vp + col;
     double2 acc[3];
     hop64_col(l, sUb, d.V3, up, dn, x, acc);
-    const double th = __ldg(theta + d.kv + j);
+    const double th = __ldg(theta + d.kv + LAPH_IX(j, d.k));
     double r2 = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(kSites64, 3)
       r2 += r.x * r.x + r.y * r.y;
       if (valid) Sp[col + (size_t)a * d.V3 + s] = make_float2((float)(sc * r.x), (float)(sc * r.y));
     }
-    sPart[j - j0][threadIdx.x] = valid ? (float)r2 : 0.f;
+    sPart[LAPH_IX(j - j0, kColsFP64)][threadIdx.x] = valid ? (float)r2 : 0.f;
   }
   __syncthreads();
   // column c = tid / 4 summed by 4 threads over 32 sites each, then across them

@@ -272,8 +272,8 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
     for (int j = j0 + (int)threadIdx.x; j < j1; j += NT) {
       const double a = tc[j];
-      cf[j - j0] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
-      if (FINAL) ctm[j - j0] = tc[(size_t)3 * d.k + j];
+      cf[LAPH_IX(j - j0, kCoefMax)] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
+      if (FINAL) ctm[LAPH_IX(j - j0, kCoefMax)] = tc[(size_t)3 * d.k + j];
     }
   }
   __syncthreads();
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
       const float2 pp = unpk2(P[a]), tt = unpk2(T[a]);
       acc[a] = make_float2(pp.x - tt.y, pp.y + tt.x);
     }
-    const float4 q = cf[j - j0];  // (a c_hop, a c_diag, z, g)
+    const float4 q = cf[LAPH_IX(j - j0, kCoefMax)];  // (a c_hop, a c_diag, z, g)
     const size_t col = base + (size_t)j * d.dim;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
       if (FINAL) {
         const size_t iv = col + (size_t)a * d.V3 + s;
         const double2 v = __ldg(Vp + iv);
-        const double tm = ctm[j - j0];
+        const double tm = ctm[LAPH_IX(j - j0, kCoefMax)];
         Wp[iv] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
       } else {
         Yp[col + (size_t)a * d.V3 + s] = r;
@@ -445,8 +445,8 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
     for (int j = j0 + (int)threadIdx.x; j < j1; j += NT) {
       const double a = tc[j];
-      cf[j - j0] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
-      if (FINAL) ctm[j - j0] = tc[(size_t)3 * d.k + j];
+      cf[LAPH_IX(j - j0, kCoefMax)] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
+      if (FINAL) ctm[LAPH_IX(j - j0, kCoefMax)] = tc[(size_t)3 * d.k + j];
     }
   }
   if (threadIdx.x < 32) tmem_alloc_warp(&tm_base, kTmCols);
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         }
       }
     }
-    const float4 q = cf[j - j0];  // (a c_hop, a c_diag, z, g)
+    const float4 q = cf[LAPH_IX(j - j0, kCoefMax)];  // (a c_hop, a c_diag, z, g)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const float2 pp = unpk2(P[a]), tt = unpk2(T[a]);
@@ -566,7 +566,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
       if (FINAL) {
         const size_t iv = col + (size_t)a * d.V3 + s;
         const double2 v = __ldg(Vp + iv);
-        const double tm = ctm[j - j0];
+        const double tm = ctm[LAPH_IX(j - j0, kCoefMax)];
         Wp[iv] = make_double2(fma(tm, v.x, (double)r.x), fma(tm, v.y, (double)r.y));
       } else {
         Yp[col + (size_t)a * d.V3 + s] = r;
@@ -635,8 +635,8 @@ __global__ void __launch_bounds__(kBrickNT, 1)
     const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
     for (int j = j0 + i; j < j1; j += kBrickNT) {
       const double a = tc[j];
-      cf[j - j0] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
-      if (FINAL) ctm[j - j0] = tc[(size_t)3 * d.k + j];
+      cf[LAPH_IX(j - j0, kCoefMax)] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
+      if (FINAL) ctm[LAPH_IX(j - j0, kCoefMax)] = tc[(size_t)3 * d.k + j];
     }
   }
   if (i < 32) tmem_alloc_warp(&tm_base, kTmCols);
@@ -733,7 +733,7 @@ __global__ void __launch_bounds__(kBrickNT, 1)
         }
       }
     }
-    const float4 q = cf[j - j0];  // (a c_hop, a c_diag, z, g)
+    const float4 q = cf[LAPH_IX(j - j0, kCoefMax)];  // (a c_hop, a c_diag, z, g)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const float2 pp = unpk2(P[a]), tt = unpk2(T[a]);
@@ -750,7 +750,7 @@ __global__ void __launch_bounds__(kBrickNT, 1)
       }
       if (FINAL) {
         const double2 v = __ldg(Vp + ia);
-        const double tm = ctm[j - j0];
+        const double tm = ctm[LAPH_IX(j - j0, kCoefMax)];
         Wp[ia] = make_double2(fma(tm, v.x, (double)rr.x), fma(tm, v.y, (double)rr.y));
       } else {
         Yp[ia] = rr;
@@ -830,8 +830,8 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
     for (int j = j0 + (int)threadIdx.x; j < j1; j += NT) {
       const double a = tc[j];
-      cf[j - j0] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
-      if (FINAL) ctm[j - j0] = tc[(size_t)3 * d.k + j];
+      cf[LAPH_IX(j - j0, kCoefMax)] = make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
+      if (FINAL) ctm[LAPH_IX(j - j0, kCoefMax)] = tc[(size_t)3 * d.k + j];
     }
   }
   if (threadIdx.x == 0) {
@@ -958,8 +958,8 @@ __global__ void __launch_bounds__(NT, 512 / NT)
       float2 xu[3], xd[3];
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        xu[b] = sb[b * XC + upl[mu]];
-        xd[b] = sb[b * XC + dnl[mu]];
+        xu[b] = sb[LAPH_IX(b * XC + upl[mu], sstride)];
+        xd[b] = sb[LAPH_IX(b * XC + dnl[mu], sstride)];
       }
       uint32_t w[16], w16, w17;
       __syncwarp();
@@ -983,24 +983,24 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         }
       }
     }
-    const float4 q = cf[j - j0];  // (a c_hop, a c_diag, z, g)
+    const float4 q = cf[LAPH_IX(j - j0, kCoefMax)];  // (a c_hop, a c_diag, z, g)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const float2 pp = unpk2(P[a]), tt = unpk2(T[a]);
       const float2 acc = make_float2(pp.x - tt.y, pp.y + tt.x);
-      const float2 xs = sb[a * XC + i], ss = sb[3 * XC + a * NT + i];
+      const float2 xs = sb[LAPH_IX(a * XC + i, sstride)], ss = sb[LAPH_IX(3 * XC + a * NT + i, sstride)];
       float2 rr;
       rr.x = fmaf(q.x, acc.x, fmaf(q.y, xs.x, q.w * ss.x));
       rr.y = fmaf(q.x, acc.y, fmaf(q.y, xs.y, q.w * ss.y));
       if (HAS_Z) {
-        const float2 zz = sb[3 * XC + 3 * NT + a * NT + i];
+        const float2 zz = sb[LAPH_IX(3 * XC + 3 * NT + a * NT + i, sstride)];
         rr.x = fmaf(q.z, zz.x, rr.x);
         rr.y = fmaf(q.z, zz.y, rr.y);
       }
       if (FINAL) {
         const size_t iv = col + (size_t)a * d.V3 + s;
         const double2 v = __ldg(Vp + iv);
-        const double tm = ctm[j - j0];
+        const double tm = ctm[LAPH_IX(j - j0, kCoefMax)];
         Wp[iv] = make_double2(fma(tm, v.x, (double)rr.x), fma(tm, v.y, (double)rr.y));
       } else {
         Yp[col + (size_t)a * d.V3 + s] = rr;
