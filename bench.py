@@ -635,7 +635,7 @@ def main():
     ap.add_argument("--link-prec", default=None, choices=["bf16", "fp32"])
     ap.add_argument("--timeslices", type=int, default=None)
     ap.add_argument("--block", type=int, default=0)
-    ap.add_argument("--filter-kernel", type=int, default=1, choices=[0, 1, 2, 3, 4])
+    ap.add_argument("--filter-kernel", type=int, default=1, choices=[0, 1, 2, 3, 4, 5])
     ap.add_argument("--guard", type=int, default=None)
     ap.add_argument("--sweeps", type=int, default=0)
     ap.add_argument("--lam-cut0", type=float, default=0.0)
@@ -765,7 +765,7 @@ def main():
     achieved = alg_bytes / (filt_ms / 1000.0) / 1e9 if filt_ms > 0 else None
     achieved_s8d = alg_s8d / (filt_ms / 1000.0) / 1e9 if filt_ms > 0 else None
     fk = cfg.get("filter_kernel", 1)
-    kname = ({2: "k_cheb_mrhs3", 3: "k_cheb_mrhs4", 4: "k_cheb_mrhs5"}.get(fk, "k_cheb_mrhs2")) if fk >= 1 and kb <= 64 else "k_cheb_mrhs"
+    kname = ({2: "k_cheb_mrhs3", 3: "k_cheb_mrhs4", 4: "k_cheb_mrhs5", 5: "k_cheb_mrhs6"}.get(fk, "k_cheb_mrhs2")) if fk >= 1 and kb <= 64 else "k_cheb_mrhs"
     roofline = {"kernel": f"{kname} (lap_cheb_mrhs)", "bound": "hbm", "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm if achieved else None, "peak_source": src,
                 "traffic": NCU_TRAFFIC_RATIO * alg_bytes / max(flaunch, 1) if kname == "k_cheb_mrhs2" else None,

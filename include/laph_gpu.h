@@ -213,9 +213,11 @@ typedef struct {
                            links in shared memory (default; block <= 64); 2 as 1
                            with the backward links in tensor memory; 3 as 2 with
                            the vectors staged by a bulk-copy pipeline; 4 as 2 on
-                           512-site bricks (2-4: block <= 64; 3 and 4 need every
-                           L in {16, 32, 64, 128}, else 1 runs).  All give the
-                           same results bit for bit; 1 is the fastest measured  */
+                           512-site bricks; 5 as 2 with each thread's next-column
+                           operands in flight through cp.async (2-5: block <= 64;
+                           3 and 4 need every L in {16, 32, 64, 128}, else 1
+                           runs).  All give the same results bit for bit; 1 is
+                           the fastest measured                                  */
   int jacobi_sweeps;    /* cap on Jacobi sweeps per Rayleigh-Ritz (0: 2); an
                            unfinished sweep set only delays convergence, since
                            residuals are always computed from the new vectors   */

@@ -580,6 +580,209 @@ __global__ void __launch_bounds__(NT, 512 / NT)
   if (threadIdx.x < 32) tmem_dealloc_warp(base, kTmCols);
 }
 
+// Variant 5: variant 2 with each thread's operands of the next column in
+// flight while it computes the current one.  The filter waits on L2: a warp
+// issues its 27 loads of a column and then has nothing to do until they
+// return.  Here every thread copies its own 27 values of column j + 1 (the 21
+// of X at the site and its six neighbours, S, Z) with cp.async into its own
+// slots of a two-stage shared-memory buffer, then computes column j from the
+// slots filled one column earlier; no thread reads another thread's slots, so
+// there is no CTA barrier, only the thread's own cp.async.wait_group.  The
+// backward links live in tensor memory (as variant 2), so the buffer (27 x 8 B
+// x NT x 2 stages: 55 KB at NT = 128) leaves 4 CTAs per SM.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+constexpr int kPipeSlots = 27;  // per thread and stage: xu[3][3], xd[3][3], xs[3], ss[3], zz[3]
+
+template <typename LT, bool HAS_Z, bool FINAL, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
+    k_cheb_mrhs6(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, const int* __restrict__ start,
+                 int np, int kb, const LT* __restrict__ links, const float* __restrict__ scale,
+                 const float2* __restrict__ Xp, const float2* __restrict__ Zp, const float2* __restrict__ Sp,
+                 float2* __restrict__ Yp, const double2* __restrict__ Vp, double2* __restrict__ Wp,
+                 const double* __restrict__ tcoef, int step) {
+  constexpr uint32_t kTmCols = NT > 128 ? 128u : 64u;
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active) return;
+  const ProbDesc d = pd[p];
+  const int nst = (d.V3 + NT - 1) / NT;
+  const int t = blockIdx.x - start[p];
+  const int st = t % nst, cb = t / nst;
+  const int s_own = st * NT + threadIdx.x;
+  const bool valid = s_own < d.V3;
+  const int s = valid ? s_own : d.V3 - 1;
+  const int j1 = min(cb * kb + kb, d.k);
+  const int nlock = ps[p].nlock;
+  if (FINAL && valid) {
+    for (int j = cb * kb; j < min(j1, nlock); ++j) {
+      const size_t i = (size_t)d.blk + (size_t)j * d.dim + s;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) Wp[i + (size_t)a * d.V3] = __ldg(Vp + i + (size_t)a * d.V3);
+    }
+  }
+  const int j0 = max(cb * kb, nlock);
+  if (j0 >= j1) return;  // uniform over the CTA, before the allocation
+  __shared__ float4 cf[kCoefMax];
+  __shared__ double ctm[kCoefMax];
+  __shared__ uint32_t tm_base;
+  extern __shared__ __align__(16) float2 pipe[];  // [stage][slot][NT]
+  {
+    const double c_hop = ps[p].c_hop, c_diag = ps[p].c_diag;
+    const double* tc = tcoef + d.tc + (size_t)step * 3 * d.k;
+    for (int j = j0 + (int)threadIdx.x; j < j1; j += NT) {
+      const double a = tc[j];
+      cf[LAPH_IX(j - j0, kCoefMax)] =
+          make_float4((float)(a * c_hop), (float)(a * c_diag), (float)tc[d.k + j], (float)tc[2 * d.k + j]);
+      if (FINAL) ctm[LAPH_IX(j - j0, kCoefMax)] = tc[(size_t)3 * d.k + j];
+    }
+  }
+  if (threadIdx.x < 32) tmem_alloc_warp(&tm_base, kTmCols);
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const uint32_t base = tm_base;
+  const uint32_t tl = tmem_lane_addr(base, (threadIdx.x >> 7) * 64u);
+  const Lat g{d.L, d.L * d.L, d.V3};
+  int sx, sy, sz;
+  site_xyz(g, s, sx, sy, sz);
+  int up[3], dn[3];
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu) {
+    up[mu] = nb_up(g, sx, sy, sz, mu);
+    dn[mu] = nb_dn(g, sx, sy, sz, mu);
+  }
+  const size_t bcol = (size_t)d.blk;
+  // this thread's copies of column j into stage b
+  auto issue = [&](int j, int b) {
+    float2* sl = pipe + (size_t)b * kPipeSlots * NT + threadIdx.x;
+    const size_t col = bcol + (size_t)j * d.dim;
+    const float2* x = Xp + col;
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cp_async8(sl + (size_t)(mu * 3 + c) * NT, x + (size_t)c * d.V3 + up[mu]);
+        cp_async8(sl + (size_t)(9 + mu * 3 + c) * NT, x + (size_t)c * d.V3 + dn[mu]);
+      }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cp_async8(sl + (size_t)(18 + c) * NT, x + (size_t)c * d.V3 + s);
+      cp_async8(sl + (size_t)(21 + c) * NT, Sp + col + (size_t)c * d.V3 + s);
+      if (HAS_Z) cp_async8(sl + (size_t)(24 + c) * NT, Zp + col + (size_t)c * d.V3 + s);
+    }
+  };
+  issue(j0, 0);
+  cp_async_commit();
+  const LT* U = links + d.uf;
+  const float* scl = scale + d.sc;
+  float2 uf[3][9];
+#pragma unroll
+  for (int mu = 0; mu < 3; ++mu) {
+    uint32_t w[16], w16 = 0, w17 = 0;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      uf[mu][e] = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + s, s);
+      const float2 bwl = ld_lk(U, scl, (size_t)(mu * 9 + e) * d.V3 + dn[mu], dn[mu]);
+      if (e < 8) {
+        w[2 * e] = __float_as_uint(bwl.x);
+        w[2 * e + 1] = __float_as_uint(-bwl.y);
+      } else {
+        w16 = __float_as_uint(bwl.x);
+        w17 = __float_as_uint(-bwl.y);
+      }
+    }
+    __syncwarp();
+    tmem_st16(tl + 16u * mu, w);
+    tmem_st2(tl + 48u + 2u * mu, w16, w17);
+  }
+  tmem_wait_st();
+  const int s0 = st * NT, nsite = min(NT, d.V3 - s0);
+  const bool pf = threadIdx.x == 0 && (nsite % 2 == 0) && (d.dim % 2 == 0);
+  auto prefetch = [&](int j) {
+    if (!pf || j >= j1) return;
+    const size_t col = bcol + (size_t)j * d.dim;
+    const unsigned bytes = 8u * nsite;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      l2_prefetch(Xp + col + (size_t)c * d.V3 + s0, bytes);
+      l2_prefetch(Sp + col + (size_t)c * d.V3 + s0, bytes);
+      if (HAS_Z) l2_prefetch(Zp + col + (size_t)c * d.V3 + s0, bytes);
+    }
+    if (FINAL)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) l2_prefetch(Vp + col + (size_t)c * d.V3 + s0, 2 * bytes);
+  };
+#pragma unroll 1
+  for (int j = j0 + 1; j < min(j1, j0 + 1 + kPrefetch); ++j) prefetch(j);
+#pragma unroll 1
+  for (int j = j0; j < j1; ++j) {
+    const int b = (j - j0) & 1;
+    prefetch(j + 1 + kPrefetch);
+    if (j + 1 < j1) issue(j + 1, b ^ 1);
+    cp_async_commit();  // possibly empty: the group count stays one per column
+    cp_async_wait<1>();  // this thread's copies of column j have landed
+    const float2* sl = pipe + (size_t)b * kPipeSlots * NT + threadIdx.x;
+    const size_t col = bcol + (size_t)j * d.dim;
+    unsigned long long P[3] = {0ull, 0ull, 0ull}, T[3] = {0ull, 0ull, 0ull};
+#pragma unroll
+    for (int mu = 0; mu < 3; ++mu) {
+      uint32_t w[16], w16, w17;
+      __syncwarp();
+      tmem_ld16(tl + 16u * mu, w);
+      tmem_ld2(tl + 48u + 2u * mu, w16, w17);
+      tmem_wait_ld18(w, w16, w17);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float2 xu = sl[(size_t)(mu * 3 + c) * NT], xd = sl[(size_t)(9 + mu * 3 + c) * NT];
+        const unsigned long long ur = pk2(xu.x, xu.x), ui = pk2(xu.y, xu.y);
+        const unsigned long long dr = pk2(xd.x, xd.x), di = pk2(xd.y, xd.y);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int e = 3 * c + a;
+          const unsigned long long lf = pk2(uf[mu][3 * a + c].x, uf[mu][3 * a + c].y);
+          const unsigned long long lb = e < 8 ? pk2(__uint_as_float(w[2 * e]), __uint_as_float(w[2 * e + 1]))
+                                              : pk2(__uint_as_float(w16), __uint_as_float(w17));
+          ffma2(P[a], ur, lf);
+          ffma2(T[a], ui, lf);
+          ffma2(P[a], dr, lb);
+          ffma2(T[a], di, lb);
+        }
+      }
+    }
+    const float4 q = cf[LAPH_IX(j - j0, kCoefMax)];  // (a c_hop, a c_diag, z, g)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float2 pp = unpk2(P[a]), tt = unpk2(T[a]);
+      const float2 acc = make_float2(pp.x - tt.y, pp.y + tt.x);
+      const float2 xs = sl[(size_t)(18 + a) * NT], ss = sl[(size_t)(21 + a) * NT];
+      float2 rr;
+      rr.x = fmaf(q.x, acc.x, fmaf(q.y, xs.x, q.w * ss.x));
+      rr.y = fmaf(q.x, acc.y, fmaf(q.y, xs.y, q.w * ss.y));
+      if (HAS_Z) {
+        const float2 zz = sl[(size_t)(24 + a) * NT];
+        rr.x = fmaf(q.z, zz.x, rr.x);
+        rr.y = fmaf(q.z, zz.y, rr.y);
+      }
+      if (!valid) continue;
+      if (FINAL) {
+        const size_t iv = col + (size_t)a * d.V3 + s;
+        const double2 v = __ldg(Vp + iv);
+        const double tm = ctm[LAPH_IX(j - j0, kCoefMax)];
+        Wp[iv] = make_double2(fma(tm, v.x, (double)rr.x), fma(tm, v.y, (double)rr.y));
+      } else {
+        Yp[col + (size_t)a * d.V3 + s] = rr;
+      }
+    }
+  }
+  cp_async_wait<0>();
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  if (threadIdx.x < 32) tmem_dealloc_warp(base, kTmCols);
+}
+
 // Variant 4: variant 2 (backward links in tensor memory) on a 3D tile.  In
 // variants 1-3 a CTA owns R whole z-rows of one x-plane, so its x-neighbours
 // (one plane away) and the y-rows above and below always come from L2: the
@@ -1215,6 +1418,47 @@ static void launch_cheb5(const ProbDesc* pd, const ProbState* ps, const int* sta
 }
 
 template <int NT>
+static void launch_cheb6(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
+                         const void* links, const float* scale, const float2* X, const float2* Z, const float2* S,
+                         float2* Y, const double2* V, double2* W, const double* tcoef, int step, bool final_step,
+                         cudaStream_t st) {
+  const bool hz = Z != nullptr;
+  const size_t smem = sizeof(float2) * 2 * kPipeSlots * NT;
+#define LAPH_CHEB6(LT, HZ, FIN)                                                                                   \
+  k_cheb_mrhs6<LT, HZ, FIN, NT><<<nblk, NT, smem, st>>>(pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), \
+                                                        scale, X, Z, S, Y, V, W, tcoef, step)
+  if (bf16) {
+    if (hz && final_step) LAPH_CHEB6(__nv_bfloat162, true, true);
+    else if (hz) LAPH_CHEB6(__nv_bfloat162, true, false);
+    else if (final_step) LAPH_CHEB6(__nv_bfloat162, false, true);
+    else LAPH_CHEB6(__nv_bfloat162, false, false);
+  } else {
+    if (hz && final_step) LAPH_CHEB6(float2, true, true);
+    else if (hz) LAPH_CHEB6(float2, true, false);
+    else if (final_step) LAPH_CHEB6(float2, false, true);
+    else LAPH_CHEB6(float2, false, false);
+  }
+#undef LAPH_CHEB6
+}
+
+template <int NT>
+static int cheb6_attributes() {
+  const int smem = (int)sizeof(float2) * 2 * kPipeSlots * NT;
+#define LAPH_ATTR(LT, HZ, FIN) \
+  LAPH_CUDA_TRY(cudaFuncSetAttribute(k_cheb_mrhs6<LT, HZ, FIN, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))
+  LAPH_ATTR(float2, true, true);
+  LAPH_ATTR(float2, true, false);
+  LAPH_ATTR(float2, false, true);
+  LAPH_ATTR(float2, false, false);
+  LAPH_ATTR(__nv_bfloat162, true, true);
+  LAPH_ATTR(__nv_bfloat162, true, false);
+  LAPH_ATTR(__nv_bfloat162, false, true);
+  LAPH_ATTR(__nv_bfloat162, false, false);
+#undef LAPH_ATTR
+  return LAPH_OK;
+}
+
+template <int NT>
 static int cheb2_attributes() {
   const int smem = (int)sizeof(float2) * 27 * NT;
 #define LAPH_ATTR(LT, HZ, FIN) \
@@ -1237,6 +1481,9 @@ int cheb_init() {
   LAPH_TRY(cheb2_attributes<128>());
   LAPH_TRY(cheb2_attributes<256>());
   LAPH_TRY(cheb4_attributes<kStagedNT>());
+  LAPH_TRY(cheb6_attributes<64>());
+  LAPH_TRY(cheb6_attributes<128>());
+  LAPH_TRY(cheb6_attributes<256>());
   return LAPH_OK;
 }
 
@@ -1245,6 +1492,18 @@ int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np,
               const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant, int tile,
               int lmax, int* err, cudaStream_t st) {
   const bool hz = Z != nullptr;
+  if (variant == 5 && kb <= kCoefMax) {
+    if (tile == 64)
+      launch_cheb6<64>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step, st);
+    else if (tile == 256)
+      launch_cheb6<256>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step,
+                        st);
+    else
+      launch_cheb6<128>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step,
+                        st);
+    LAPH_CUDA_TRY(cudaGetLastError());
+    return LAPH_OK;
+  }
   if (variant == 4 && kb <= kCoefMax) {
     if (tile != kBrickNT || !cheb_staged_ok(lmax)) return LAPH_EINVAL;
     launch_cheb5(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step, st);

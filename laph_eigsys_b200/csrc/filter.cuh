@@ -13,7 +13,8 @@ int pack_links(const ProbDesc* pd, const int* start, int np, int nblk, const dou
 // links in tensor memory; 3: as 2 with every vector operand staged in shared memory by a
 // bulk-copy pipeline (needs tile 128 and cheb_staged_ok(L) for every problem; lmax = the
 // largest L of the batch; a pipeline wait that gives up sets *err); 4: as 2 on 512-site
-// bricks (TX = 128 / L planes x 4 z-rows; tile 512, same L condition).  Variants 1-4 need
+// bricks (TX = 128 / L planes x 4 z-rows; tile 512, same L condition); 5: as 2 with each
+// thread's next-column operands in flight through cp.async.  Variants 1-5 need
 // kb <= 64; larger blocks take variant 0.  tile: sites per CTA of variants 1 and 2 (64,
 // 128 or 256; variant 0 uses 128); nblk must match it.
 int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,

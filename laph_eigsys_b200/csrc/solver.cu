@@ -213,10 +213,10 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
     return LAPH_EINVAL;
   }
   if (opts->deg < 2 || opts->deg > kMaxFilterDeg || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1 ||
-      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 4 ||
+      opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 5 ||
       (opts->filter_tile != 0 && opts->filter_tile != 64 && opts->filter_tile != 128 && opts->filter_tile != 256)) {
     set_error("laph_solver_create: need 2 <= deg <= 128, guard >= 0, tol > 0, max_it >= 1, 0 <= block <= 512, "
-              "filter_kernel in {0, ..., 4}, filter_tile in {0, 64, 128, 256}");
+              "filter_kernel in {0, ..., 5}, filter_tile in {0, 64, 128, 256}");
     return LAPH_EINVAL;
   }
   for (int i = 0; i < n; ++i) {

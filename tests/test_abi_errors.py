@@ -46,7 +46,7 @@ def _solver_create(probs, n=None, **kw):
     ([(8, 10)], {"tol": float("nan")}),
     ([(8, 10)], {"max_it": 0}),
     ([(8, 10)], {"block": 513}),
-    ([(8, 10)], {"filter_kernel": 5}),
+    ([(8, 10)], {"filter_kernel": 6}),
     ([(8, 10)], {"filter_kernel": -1}),
     ([(2, 1)], {}),
     ([(129, 10)], {}),

@@ -136,11 +136,12 @@ def test_filter_tiles_are_bitwise_identical(gpu, prec):
     """The filter's site tile (64, 128 or 256 sites per CTA, an autotuner axis) changes only which CTA computes a
     site, not the arithmetic: every tile gives bitwise the same eigenpairs, on a batch with a ragged last tile
     (10^3 = 1000 sites, 12^3 = 1728).  The same holds for where the backward links wait between columns (shared
-    memory, filter_kernel 1, or tensor memory, filter_kernel 2): both run the same FMAs in the same order."""
+    memory, filter_kernel 1, or tensor memory, filter_kernel 2) and for where a thread's operands wait (registers,
+    or its own slots of a cp.async double buffer, filter_kernel 5): all run the same FMAs in the same order."""
     probs = [(10, 24), (12, 30)]
     links = [random_links(L, 0.35, 3400 + i) for i, (L, _) in enumerate(probs)]
     outs = []
-    for variant in (1, 2):
+    for variant in (1, 2, 5):
         for tile in (64, 128, 256):
             o = _solve(gpu, probs, links, guard=16, tol=1e-10, deg=24, filter_tile=tile, filter_kernel=variant,
                        link_prec=gpu.LINKS_BF16 if prec == "bf16" else gpu.LINKS_FP32)
