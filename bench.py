@@ -182,6 +182,7 @@ def make_opts(cfg):
                          max_it=400, deg=cfg["deg"], phase_fix=1, seed=1227, block=cfg.get("block", 0),
                          filter_kernel=cfg.get("filter_kernel", 1), jacobi_sweeps=cfg.get("sweeps", 0),
                          filter_tile=cfg.get("tile", 0), host_loop=cfg.get("host_loop", 0),
+                         **({"direct_resid": cfg["direct_resid"]} if cfg.get("direct_resid") is not None else {}),
                          lam_cut=cfg.get("lam_cut0", 0.0),
                          window={"mlp": lb.WINDOW_MLP, "lanczos": lb.WINDOW_LANCZOS, "fixed": lb.WINDOW_FIXED}[
                              cfg.get("window", "mlp")])
@@ -636,6 +637,9 @@ def main():
     ap.add_argument("--timeslices", type=int, default=None)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--filter-kernel", type=int, default=1, choices=[0, 1, 2, 3, 4, 5])
+    ap.add_argument("--direct-resid", type=float, default=None,
+                    help="passes above this largest wanted residual filter V directly in FP32 (< 0: never; "
+                         "default: the library's)")
     ap.add_argument("--guard", type=int, default=None)
     ap.add_argument("--sweeps", type=int, default=0)
     ap.add_argument("--lam-cut0", type=float, default=0.0)
@@ -676,6 +680,7 @@ def main():
     if args.guard is not None:
         cfg["guard"] = args.guard
     cfg["filter_kernel"] = args.filter_kernel
+    cfg["direct_resid"] = args.direct_resid
     cfg["host_loop"] = int(args.host_loop)
     if args.impl == "reference":
         return run_reference(args, cfg)

@@ -231,6 +231,13 @@ typedef struct {
                            with LAPH_TRACE set                                   */
   int filter_tile;      /* sites per CTA of the filter (64, 128 or 256; 0: 128);
                            laph_solver_autotune picks it                        */
+  double direct_resid;  /* a pass whose problem's largest wanted residual
+                           (relative to lam_max) is above this filters V itself
+                           in FP32, W = T_{m-1}(B) V, instead of the FP64-exact
+                           part plus the FP32 correction (no S in its steps, 72
+                           instead of 96 B per site-vector-step), until a direct
+                           pass fails to halve the residual; < 0 turns it off,
+                           and BF16 links never use it (default 1e-3)          */
 } laph_solve_opts;
 void laph_solve_opts_default(laph_solve_opts* o);
 

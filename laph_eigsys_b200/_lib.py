@@ -48,7 +48,8 @@ class laph_solve_opts(ctypes.Structure):
                 ("max_it", c_int), ("window", c_int), ("lam_cut", c_double), ("lam_max", c_double),
                 ("deg", c_int), ("phase_fix", c_int), ("seed", c_u64), ("block", c_int), ("filter_kernel", c_int),
                 ("jacobi_sweeps", c_int), ("window_margin", c_double),
-                ("host_loop", c_int), ("filter_tile", c_int)]
+                ("host_loop", c_int), ("filter_tile", c_int),
+                ("direct_resid", c_double)]
 
 
 class laph_result(ctypes.Structure):

@@ -39,6 +39,11 @@ struct ProbState {
   int nlock;                 // leading Ritz columns converged well below tol: not filtered
   int c0;                    // nlock rounded down to the Gram tile: columns [0, c0) are frozen
                              // (left out of the Rayleigh-Ritz, projected out of the rest)
+  int direct;                // this pass filters V itself in FP32 (T_{m-1}(B) V), not the
+                             // correction: set while the largest wanted residual is above
+                             // laph_solve_opts.direct_resid
+  int direct_off;            // a direct pass did not halve the residual: no more direct passes
+  double resid_begin;        // max_resid when the current pass began
 };
 
 // Block index b -> problem p with start[p] <= b < start[p+1].

@@ -568,6 +568,12 @@ __global__ void __launch_bounds__(1024) k_small(const ProbDesc* __restrict__ pd,
 //   step 2: E'_3 = (2 nu_2 B E'_2 + (T_2 - 1/2) S) / nu_3
 //   step n: E'_{n+1} = (2 nu_n B E'_n - nu_{n-1} E'_{n-1} + T_n S) / nu_{n+1}
 //   final : W' = (T_m / nu_m) V + E'_m   (= W / nu_m)
+// A direct pass (ProbState::direct) filters V itself: S holds V in FP32
+// (k_direct_start) and X_n = T_n(B) V, carried as X'_n = X_n / nu_n:
+//   step 1: X'_1 = B S / nu_1
+//   step 2: X'_2 = (2 nu_1 B X'_1 - S) / nu_2
+//   step n: X'_n = (2 nu_{n-1} B X'_{n-1} - nu_{n-2} X'_{n-2}) / nu_n   (no S)
+//   final : W' = X'_{m-1}   (T_m / nu_m = 0: the pass applies T_{m-1}(B))
 __global__ void k_coef(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, int np,
                        const double* __restrict__ theta, double* __restrict__ tcoef, double* __restrict__ scol, int m,
                        const int* __restrict__ dm) {
@@ -586,6 +592,19 @@ __global__ void k_coef(const ProbDesc* __restrict__ pd, const ProbState* __restr
     tn[1] = tb;
     for (int n = 2; n <= m; ++n) tn[n] = 2.0 * tb * tn[n - 1] - tn[n - 2];
     for (int n = 0; n <= m; ++n) nu[n] = fmax(1.0, fabs(tn[n]));
+    if (S.direct) {
+      for (int n = 1; n < m; ++n) {
+        const double a = n == 1 ? 1.0 / nu[1] : 2.0 * nu[n - 1] / nu[n];
+        const double z = n >= 3 ? -nu[n - 2] / nu[n] : 0.0;
+        const double g = n == 2 ? -1.0 / nu[2] : 0.0;
+        tc[((size_t)n * 3 + 0) * k + j] = a;
+        tc[((size_t)n * 3 + 1) * k + j] = z;
+        tc[((size_t)n * 3 + 2) * k + j] = g;
+      }
+      tc[((size_t)m * 3 + 0) * k + j] = 0.0;
+      scol[d.kv + j] = -2.0 * S.c_hop;
+      continue;
+    }
     for (int n = 1; n < m; ++n) {
       double a, z, g;
       if (n == 1) {

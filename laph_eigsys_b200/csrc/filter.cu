@@ -239,7 +239,7 @@ struct ChebCol {
 
 // NT sites (threads) per CTA, the tile the autotuner picks (64, 128 or 256);
 // 16 warps per SM at 128 registers whichever NT.
-template <typename LT, bool HAS_Z, bool FINAL, int NT>
+template <typename LT, bool HAS_Z, bool FINAL, int NT, bool HAS_S = true>
 __global__ void __launch_bounds__(NT, 512 / NT)
     k_cheb_mrhs2(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps, const int* __restrict__ start,
                  int np, int kb, const LT* __restrict__ links, const float* __restrict__ scale,
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       l2_prefetch(Xp + col + (size_t)c * d.V3 + s0, bytes);
-      l2_prefetch(Sp + col + (size_t)c * d.V3 + s0, bytes);
+      if (HAS_S) l2_prefetch(Sp + col + (size_t)c * d.V3 + s0, bytes);
       if (HAS_Z) l2_prefetch(Zp + col + (size_t)c * d.V3 + s0, bytes);
     }
     if (FINAL)
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       c.xs[a] = __ldg(x + (size_t)a * d.V3 + s);
-      c.ss[a] = __ldg(Sp + col + (size_t)a * d.V3 + s);
+      c.ss[a] = HAS_S ? __ldg(Sp + col + (size_t)a * d.V3 + s) : make_float2(0.f, 0.f);
       if (HAS_Z) c.zz[a] = __ldg(Zp + col + (size_t)a * d.V3 + s);
     }
   };
@@ -1230,6 +1230,34 @@ __global__ void __launch_bounds__(NT, 512 / NT)
   if (threadIdx.x < 32) tmem_dealloc_warp(base, kTmCols);
 }
 
+// The start of a direct pass (ProbState::direct): S = V in FP32, for the
+// unlocked columns of the problems that filter directly (the others keep the
+// S the residual kernel wrote).  Same grid as the filter: tile sites x kb
+// columns per CTA.
+__global__ void k_direct_start(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
+                               const int* __restrict__ start, int np, int kb, int tile,
+                               const double2* __restrict__ Vp, float2* __restrict__ Sp) {
+  const int p = find_prob(start, np, blockIdx.x);
+  if (!ps[p].active || !ps[p].direct) return;
+  const ProbDesc d = pd[p];
+  const int nst = (d.V3 + tile - 1) / tile;
+  const int t = blockIdx.x - start[p];
+  const int st = t % nst, cb = t / nst;
+  const int j0 = max(cb * kb, ps[p].nlock), j1 = min(cb * kb + kb, d.k);
+  for (int sl = threadIdx.x; sl < tile; sl += blockDim.x) {
+    const int s = st * tile + sl;
+    if (s >= d.V3) break;
+    for (int j = j0; j < j1; ++j) {
+      const size_t i = (size_t)d.blk + (size_t)j * d.dim + s;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double2 v = __ldg(Vp + i + (size_t)a * d.V3);
+        Sp[i + (size_t)a * d.V3] = make_float2((float)v.x, (float)v.y);
+      }
+    }
+  }
+}
+
 // ------------------------------------------------ FP64 block stencil: A W --
 // Y_j = (-Delta) W_j = 6 W_j - hop(W_j), FP64; CTA = 128 sites x a block of
 // kColsFP64 columns (stencil64cols.cuh).
@@ -1307,12 +1335,26 @@ template <int NT>
 static void launch_cheb2(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
                          const void* links, const float* scale, const float2* X, const float2* Z, const float2* S,
                          float2* Y, const double2* V, double2* W, const double* tcoef, int step, bool final_step,
-                         cudaStream_t st) {
+                         bool no_s, cudaStream_t st) {
   const bool hz = Z != nullptr;
   const size_t smem = sizeof(float2) * 27 * NT;
 #define LAPH_CHEB2(LT, HZ, FIN)                                                                                   \
   k_cheb_mrhs2<LT, HZ, FIN, NT><<<nblk, NT, smem, st>>>(pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), \
                                                         scale, X, Z, S, Y, V, W, tcoef, step)
+#define LAPH_CHEB2N(LT, FIN)                                                                                      \
+  k_cheb_mrhs2<LT, true, FIN, NT, false><<<nblk, NT, smem, st>>>(                                                  \
+      pd, ps, start, np, kb, reinterpret_cast<const LT*>(links), scale, X, Z, S, Y, V, W, tcoef, step)
+  if (no_s && hz) {  // a step of a direct pass past its second: the S coefficient is 0
+    if (bf16) {
+      if (final_step) LAPH_CHEB2N(__nv_bfloat162, true);
+      else LAPH_CHEB2N(__nv_bfloat162, false);
+    } else {
+      if (final_step) LAPH_CHEB2N(float2, true);
+      else LAPH_CHEB2N(float2, false);
+    }
+    return;
+  }
+#undef LAPH_CHEB2N
   if (bf16) {
     if (hz && final_step) LAPH_CHEB2(__nv_bfloat162, true, true);
     else if (hz) LAPH_CHEB2(__nv_bfloat162, true, false);
@@ -1472,6 +1514,14 @@ static int cheb2_attributes() {
   LAPH_ATTR(__nv_bfloat162, false, true);
   LAPH_ATTR(__nv_bfloat162, false, false);
 #undef LAPH_ATTR
+#define LAPH_ATTRN(LT, FIN)                                                                                  \
+  LAPH_CUDA_TRY(cudaFuncSetAttribute(k_cheb_mrhs2<LT, true, FIN, NT, false>,                               \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem))
+  LAPH_ATTRN(float2, true);
+  LAPH_ATTRN(float2, false);
+  LAPH_ATTRN(__nv_bfloat162, true);
+  LAPH_ATTRN(__nv_bfloat162, false);
+#undef LAPH_ATTRN
   return LAPH_OK;
 }
 
@@ -1490,7 +1540,7 @@ int cheb_init() {
 int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int bf16,
               const void* links, const float* scale, const float2* X, const float2* Z, const float2* S, float2* Y,
               const double2* V, double2* W, const double* tcoef, int step, bool final_step, int variant, int tile,
-              int lmax, int* err, cudaStream_t st) {
+              int lmax, int* err, bool no_s, cudaStream_t st) {
   const bool hz = Z != nullptr;
   if (variant == 5 && kb <= kCoefMax) {
     if (tile == 64)
@@ -1531,13 +1581,14 @@ int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np,
   }
   if (variant >= 1 && kb <= kCoefMax) {
     if (tile == 64)
-      launch_cheb2<64>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step, st);
+      launch_cheb2<64>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step,
+                       no_s, st);
     else if (tile == 256)
       launch_cheb2<256>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step,
-                        st);
+                        no_s, st);
     else
       launch_cheb2<128>(pd, ps, start, np, nblk, kb, bf16, links, scale, X, Z, S, Y, V, W, tcoef, step, final_step,
-                        st);
+                        no_s, st);
     LAPH_CUDA_TRY(cudaGetLastError());
     return LAPH_OK;
   }
@@ -1556,6 +1607,13 @@ int cheb_step(const ProbDesc* pd, const ProbState* ps, const int* start, int np,
     else LAPH_CHEB(float2, false, false);
   }
 #undef LAPH_CHEB
+  LAPH_CUDA_TRY(cudaGetLastError());
+  return LAPH_OK;
+}
+
+int direct_start(const ProbDesc* pd, const ProbState* ps, const int* start, int np, int nblk, int kb, int tile,
+                 const double2* V, float2* S, cudaStream_t st) {
+  k_direct_start<<<nblk, 128, 0, st>>>(pd, ps, start, np, kb, tile, V, S);
   LAPH_CUDA_TRY(cudaGetLastError());
   return LAPH_OK;
 }

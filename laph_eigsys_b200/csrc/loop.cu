@@ -31,6 +31,7 @@ __global__ void k_loop_init(LoopState* ls, const int* __restrict__ wdeg, int np)
     ls->m = 0;
     ls->npass = 0;
     ls->deg0 = s_max;
+    ls->direct = 0;
     ls->sv_steps = 0.0;
     ls->fbytes[0] = ls->fbytes[1] = 0.0;
     ls->filt_ns = 0.0;
@@ -42,7 +43,7 @@ __global__ void k_loop_init(LoopState* ls, const int* __restrict__ wdeg, int np)
 __global__ void k_loop_pass_begin(const ProbDesc* __restrict__ pd, ProbState* __restrict__ ps, int np, LoopState* ls,
                                   int* __restrict__ degs, double* __restrict__ lam_max0, int* __restrict__ fallback,
                                   const cudaGraphConditionalHandle* __restrict__ steps, LoopParams lp) {
-  __shared__ int s_it, s_m;
+  __shared__ int s_it, s_m, s_nact, s_ndir;
   __shared__ double s_sv, s_b0, s_b1;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -50,6 +51,7 @@ __global__ void k_loop_pass_begin(const ProbDesc* __restrict__ pd, ProbState* __
     s_m = lp.mdeg;
     if (s_it == 1 && ls->deg0 > 0) s_m = min(s_m, max(2, ls->deg0));
     s_sv = s_b0 = s_b1 = 0.0;
+    s_nact = s_ndir = 0;
   }
   __syncthreads();
   const int it = s_it;
@@ -69,6 +71,17 @@ __global__ void k_loop_pass_begin(const ProbDesc* __restrict__ pd, ProbState* __
         S.c_diag = (lp.lam_top + cut - 12.0) / (lp.lam_top - cut);
       }
     }
+    // a direct pass while the Ritz vectors are far from converged (FP32 rounding of T(B)V is harmless there),
+    // until one fails to halve the residual
+    if (S.active) {
+      if (S.direct && !(S.max_resid < 0.5 * S.resid_begin)) S.direct_off = 1;
+      S.resid_begin = S.max_resid;
+    }
+    S.direct = S.active && !S.direct_off && lp.direct_resid >= 0.0 && !(S.max_resid <= lp.direct_resid) ? 1 : 0;
+    if (S.active) {
+      atomicAdd(&s_nact, 1);
+      if (S.direct) atomicAdd(&s_ndir, 1);
+    }
     // degree cap while the Ritz vectors are still poor: amplification <= 1e6 at lambda = 0
     if (S.active && S.max_resid > lp.cap_resid) {
       const double tb0 = 1.0 + 2.0 * S.lam_cut / (S.lam_max - S.lam_cut);
@@ -79,6 +92,7 @@ __global__ void k_loop_pass_begin(const ProbDesc* __restrict__ pd, ProbState* __
   }
   __syncthreads();
   const int m = s_m;
+  const bool nos = s_nact > 0 && s_ndir == s_nact;
   // counters of this pass (the solver's filter byte model, per problem)
   for (int p = tid; p < np; p += blockDim.x) {
     const ProbState& S = ps[p];
@@ -86,22 +100,26 @@ __global__ void k_loop_pass_begin(const ProbDesc* __restrict__ pd, ProbState* __
     const ProbDesc d = pd[p];
     const int nl = S.nlock, nact = d.k - nl;
     const int nblk = (d.k + lp.kb - 1) / lp.kb - nl / lp.kb;
-    double per = 0.0;
+    double per = S.direct ? 72.0 : 0.0;  // a direct pass starts with S = FP32(V)
     for (int n = 1; n < m; ++n) {
-      const int reads = n == 1 ? 1 : (n == 2 ? 2 : 3);
+      const int reads = n == 1 ? 1 : (n == 2 ? 2 : (nos ? 2 : 3));
       per += reads * 24.0 + (n == m - 1 ? 96.0 : 24.0);
     }
     atomicAdd(&s_sv, (double)d.V3 * nact * (m - 1));
     atomicAdd(&s_b0, (double)d.V3 * (nact * per + nl * 96.0 + (double)nblk * (m - 1) * lp.lbytes));
     atomicAdd(&s_b1, (double)d.V3 * (m - 1) * (nact * 72.0 + (double)nblk * lp.lbytes));
   }
-  // the filter steps of this pass: n = 1..m-2 plain (0), n = m-1 the last (1), none beyond (2)
-  for (int n = 1 + tid; n < lp.mdeg; n += blockDim.x)
-    cudaGraphSetConditional(steps[n], n < m - 1 ? 0u : (n == m - 1 ? 1u : 2u));
+  // the filter steps of this pass: n = 1..m-2 middle (0), n = m-1 the last (1), the same without S (2, 3) for
+  // n >= 3 of an all-direct pass, none beyond (4: past the last branch of every SWITCH)
+  for (int n = 1 + tid; n < lp.mdeg; n += blockDim.x) {
+    const unsigned base = n < m - 1 ? 0u : (n == m - 1 ? 1u : 4u);
+    cudaGraphSetConditional(steps[n], base < 2u && nos && n >= 3 ? base + 2u : base);
+  }
   __syncthreads();
   if (tid == 0) {
     ls->it = it;
     ls->m = m;
+    ls->direct = nos ? 1 : 0;
     degs[ls->npass] = m;
     ls->npass += 1;
     ls->sv_steps += s_sv;

@@ -14,6 +14,7 @@ struct LoopState {
   int m;                         // filter degree of the current pass
   int npass;                     // passes run
   int deg0;                      // learned first-pass degree cap (0: none)
+  int direct;                    // every active problem runs the current pass directly (no S past step 2)
   double sv_steps;               // unlocked site-vector-steps filtered
   double fbytes[2];              // filter bytes (correction form, 72 B unit)
   double filt_ns;                // filter time from the global timer
@@ -32,6 +33,7 @@ struct LoopParams {
   double lam_top;    // exact upper bound of the spectrum (12 or opts.lam_max)
   double cap_resid;  // degree cap while the largest wanted residual exceeds this
   double win_check;  // the learned window's check after its first pass
+  double direct_resid;  // a problem's pass is direct while its largest wanted residual exceeds this (< 0: never)
 };
 
 // Stamp the global timer into *t.
@@ -39,8 +41,10 @@ int loop_stamp(unsigned long long* t, cudaStream_t st);
 // Reset the counters; deg0 = max over problems of the learned degrees (wdeg may be null).
 int loop_init(LoopState* ls, const int* wdeg, int np, cudaStream_t st);
 // Begin a pass: it += 1, the learned window's check (it == 2), the degree m,
-// the counters, and the SWITCH handles of the filter steps n = 1..mdeg-1:
-// 0 = a plain step (n < m - 1), 1 = the last step (n = m - 1), 2 = no step.
+// each problem's direct flag, the counters, and the SWITCH handles of the
+// filter steps n = 1..mdeg-1: 0 = a middle step (n < m - 1), 1 = the last step
+// (n = m - 1), 2 / 3 = the same without S (n >= 3 of a pass every active
+// problem runs directly), 4 = no step.
 int loop_pass_begin(const ProbDesc* pd, ProbState* ps, int np, LoopState* ls, int* degs, double* lam_max0,
                     int* fallback, const cudaGraphConditionalHandle* steps, const LoopParams& lp, cudaStream_t st);
 // End of the filter part of a pass: accumulate its time.

@@ -159,6 +159,17 @@ int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
 extern "C" {
 
+// default laph_solve_opts.direct_resid: passes whose largest wanted residual (relative to lam_max) is above
+// it filter V directly in FP32; the FP32 rounding of T_m(B)V (about m * 6e-8 relative) stays far below it.
+// 1e-4 also takes the pass that brings the first columns to the locking threshold and delays locking:
+// measured slower than 1e-3 (26.8 against 27.6 timeslices/s at 32^3 x 64, same box)
+constexpr double kDirectResid = 1e-3;
+// The threshold a solve uses: none with BF16 links, whose rounding (about 4e-3 relative) would put the
+// direct filter's operator itself that far from B.
+static double direct_resid(const laph_solve_opts& o) {
+  return o.link_prec == LAPH_LINKS_BF16 ? -1.0 : o.direct_resid;
+}
+
 void laph_solve_opts_default(laph_solve_opts* o) {
   std::memset(o, 0, sizeof *o);
   o->smear_kind = LAPH_SMEAR_NONE;
@@ -171,6 +182,7 @@ void laph_solve_opts_default(laph_solve_opts* o) {
   o->phase_fix = 1;
   o->seed = 1227;
   o->filter_kernel = 1;
+  o->direct_resid = kDirectResid;
 }
 
 int laph_solver_destroy(laph_solver* s) {
@@ -214,9 +226,10 @@ int laph_solver_create(laph_solver** out, const laph_problem* probs, int n, cons
   }
   if (opts->deg < 2 || opts->deg > kMaxFilterDeg || opts->guard < 0 || !(opts->tol > 0.0) || opts->max_it < 1 ||
       opts->block < 0 || opts->block > 512 || opts->filter_kernel < 0 || opts->filter_kernel > 5 ||
-      (opts->filter_tile != 0 && opts->filter_tile != 64 && opts->filter_tile != 128 && opts->filter_tile != 256)) {
+      (opts->filter_tile != 0 && opts->filter_tile != 64 && opts->filter_tile != 128 && opts->filter_tile != 256) ||
+      !std::isfinite(opts->direct_resid)) {
     set_error("laph_solver_create: need 2 <= deg <= 128, guard >= 0, tol > 0, max_it >= 1, 0 <= block <= 512, "
-              "filter_kernel in {0, ..., 5}, filter_tile in {0, 64, 128, 256}");
+              "filter_kernel in {0, ..., 5}, filter_tile in {0, 64, 128, 256}, finite direct_resid");
     return LAPH_EINVAL;
   }
   for (int i = 0; i < n; ++i) {
@@ -419,6 +432,7 @@ int laph_solver_set_links(laph_solver* s, int i, const double* links, int layout
 // one outer iteration at 32^3 x 64, but the extra filter steps cost more than
 // the Rayleigh-Ritz they save (20.3 against 21.0 timeslices/s).
 constexpr double kCapResid = 1e-2;
+
 // Largest wanted residual after the learned window's first pass that counts
 // as a working window (the random start block has residuals of order 1).
 constexpr double kWindowCheck = 0.2;
@@ -450,20 +464,22 @@ static int iteration_rr(laph_solver* s, int first_iter) {
   return LAPH_OK;
 }
 
-// Step n (1-based) of a filter pass; fin: the pass's last step (writes W).
-static int filter_step(laph_solver* s, int n, bool fin, cudaStream_t st) {
+// Step n (1-based) of a filter pass; fin: the pass's last step (writes W); nos: every active problem runs
+// the pass directly, so steps past the second read no S.
+static int filter_step(laph_solver* s, int n, bool fin, bool nos, cudaStream_t st) {
   const int bf = s->o.link_prec == LAPH_LINKS_BF16;
   const void* links = bf ? s->Ubf : static_cast<const void*>(s->Uf32);
   const float2* X = (n == 1) ? s->S : s->E[(n - 2) % 3];
   const float2* Z = (n >= 3) ? s->E[(n - 3) % 3] : nullptr;
   float2* Yo = s->E[(n - 1) % 3];
   return cheb_step(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, bf, links, s->scale, X, Z, s->S, Yo, s->V,
-                   s->W, s->tcoef, n, fin, s->fvariant, s->tile, s->lmax, s->d_ferr, st);
+                   s->W, s->tcoef, n, fin, s->fvariant, s->tile, s->lmax, s->d_ferr, nos && n >= 3, st);
 }
 
-static int filter(laph_solver* s, int m) {
+static int filter(laph_solver* s, int m, bool nos) {
   LAPH_TRY(coef(s->d_pd, s->d_ps, s->np, s->theta, s->tcoef, s->scol, m, nullptr, s->st));
-  for (int n = 1; n < m; ++n) LAPH_TRY(filter_step(s, n, n == m - 1, s->st));
+  LAPH_TRY(direct_start(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, s->tile, s->V, s->S, s->st));
+  for (int n = 1; n < m; ++n) LAPH_TRY(filter_step(s, n, n == m - 1, nos, s->st));
   return LAPH_OK;
 }
 
@@ -493,12 +509,13 @@ static int capture(laph_solver* s, cudaGraphExec_t* exec, F body) {
   return LAPH_OK;
 }
 
-static int filter_graph(laph_solver* s, int m) {
-  auto it = s->g_filter.find(m);
+static int filter_graph(laph_solver* s, int m, bool nos) {
+  const int key = 2 * m + (nos ? 1 : 0);
+  auto it = s->g_filter.find(key);
   if (it == s->g_filter.end()) {
     cudaGraphExec_t ex = nullptr;
-    LAPH_TRY(capture(s, &ex, [&] { return filter(s, m); }));
-    it = s->g_filter.emplace(m, ex).first;
+    LAPH_TRY(capture(s, &ex, [&] { return filter(s, m, nos); }));
+    it = s->g_filter.emplace(key, ex).first;
   }
   LAPH_CUDA_TRY(cudaGraphLaunch(it->second, s->st));
   return LAPH_OK;
@@ -692,6 +709,7 @@ static int build_solve_graph(laph_solver* s) {
   lp.lam_top = o.lam_max > 0.0 ? o.lam_max : 12.0;
   lp.cap_resid = kCapResid;
   lp.win_check = kWindowCheck;
+  lp.direct_resid = direct_resid(o);
   long long nsetup = 0;
   std::vector<cudaGraphNode_t> deps;
   int rc = capture_into(s, g, deps, [&]() -> int {
@@ -708,7 +726,7 @@ static int build_solve_graph(laph_solver* s) {
   // the pass: one SWITCH handle per filter step position
   std::vector<cudaGraphConditionalHandle> hs(s->mdeg + 1, 0);
   for (int n = 1; n < s->mdeg; ++n)
-    if (cudaGraphConditionalHandleCreate(&hs[n], body, 2, 0) != cudaSuccess) {
+    if (cudaGraphConditionalHandleCreate(&hs[n], body, 4, 0) != cudaSuccess) {
       set_error("conditional graph nodes not available");
       return done(LAPH_ECUDA);
     }
@@ -718,15 +736,19 @@ static int build_solve_graph(laph_solver* s) {
   rc = capture_into(s, body, bd, [&]() -> int {
     LAPH_TRY(loop_pass_begin(s->d_pd, s->d_ps, s->np, s->ls, s->d_degs, s->d_lam_max0, s->d_fallback, s->d_steps,
                              lp, s->st));
-    return coef(s->d_pd, s->d_ps, s->np, s->theta, s->tcoef, s->scol, 0, &s->ls->m, s->st);
+    LAPH_TRY(coef(s->d_pd, s->d_ps, s->np, s->theta, s->tcoef, s->scol, 0, &s->ls->m, s->st));
+    return direct_start(s->d_pd, s->d_ps, s->st_filt, s->np, s->nb_filt, s->kb, s->tile, s->V, s->S, s->st);
   });
   if (rc != LAPH_OK) return done(rc);
+  // SWITCH per step position: middle / last step, and for n >= 3 the same two without S
   for (int n = 1; n < s->mdeg; ++n) {
-    cudaGraph_t b[2];
-    if ((rc = add_conditional(body, bd, hs[n], cudaGraphCondTypeSwitch, 2, b)) != LAPH_OK) return done(rc);
-    for (int fin = 0; fin < 2; ++fin) {
+    const unsigned nb = n >= 3 ? 4u : 2u;
+    cudaGraph_t b[4];
+    if ((rc = add_conditional(body, bd, hs[n], cudaGraphCondTypeSwitch, nb, b)) != LAPH_OK) return done(rc);
+    for (unsigned br = 0; br < nb; ++br) {
       std::vector<cudaGraphNode_t> none;
-      if ((rc = capture_into(s, b[fin], none, [&]() -> int { return filter_step(s, n, fin == 1, s->st); })) != LAPH_OK)
+      if ((rc = capture_into(s, b[br], none,
+                             [&]() -> int { return filter_step(s, n, (br & 1u) != 0, br >= 2, s->st); })) != LAPH_OK)
         return done(rc);
     }
   }
@@ -778,8 +800,9 @@ static int run_device_loop(laph_solver* s, laph_result* res) {
   for (int m : s->degs) fl += m - 1;
   s->cnt[0] = (long long)ls.sv_steps;
   s->cnt[1] = fl;
-  // per pass: loop_pass_begin, coef, the m - 1 steps, loop_pass_end, 8 Rayleigh-Ritz kernels, loop_cond
-  s->cnt[2] = s->solve_setup_launches + 12LL * ls.npass + fl;
+  // per pass: loop_pass_begin, coef, direct_start, the m - 1 steps, loop_pass_end, 8 Rayleigh-Ritz kernels,
+  // loop_cond
+  s->cnt[2] = s->solve_setup_launches + 13LL * ls.npass + fl;
   s->fbytes[0] = ls.fbytes[0];
   s->fbytes[1] = ls.fbytes[1];
   s->ran = 1;
@@ -917,6 +940,23 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
       const int m_safe = std::isfinite(ratio) ? (int)std::min(std::floor(ratio), 1e6) : 2;  // NaN window: degree 2
       m = std::min(m, std::max(2, m_safe));
     }
+    // Direct passes: a problem whose largest wanted residual is above direct_resid filters V itself in FP32
+    // this pass (the device loop's rule, k_loop_pass_begin); when every active problem does, the steps past
+    // the second read no S.
+    int nact_p = 0, ndir_p = 0;
+    const double dres = direct_resid(o);
+    for (int i = 0; i < s->np; ++i) {
+      ProbState& p = s->hps[i];
+      if (p.active) {
+        if (p.direct && !(p.max_resid < 0.5 * p.resid_begin)) p.direct_off = 1;
+        p.resid_begin = p.max_resid;
+      }
+      p.direct = p.active && !p.direct_off && dres >= 0.0 && !(p.max_resid <= dres) ? 1 : 0;
+      nact_p += p.active ? 1 : 0;
+      ndir_p += p.direct;
+    }
+    const bool nos = nact_p > 0 && ndir_p == nact_p;
+    LAPH_CUDA_TRY(cudaMemcpyAsync(s->d_ps, s->hps.data(), s->np * sizeof(ProbState), cudaMemcpyHostToDevice, s->st));
     const double lbytes = s->o.link_prec == LAPH_LINKS_BF16 ? 112.0 : 216.0;  // per site per column block
     for (int i = 0; i < s->np; ++i) {
       if (!s->hps[i].active) continue;
@@ -924,9 +964,9 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
       const int nl = s->hps[i].nlock, nact = d.k - nl;
       s->cnt[0] += (long long)d.V3 * nact * (m - 1);
       const int nblk = (d.k + s->kb - 1) / s->kb - nl / s->kb;  // column blocks with an unlocked column
-      double per = 0.0;  // bytes per unlocked site-vector over the pass
+      double per = s->hps[i].direct ? 72.0 : 0.0;  // bytes per unlocked site-vector over the pass
       for (int n = 1; n < m; ++n) {
-        const int reads = n == 1 ? 1 : (n == 2 ? 2 : 3);
+        const int reads = n == 1 ? 1 : (n == 2 ? 2 : (nos ? 2 : 3));
         per += reads * 24.0 + (n == m - 1 ? 96.0 : 24.0);
       }
       s->fbytes[0] += (double)d.V3 * (nact * per + nl * 96.0 + (double)nblk * (m - 1) * lbytes);
@@ -934,12 +974,12 @@ int laph_solver_run(laph_solver* s, laph_result* res) {
     }
     s->cnt[1] += m - 1;
     s->degs.push_back(m);
-    if (trace) std::fprintf(stderr, "laph_trace it %d filter degree %d\n", it, m);
+    if (trace) std::fprintf(stderr, "laph_trace it %d filter degree %d direct %d/%d\n", it, m, ndir_p, nact_p);
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[0], s->st));
-    LAPH_TRY(filter_graph(s, m));
+    LAPH_TRY(filter_graph(s, m, nos));
     LAPH_CUDA_TRY(cudaEventRecord(s->evf[1], s->st));
     LAPH_TRY(rr_graph(s));
-    nlaunch += 1 + (m - 1) + 8;
+    nlaunch += 2 + (m - 1) + 8;
     float f = 0.f;
     LAPH_CUDA_TRY(cudaEventSynchronize(s->evf[1]));
     LAPH_CUDA_TRY(cudaEventElapsedTime(&f, s->evf[0], s->evf[1]));

@@ -170,3 +170,32 @@ def test_staged_filter_is_bitwise_identical(gpu, prec):
             for (ea, va, pa), (eb, vb, pb) in zip(outs[0]["eig"], o["eig"]):
                 assert np.array_equal(ea, eb) and np.array_equal(va, vb) and np.array_equal(pa, pb)
             assert outs[0]["res"][0]["iters"] == o["res"][0]["iters"]
+
+
+def test_direct_passes_converge_to_the_same_eigensystem(gpu):
+    """Passes whose largest wanted residual is above direct_resid filter V itself in FP32 (T_{m-1}(B) V, no S);
+    the correction form takes over below it.  The eigenpairs match a solve without direct passes (eigenvalues to
+    1e-10 of lambda_max, the nev-block projectors to the residual over the gap), with the default threshold and
+    with direct_resid = 0 (direct until a pass fails to halve the residual, then the correction form: the guard
+    that keeps a solve from stalling at the FP32 filter's floor).  BF16 links never take direct passes: their
+    results equal the direct_resid = -1 run bit for bit.  Both loops stay bitwise identical with direct passes."""
+    probs = [(10, 24), (12, 30)]
+    links = [random_links(L, 0.35, 3600 + i) for i, (L, _) in enumerate(probs)]
+    kw = dict(smear_kind=gpu.SMEAR_STOUT, smear_p1=0.1, smear_iters=2, guard=16, tol=1e-11, deg=32, max_it=300)
+    off = _solve(gpu, probs, links, direct_resid=-1.0, **kw)
+    assert off["status"] == 0
+    for dr in (1e-3, 0.0):
+        on = _solve(gpu, probs, links, direct_resid=dr, **kw)
+        assert on["status"] == 0, dr
+        for (ea, va, _), (eb, vb, _) in zip(on["eig"], off["eig"]):
+            assert np.max(np.abs(ea - eb)) <= 1e-10 * 12.0, dr
+            proj = va @ (va.conj().T @ vb) - vb
+            assert np.linalg.norm(proj) / np.sqrt(vb.shape[1]) <= 1e-6, dr
+    host = _solve(gpu, probs, links, direct_resid=1e-3, host_loop=1, **kw)
+    dev = _solve(gpu, probs, links, direct_resid=1e-3, **kw)
+    for (ea, va, _), (eb, vb, _) in zip(dev["eig"], host["eig"]):
+        assert np.array_equal(ea, eb) and np.array_equal(va, vb)
+    assert np.allclose(dev["fbytes"], host["fbytes"], rtol=1e-12)
+    bf = [_solve(gpu, probs, links, direct_resid=dr, link_prec=gpu.LINKS_BF16, **kw) for dr in (1e-3, -1.0)]
+    for (ea, va, _), (eb, vb, _) in zip(bf[0]["eig"], bf[1]["eig"]):
+        assert np.array_equal(ea, eb) and np.array_equal(va, vb)
