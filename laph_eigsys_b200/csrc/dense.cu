@@ -13,9 +13,10 @@
 // block against them, and the rotation and residual write active columns only.
 // These replace SLEPc's BV orthogonalisation and DS dense eigensolve inside
 // EPSSolve (src/ev_ts.cpp:263).  tcgen05 has no FP64 kind, so the Gram and the
-// rotation run on the FP64 tensor path of mma.sync (m8n8k4 f64, four real
-// MMAs per complex product): at the same peak as the FP64 FMA pipe, but one
-// instruction per 256 FMAs, which measured 7-10% faster for each kernel.
+// rotation run on the FP64 tensor path of mma.sync (four real MMAs per complex
+// product): at the same peak as the FP64 FMA pipe, but one instruction per 256
+// FMAs (m8n8k4, the rotation) or 2048 (m16n8k16, the Gram), which measured
+// 7-10% faster for each kernel than FMA, and the Gram another 9% on m16n8k16.
 #include "batch.cuh"
 #include "dense.cuh"
 #include "filter.cuh"
@@ -33,10 +34,21 @@ __device__ __forceinline__ void dmma884(double (&acc)[2], double a, double b) {
       : "+d"(acc[0]), "+d"(acc[1])
       : "d"(a), "d"(b));
 }
+// d(16x8, 4 per thread) += a(16x16, 8 per thread) b(16x8, 4 per thread), FP64 tensor MMA: the same peak as
+// m8n8k4 (37.1 TFLOP/s measured for both on this part) with an eighth of the instructions.  Fragments, g =
+// lane / 4, t = lane % 4: a[r] = A(g + 8 (r & 1), t + 4 (r >> 1)); b[r] = B(t + 4 r, g); d[0..1] = D(g, 2t + {0,1}),
+// d[2..3] = D(g + 8, 2t + {0,1}).
+__device__ __forceinline__ void dmma16816(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+        "d"(b[2]), "d"(b[3]));
+}
 
 // ------------------------------------------------------------------ Gram ---
 // CTA: 64 threads, output tiles G[ti,tj] = W_ti^H W_tj and H[ti,tj] = W_ti^H Y_tj
-// (32 x 32 each; warp 0 forms G, warp 1 H), over the rows of one chunk; the
+// (32 x 32 each, as 2 x 4 m16n8k16 tiles; warp 0 forms G, warp 1 H), over the rows of one chunk; the
 // W_ti tile is staged once for both products.  Rows arrive through a
 // two-stage cp.async ring (dynamic shared memory [stage][A|W|Y][col][GP]),
 // so the next 16 rows load while the current 16 are multiplied.
@@ -84,18 +96,21 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
     cp_async_commit();
   };
   // FP64 tensor path: warp 0 forms G = W_ti^H W_tj, warp 1 H = W_ti^H Y_tj, each
-  // as 4 x 4 8x8 MMA tiles; conj(w) b = (wr br + wi bi) + i (wr bi - wi br)
+  // as 2 x 4 tiles of m16n8k16 (one MMA per tile and stage of 16 rows);
+  // conj(w) b = (wr br + wi bi) + i (wr bi - wi br), the last as wi (-br)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int fr = lane >> 2, fk = lane & 3;
-  double accr[4][4][2], acci[4][4][2];
+  const int g = lane >> 2, t4 = lane & 3;
+  double accr[2][4][4], acci[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) accr[i][j][0] = accr[i][j][1] = acci[i][j][0] = acci[i][j][1] = 0.0;
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) accr[i][j][e] = acci[i][j][e] = 0.0;
   const int nstep = (r1 - r0 + GK - 1) / GK;
   // On a diagonal tile pair (ti == tj) the reduction keeps only the upper
-  // triangle (G and H are Hermitian), so the 8x8 MMA tiles below the diagonal
-  // are skipped: 10 of 16 per warp.
+  // triangle (G and H are Hermitian): the 16x8 tiles entirely below the
+  // diagonal (rows 16-31 x columns 0-15) are skipped, 2 of 8 per warp.
   const bool diag = ti == tj;
   load(r0, 0);
   for (int it = 0; it < nstep; ++it) {
@@ -109,58 +124,56 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
     __syncthreads();
     const double2* sA = gsm + b * 3 * GT * GP;
     const double2* sB = sA + (1 + warp) * GT * GP;  // W_tj or Y_tj
+    // A fragments (m16 x k16, row = column of W_ti, k = row of the stage): a[r] at (g + 8 (r & 1), t4 + 4 (r >> 1))
+    double ar[2][8], ai[2][8];
 #pragma unroll
-    for (int ks = 0; ks < GK / 4; ++ks) {
-      const int q = 4 * ks + fk;
-      double wr[4], wi[4], wn[4], br[4], bi[4];
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const double2 a = sA[(8 * i + fr) * GP + q];
-        wr[i] = a.x;
-        wi[i] = a.y;
-        wn[i] = -a.y;
+      for (int r = 0; r < 8; ++r) {
+        const double2 a = sA[(16 * i + g + 8 * (r & 1)) * GP + t4 + 4 * (r >> 1)];
+        ar[i][r] = a.x;
+        ai[i][r] = a.y;
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const double2 bb = sB[(8 * j + fr) * GP + q];
-        br[j] = bb.x;
-        bi[j] = bb.y;
+    for (int j = 0; j < 4; ++j) {
+      // B fragment (k16 x n8): b[r] at (t4 + 4 r, g)
+      double br[4], bi[4], bn[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const double2 v = sB[(8 * j + g) * GP + t4 + 4 * r];
+        br[r] = v.x;
+        bi[r] = v.y;
+        bn[r] = -v.x;
       }
-      // below the diagonal of a diagonal tile: never read
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
+        if (!diag || !(i == 1 && j < 2)) dmma16816(accr[i][j], ar[i], br);
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (!diag || i <= j) dmma884(accr[i][j], wr[i], br[j]);
+      for (int i = 0; i < 2; ++i)
+        if (!diag || !(i == 1 && j < 2)) dmma16816(acci[i][j], ar[i], bi);
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
+        if (!diag || !(i == 1 && j < 2)) dmma16816(accr[i][j], ai[i], bi);
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (!diag || i <= j) dmma884(acci[i][j], wr[i], bi[j]);
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (!diag || i <= j) dmma884(accr[i][j], wi[i], bi[j]);
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (!diag || i <= j) dmma884(acci[i][j], wn[i], br[j]);
+      for (int i = 0; i < 2; ++i)
+        if (!diag || !(i == 1 && j < 2)) dmma16816(acci[i][j], ai[i], bn);
     }
     __syncthreads();
   }
-  // partial layout: [chunk][which][pair][32*32]
+  // partial layout: [chunk][which][pair][32*32]; C fragment rows g (+8), columns 2 t4 + {0, 1}
   double2* o = gpart + d.gp + ((size_t)(chunk * 2 + warp) * npair + pair) * (GT * GT);
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (diag && i > j) continue;
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int e = 0; e < 2; ++e)
-        o[(8 * i + fr) * GT + 8 * j + 2 * fk + e] = make_double2(accr[i][j][e], acci[i][j][e]);
-    }
+      for (int h = 0; h < 2; ++h) {
+        const int rb = 2 * i + h;  // 8-row block of the output
+        if (diag && rb > j) continue;
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          o[(16 * i + 8 * h + g) * GT + 8 * j + 2 * t4 + e] = make_double2(accr[i][j][2 * h + e], acci[i][j][2 * h + e]);
+      }
 }
 
 
