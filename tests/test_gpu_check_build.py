@@ -48,7 +48,7 @@ def _workload(out_path):
     c.close()
     kw = dict(smear_kind=lb.SMEAR_STOUT, smear_p1=0.1, smear_iters=2, guard=16, tol=1e-10, deg=24)
     for fk, probs in ((0, [(6, 12), (8, 20)]), (1, [(6, 12), (8, 20)]), (2, [(6, 12), (8, 20)]),
-                      (3, [(16, 24)]), (4, [(16, 24)])):
+                      (3, [(16, 24)]), (4, [(16, 24)]), (5, [(6, 12), (8, 20)])):
         s = lb.Solver(probs, filter_kernel=fk, **kw)
         for i, (L, _) in enumerate(probs):
             s.set_links(i, random_links(L, 0.35, 920 + L))
