@@ -50,9 +50,12 @@ __device__ __forceinline__ void dmma16816(double (&d)[4], const double (&a)[8], 
 // CTA: 64 threads, output tiles G[ti,tj] = W_ti^H W_tj and H[ti,tj] = W_ti^H Y_tj
 // (32 x 32 each, as 2 x 4 m16n8k16 tiles; warp 0 forms G, warp 1 H), over the rows of one chunk; the
 // W_ti tile is staged once for both products.  Rows arrive through a
-// two-stage cp.async ring (dynamic shared memory [stage][A|W|Y][col][GP]),
+// two-stage cp.async ring (dynamic shared memory [stage][A|W|Y][col][GP], row q of column c at
+// c GP + (q ^ 4 (c & 1)): the 16-byte fragment reads of a quarter warp, two columns of one parity pair,
+// then fall on eight different bank groups),
 // so the next 16 rows load while the current 16 are multiplied.
-constexpr int GT = 32, GK = 16, GP = GK + 1;
+constexpr int GT = 32, GK = 16, GP = GK;
+__device__ __forceinline__ int gsw(int c, int q) { return c * GP + (q ^ ((c & 1) << 2)); }
 constexpr int kGramSmem = 2 * 3 * GT * GP * (int)sizeof(double2);
 
 __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, const ProbState* __restrict__ ps,
@@ -89,9 +92,9 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
       const int row = r + q;
       const bool ok = row < r1;
       const size_t off = (size_t)c * d.dim + (ok ? row : 0);
-      cp_async16(s + LAPH_IX(c * GP + q, GT * GP), A + off, ok);
-      cp_async16(s + (GT + c) * GP + q, BW + off, ok);
-      cp_async16(s + (2 * GT + c) * GP + q, BY + off, ok);
+      cp_async16(s + LAPH_IX(gsw(c, q), GT * GP), A + off, ok);
+      cp_async16(s + gsw(GT + c, q), BW + off, ok);
+      cp_async16(s + gsw(2 * GT + c, q), BY + off, ok);
     }
     cp_async_commit();
   };
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
     for (int i = 0; i < 2; ++i)
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
-        const double2 a = sA[(16 * i + g + 8 * (r & 1)) * GP + t4 + 4 * (r >> 1)];
+        const double2 a = sA[gsw(16 * i + g + 8 * (r & 1), t4 + 4 * (r >> 1))];
         ar[i][r] = a.x;
         ai[i][r] = a.y;
       }
@@ -140,7 +143,7 @@ __global__ void __launch_bounds__(64) k_gram(const ProbDesc* __restrict__ pd, co
       double br[4], bi[4], bn[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        const double2 v = sB[(8 * j + g) * GP + t4 + 4 * r];
+        const double2 v = sB[gsw(8 * j + g, t4 + 4 * r)];
         br[r] = v.x;
         bi[r] = v.y;
         bn[r] = -v.x;
