@@ -48,6 +48,8 @@ def _solver_create(probs, n=None, **kw):
     ([(8, 10)], {"block": 513}),
     ([(8, 10)], {"filter_kernel": 6}),
     ([(8, 10)], {"filter_kernel": -1}),
+    ([(8, 10)], {"direct_resid": float("nan")}),
+    ([(8, 10)], {"direct_resid": float("inf")}),
     ([(2, 1)], {}),
     ([(129, 10)], {}),
     ([(8, 0)], {}),
