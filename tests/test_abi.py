@@ -61,3 +61,16 @@ def test_fp64_probe_measures_plausible_peaks():
     import laph_eigsys_b200 as lb
     fma, dmma = lb.probe_fp64(0)
     assert 10.0 < fma < 120.0 and 10.0 < dmma < 120.0, (fma, dmma)
+
+
+def test_solve_opts_mirror_matches_the_c_struct():
+    """laph_solve_opts_default writes the C struct: it must end exactly where the ctypes mirror ends (a sentinel
+    just past it stays untouched) and its last field, direct_resid, must read back as the library's default."""
+    import ctypes
+    import laph_eigsys_b200 as lb
+    n = ctypes.sizeof(lb._lib.laph_solve_opts)
+    buf = (ctypes.c_ubyte * (n + 64))(*([0xA5] * (n + 64)))
+    lb.lib.laph_solve_opts_default(ctypes.cast(buf, ctypes.POINTER(lb._lib.laph_solve_opts)))
+    assert bytes(buf[n:]) == b"\xa5" * 64
+    o = lb._lib.laph_solve_opts.from_buffer(buf)
+    assert o.direct_resid == 1e-3 and o.filter_kernel == 1 and o.guard == 16 and o.max_it == 200
