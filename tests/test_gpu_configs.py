@@ -8,6 +8,10 @@ with every error stated (printed) as well as bounded:
       T_8(B) (the reference's EPSSolve, src/ev_ts.cpp:231-263).
   C2  24^3, eps 0.3, seed 1228, HYP 0.62 / 0.62 x 1, nev 120: timeslices 0
       and 1 against the oracle's smearing + FP64 Krylov-Schur on T_12(B).
+  C3  32^3, eps 0.3, seed 1229, stout 5 x 0.1, nev 120, with the BF16 +
+      per-site-scale filter links that configuration specifies, and C4's
+      32^3 lattice (seed 1232, APE 0.5 x 10, nev 180): a timeslice each at
+      the configurations' tolerance 1e-9 against the oracle's Krylov-Schur.
 
 The block solver's filter runs in FP32 (FP64 Rayleigh-Ritz); its errors are
 those of the FP32-filter path against the FP64 oracle.  Eigenvalues are FP64
@@ -112,3 +116,35 @@ def test_c2_against_krylov_schur(gpu, orc, tol, vectors):
         assert st == 0 and nconv >= nev
         Vo, _ = orc.fix_phase(Vk)
         _check(orc, Us, L, V, Vo, ritz[nev], tol, vectors, f"c2 t={t} tol={tol}")
+
+
+@pytest.mark.parametrize("case", ["c3_bf16", "c4_32"])
+def test_headline_volume_against_krylov_schur(gpu, orc, case):
+    """32^3 timeslices at the configuration tolerance 1e-9, each against the oracle's smearing + FP64 Krylov-Schur on
+    T_12(B) (tol 1e-10): eigenvalues (FP64 Rayleigh quotients) to 1e-10 relative each and of lambda_max, residuals
+    at the tolerance, tr(V^dag V) = nev, and the nev-block subspace to the residual over the gap."""
+    L = 32
+    if case == "c3_bf16":
+        nev, seed, kind, p1, iters = 120, 1229, gpu.SMEAR_STOUT, 0.1, 5
+        prec = gpu.LINKS_BF16
+    else:
+        nev, seed, kind, p1, iters = 180, 1232, gpu.SMEAR_APE, 0.5, 10
+        prec = gpu.LINKS_FP32
+    U = _links(gpu, L, 1, 0.3, seed, [0])[0]
+    s = gpu.Solver([(L, nev)], guard=16, tol=1e-9, deg=48, max_it=400, link_prec=prec, window=gpu.WINDOW_LANCZOS,
+                   smear_kind=kind, smear_p1=p1, smear_iters=iters, smear_compat=1)
+    s.set_links(0, U)
+    st, res = s.run()
+    assert st == 0, res
+    (ev, V, _), ritz = s.get(0), s.ritz(0)
+    s.close()
+    orc.set_threads(os.cpu_count() or 1)
+    Us = orc.smear_stout(U, L, p1, iters, 1) if case == "c3_bf16" else orc.smear_ape(U, L, p1, iters, 1)
+    st, _, Vk, nconv, _, _ = orc.eps_solve(Us, L, 12.0, float(1.1 * (-ev)[-1]), 12, nev, tol=1e-10, max_it=400)
+    assert st == 0 and nconv >= nev
+    Vo, _ = orc.fix_phase(Vk)
+    r = _check(orc, Us, L, V, Vo, ritz[nev], 1e-9, False, f"{case} vs Krylov-Schur")
+    # Davis-Kahan: sin of the largest angle <= residual / gap after lambda_nev (the solver's own Ritz value nev + 1)
+    gap = float(ritz[nev] - (-ev)[-1])
+    assert gap > 0
+    assert r["block_proj"] <= max(10 * 1e-9 * 12.0 / gap, 1e-8), (r["block_proj"], gap)
