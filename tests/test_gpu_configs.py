@@ -118,28 +118,36 @@ def test_c2_against_krylov_schur(gpu, orc, tol, vectors):
         _check(orc, Us, L, V, Vo, ritz[nev], tol, vectors, f"c2 t={t} tol={tol}")
 
 
-@pytest.mark.parametrize("case", ["c3_bf16", "c4_32"])
+@pytest.mark.parametrize("case", ["c3_bf16", "c4_32", "c5_48"])
 def test_headline_volume_against_krylov_schur(gpu, orc, case):
-    """32^3 timeslices at the configuration tolerance 1e-9, each against the oracle's smearing + FP64 Krylov-Schur on
-    T_12(B) (tol 1e-10): eigenvalues (FP64 Rayleigh quotients) to 1e-10 relative each and of lambda_max, residuals
-    at the tolerance, tr(V^dag V) = nev, and the nev-block subspace to the residual over the gap."""
-    L = 32
+    """32^3 and 48^3 timeslices at the configuration tolerance 1e-9, each against the oracle's smearing + FP64
+    Krylov-Schur on T_12(B) (tol 1e-10): eigenvalues (FP64 Rayleigh quotients) to 1e-10 relative each and of
+    lambda_max, residuals at the tolerance, tr(V^dag V) = nev, and the nev-block subspace to the residual over the
+    gap.  C5 (48^3, eps 0.25, stout 6 x 0.1, nev 220) runs with the learned window it specifies."""
+    L, eps, window = 32, 0.3, gpu.WINDOW_LANCZOS
     if case == "c3_bf16":
         nev, seed, kind, p1, iters = 120, 1229, gpu.SMEAR_STOUT, 0.1, 5
         prec = gpu.LINKS_BF16
-    else:
+    elif case == "c4_32":
         nev, seed, kind, p1, iters = 180, 1232, gpu.SMEAR_APE, 0.5, 10
         prec = gpu.LINKS_FP32
-    U = _links(gpu, L, 1, 0.3, seed, [0])[0]
-    s = gpu.Solver([(L, nev)], guard=16, tol=1e-9, deg=48, max_it=400, link_prec=prec, window=gpu.WINDOW_LANCZOS,
+    else:
+        L, eps, window = 48, 0.25, gpu.WINDOW_MLP
+        nev, seed, kind, p1, iters = 220, 1233, gpu.SMEAR_STOUT, 0.1, 6
+        prec = gpu.LINKS_FP32
+    U = _links(gpu, L, 1, eps, seed, [0])[0]
+    s = gpu.Solver([(L, nev)], guard=16, tol=1e-9, deg=48, max_it=400, link_prec=prec, window=window,
                    smear_kind=kind, smear_p1=p1, smear_iters=iters, smear_compat=1)
+    if window == gpu.WINDOW_MLP:
+        from laph_eigsys_b200 import window as lw
+        lw.set_model(s, lw.load_model())
     s.set_links(0, U)
     st, res = s.run()
     assert st == 0, res
     (ev, V, _), ritz = s.get(0), s.ritz(0)
     s.close()
     orc.set_threads(os.cpu_count() or 1)
-    Us = orc.smear_stout(U, L, p1, iters, 1) if case == "c3_bf16" else orc.smear_ape(U, L, p1, iters, 1)
+    Us = orc.smear_ape(U, L, p1, iters, 1) if case == "c4_32" else orc.smear_stout(U, L, p1, iters, 1)
     st, _, Vk, nconv, _, _ = orc.eps_solve(Us, L, 12.0, float(1.1 * (-ev)[-1]), 12, nev, tol=1e-10, max_it=400)
     assert st == 0 and nconv >= nev
     Vo, _ = orc.fix_phase(Vk)
