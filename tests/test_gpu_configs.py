@@ -9,9 +9,11 @@ with every error stated (printed) as well as bounded:
   C2  24^3, eps 0.3, seed 1228, HYP 0.62 / 0.62 x 1, nev 120: timeslices 0
       and 1 against the oracle's smearing + FP64 Krylov-Schur on T_12(B).
   C3  32^3, eps 0.3, seed 1229, stout 5 x 0.1, nev 120, with the BF16 +
-      per-site-scale filter links that configuration specifies, and C4's
-      32^3 lattice (seed 1232, APE 0.5 x 10, nev 180): a timeslice each at
-      the configurations' tolerance 1e-9 against the oracle's Krylov-Schur.
+      per-site-scale filter links that configuration specifies, C4's 32^3
+      lattice (seed 1232, APE 0.5 x 10, nev 180) and C5's 48^3 lattice
+      (seed 1233, eps 0.25, stout 6 x 0.1, nev 220, learned window): a
+      timeslice each at the configurations' tolerance 1e-9 against the
+      oracle's Krylov-Schur.
 
 The block solver's filter runs in FP32 (FP64 Rayleigh-Ritz); its errors are
 those of the FP32-filter path against the FP64 oracle.  Eigenvalues are FP64
