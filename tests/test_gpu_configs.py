@@ -158,3 +158,28 @@ def test_headline_volume_against_krylov_schur(gpu, orc, case):
     gap = float(ritz[nev] - (-ev)[-1])
     assert gap > 0
     assert r["block_proj"] <= max(10 * 1e-9 * 12.0 / gap, 1e-8), (r["block_proj"], gap)
+
+
+def test_largest_lattice_in_the_suite_64(gpu, orc):
+    """64^3 (262144 sites, vectors of 786432 complex entries: past every 32-bit product of sites and columns the
+    smaller cases reach), stout 2 x 0.1: the MatShell product T_12(B) x against the oracle's tv_iter (1e-13; the
+    fused product's grid-stride form, more CTAs than co-resident slots), and the block solver's nev = 16 against the
+    oracle's Krylov-Schur (eigenvalues to 1e-10, residuals at the tolerance)."""
+    L, nev, tol = 64, 16, 1e-9
+    U = _links(gpu, L, 1, 0.3, 1240, [0])[0]
+    orc.set_threads(os.cpu_count() or 1)
+    Us = orc.smear_stout(U, L, 0.1, 2, 1)
+    ctx = gpu.Context(L, 12.0, 0.6, 12)
+    ctx.set_links(Us)
+    rng = np.random.default_rng(7)
+    x = rng.normal(size=3 * L ** 3) + 1j * rng.normal(size=3 * L ** 3)
+    y = ctx.matmult(x, 12)
+    ctx.close()
+    yr = orc.tv_iter(Us, L, 12.0, 0.6, 12, x)
+    assert np.linalg.norm(y - yr) / np.linalg.norm(yr) <= 1e-13
+    out = _solve(gpu, L, nev, [U], tol, 48, smear_kind=gpu.SMEAR_STOUT, smear_p1=0.1, smear_iters=2, smear_compat=1)
+    (ev, V, _), ritz = out[0]
+    st, _, Vk, nconv, _, _ = orc.eps_solve(Us, L, 12.0, float(1.5 * (-ev)[-1]), 12, nev, tol=1e-10, max_it=400)
+    assert st == 0 and nconv >= nev
+    Vo, _ = orc.fix_phase(Vk)
+    _check(orc, Us, L, V, Vo, ritz[nev], tol, False, "64^3 vs Krylov-Schur")
