@@ -884,7 +884,7 @@ def main():
         configs = {}
         for name, kw in (("c1", dict(parity={"kind": "dense", "timeslices": range(16)})),
                          ("c2", dict(wave=16, parity={"kind": "ks", "timeslices": [0]})),
-                         ("c3_bf16", dict(link_prec="bf16")),
+                         ("c3_bf16", dict(link_prec="bf16", parity={"kind": "ks", "timeslices": [0]})),
                          ("c4_wave", dict(wave=[8, 12, 16])),
                          ("c5_wave", dict(wave=16))):
             base = CONFIGS[name.split("_")[0]]
