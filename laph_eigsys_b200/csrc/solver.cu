@@ -1253,7 +1253,6 @@ int laph_solver_footprint(const laph_problem* probs, int n, const laph_solve_opt
     set_error("laph_solver_footprint: bad argument");
     return LAPH_EINVAL;
   }
-  const int kb = opts->block > 0 ? opts->block : 32;
   long long o_u64 = 0, o_uf = 0, o_sc = 0, o_blk = 0, o_kk = 0, o_kv = 0, o_gp = 0, o_rp = 0, o_tc = 0;
   long long max_run = 0, max_v3 = 0;
   for (int i = 0; i < n; ++i) {
